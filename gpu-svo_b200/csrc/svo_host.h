@@ -1,0 +1,15 @@
+// svo_host.h -- host-side pieces of the C ABI (mesh input, OBJ output).
+#pragma once
+#include <cstdint>
+
+#include "svo_b200.h"
+
+namespace svo::host {
+
+void set_error(const char *msg);
+
+// writeVoxel body (src/SVO.cu:755-777): one cube per surface voxel, origin =
+// min + width * (x, y, z) computed on the host (separately rounded).
+int write_voxels(const uint64_t *keys, int64_t n, const float origin[3], float width, const char *path);
+
+}  // namespace svo::host

@@ -1,0 +1,99 @@
+// svo_internal.h -- launch wrappers shared between the kernel files and the C ABI.
+#pragma once
+#include <algorithm>
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "svo_b200.h"
+#include "svo_device.cuh"
+
+namespace svo {
+
+constexpr int kMaxLevels = 24;
+constexpr int kMaxRes = 2048;
+
+// Voxelizer work-split thresholds (bbox volume in voxels).
+struct VoxTuning {
+    uint32_t serial_max = 64;    // tested by one thread
+    uint32_t warp_max = 8192;    // tested by one warp; larger -> CTA queue
+};
+
+// Occupancy bitmap pyramid: level 0 is the voxel grid (one bit per Morton
+// code), level l+1 bit j = OR of level-l bits 8j..8j+7.  Every level is stored
+// as u64 words padded to whole 512-bit blocks; cnt holds one popcount per
+// 512-bit block of every level, pre its exclusive prefix sum.
+struct Pyramid {
+    int levels = 0;                      // stored levels (>= 5)
+    int grid_levels = 0;                 // log2(R) + 1 levels of the real grid
+    uint64_t woff[kMaxLevels] = {};      // u64 word offset of level l
+    uint64_t words[kMaxLevels] = {};     // u64 words of level l
+    uint64_t coff[kMaxLevels + 1] = {};  // block-count offset of level l
+    uint64_t total_words = 0;
+    uint64_t total_blocks = 0;
+    uint32_t ctas = 0;                   // pyramid CTAs (level-0 chunks of 2048 words)
+};
+
+Pyramid make_pyramid(int rx, int ry, int rz);
+
+// Per-level inputs of the node emission kernel.
+struct EmitLevel {
+    uint32_t off;          // first node index of the level
+    uint32_t n;            // nodes in the level
+    const uint64_t *K1;    // sorted codes of level l+1 (the level's groups); level T: its own code
+    const uint64_t *bits;  // bitmap of level l
+    uint64_t coff;         // block-count offset of level l
+    uint32_t side;         // grid side at this level (R >> l)
+    float width;           // node width
+};
+
+struct EmitParams {
+    int T;                  // top level index (depth - 1)
+    uint32_t N;             // total nodes
+    uint32_t flags;
+    EmitLevel lv[kMaxLevels];
+    const uint32_t *pre;    // exclusive prefix of the block counts
+    const GridParams *gp;
+    svo_node *nodes;
+    svo_vertex *verts;      // may be null (SVO_FLAG_NO_VERT_EDGE)
+    svo_edge *edges;
+    unsigned long long *dups;  // [0] vertex, [1] edge consecutive duplicates
+};
+
+cudaError_t launch_bbox(const float *pts, int64_t n, int rx, int ry, int rz, uint32_t *mm_scratch,
+                        GridParams *gp, cudaStream_t st);
+// mm[0] = min, mm[1] = max of n int32 indices.
+cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaStream_t st);
+cudaError_t launch_voxelize(const float *pts, const int32_t *tris, int64_t nt, const GridParams *gp,
+                            int rx, int ry, int rz, bool strict, uint32_t *bm, const VoxTuning &tune,
+                            uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms,
+                            cudaStream_t st);
+// Builds levels 1.. of the pyramid and the per-block counts.
+cudaError_t launch_pyramid(const Pyramid &py, uint64_t *bits, uint32_t *cnt, uint32_t *done,
+                           cudaStream_t st);
+// Exclusive scan of n u32 values; out has n + 1 entries (out[n] = total).
+// scratch: >= scan_scratch_words(n) u64 words, zeroed by the call.
+size_t scan_scratch_words(uint64_t n);
+cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned long long *scratch,
+                        uint32_t *status, cudaStream_t st);
+// Level totals C_l = pre[coff[l+1]] - pre[coff[l]] into totals[l].
+cudaError_t launch_level_totals(const Pyramid &py, const uint32_t *pre, uint32_t *totals,
+                                cudaStream_t st);
+// Sorted codes of levels [l0, l1): out + koff[l] receives level l's codes.
+cudaError_t launch_compact(const Pyramid &py, const uint64_t *bits, const uint32_t *pre, int l0,
+                           int l1, uint64_t *out, const uint64_t *koff, cudaStream_t st);
+cudaError_t launch_emit(const EmitParams &p, int num_sms, cudaStream_t st);
+// Stable removal of consecutive duplicates (thrust::unique semantics).
+cudaError_t launch_unique_vertices(const svo_vertex *in, uint64_t n, svo_vertex *out,
+                                   uint32_t *tile_counts, uint32_t *tile_pre,
+                                   unsigned long long *scan_scratch, uint32_t *status,
+                                   cudaStream_t st);
+cudaError_t launch_unique_edges(const svo_edge *in, uint64_t n, svo_edge *out, uint32_t *tile_counts,
+                                uint32_t *tile_pre, unsigned long long *scan_scratch,
+                                uint32_t *status, cudaStream_t st);
+constexpr uint32_t kUniqueTile = 4096;
+
+// Morton-keyed unique vertex/edge/face keys of all nodes (SVO_FLAG_DEDUP).
+int build_dedup(cudaMemPool_t pool, cudaStream_t st, const EmitParams &p, uint64_t n_out[3], uint64_t *out[3],
+                int num_sms);
+
+}  // namespace svo

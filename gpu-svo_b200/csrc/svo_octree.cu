@@ -1,0 +1,713 @@
+// svo_octree.cu -- octree levels, node records, vertex/edge arrays.
+//
+// The reference builds the octree bottom-up one level per host iteration
+// (src/SVO.cu:383-495): compact a dense flag array, group codes by parent,
+// place each group's 8 siblings, fill missing siblings, link parents and
+// children.  Here every level comes out of one occupancy-bitmap pyramid:
+//   * level l+1 bit j is the OR of level-l bits 8j..8j+7 (a byte test), so
+//     one streaming pass builds all levels (k_pyramid);
+//   * one popcount per 512-bit block and a single exclusive scan give O(1)
+//     rank queries on every level (k_scan);
+//   * the node at local index 8g+k of level l has code 8*K[l+1][g] + k, where
+//     K[l+1] is the sorted list of set bits of level l+1 (k_compact); its
+//     children start at 8*rank_l(code) in level l-1, its parent sits at
+//     8*rank_{l+2}(code >> 6) + ((code >> 3) & 7) in level l+1 -- exactly the
+//     indices the reference's scans produce (src/SVO.cu:221-339);
+//   * k_emit writes node records, vertex and edge arrays in one pass, staged
+//     per warp in shared memory so every global store is a full 512-byte
+//     coalesced streaming write.
+#include <cuda/atomic>
+
+#include "svo_internal.h"
+
+namespace svo {
+
+Pyramid make_pyramid(int rx, int ry, int rz) {
+    Pyramid py;
+    int rmax = std::max(rx, std::max(ry, rz));
+    int k = 0;
+    while ((1 << k) < rmax) ++k;
+    py.grid_levels = k + 1;
+    py.levels = std::max(py.grid_levels, 5);
+    const uint64_t bits0 = 1ull << (3 * k);
+    uint64_t w0 = (bits0 + 63) / 64;
+    w0 = std::max<uint64_t>(w0, 2048);
+    w0 = (w0 + 2047) / 2048 * 2048;
+    auto up8 = [](uint64_t v) { return (v + 7) / 8 * 8; };
+    py.words[0] = w0;
+    py.words[1] = w0 / 8;
+    py.words[2] = w0 / 64;
+    py.words[3] = up8(w0 / 512);
+    py.words[4] = up8((w0 / 2048 + 1) / 2);
+    for (int l = 5; l < py.levels; ++l) py.words[l] = up8((py.words[l - 1] + 7) / 8);
+    uint64_t wo = 0, co = 0;
+    for (int l = 0; l < py.levels; ++l) {
+        py.woff[l] = wo;
+        py.coff[l] = co;
+        wo += py.words[l];
+        co += py.words[l] / 8;
+    }
+    py.coff[py.levels] = co;
+    py.total_words = wo;
+    py.total_blocks = co;
+    py.ctas = (uint32_t)(w0 / 2048);
+    return py;
+}
+
+namespace {
+
+// 8-bit mask of the non-zero bytes of v.
+__device__ __forceinline__ uint32_t nz_bytes(uint64_t v) {
+    uint64_t m = v | (v >> 4);
+    m |= m >> 2;
+    m |= m >> 1;
+    m &= 0x0101010101010101ull;
+    return (uint32_t)((m * 0x0102040810204080ull) >> 56);
+}
+
+// Levels 1..4 per CTA (a CTA owns 2048 words of level 0), then the last CTA
+// to finish builds the remaining levels.
+__global__ void __launch_bounds__(256) k_pyramid(Pyramid py, uint64_t *__restrict__ bits,
+                                                 uint32_t *__restrict__ cnt, uint32_t *__restrict__ done) {
+    __shared__ uint64_t s1[256];
+    __shared__ uint64_t s2[32];
+    __shared__ uint64_t s3[4];
+    __shared__ bool s_last;
+    const uint32_t b = blockIdx.x, t = threadIdx.x;
+    {
+        const uint4 *src = reinterpret_cast<const uint4 *>(bits + py.woff[0] + (uint64_t)b * 2048 + t * 8);
+        uint64_t w1 = 0;
+        uint32_t c0 = 0;
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint4 v = __ldcs(src + q);
+            const uint64_t a = ((uint64_t)v.y << 32) | v.x, c = ((uint64_t)v.w << 32) | v.z;
+            c0 += __popcll(a) + __popcll(c);
+            w1 |= (uint64_t)nz_bytes(a) << (16 * q);
+            w1 |= (uint64_t)nz_bytes(c) << (16 * q + 8);
+        }
+        cnt[py.coff[0] + (uint64_t)b * 256 + t] = c0;
+        bits[py.woff[1] + (uint64_t)b * 256 + t] = w1;
+        s1[t] = w1;
+    }
+    __syncthreads();
+    if (t < 32) {
+        uint64_t w = 0;
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint64_t v = s1[8 * t + k];
+            c += __popcll(v);
+            w |= (uint64_t)nz_bytes(v) << (8 * k);
+        }
+        cnt[py.coff[1] + (uint64_t)b * 32 + t] = c;
+        bits[py.woff[2] + (uint64_t)b * 32 + t] = w;
+        s2[t] = w;
+    }
+    __syncthreads();
+    if (t < 4) {
+        uint64_t w = 0;
+        uint32_t c = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint64_t v = s2[8 * t + k];
+            c += __popcll(v);
+            w |= (uint64_t)nz_bytes(v) << (8 * k);
+        }
+        cnt[py.coff[2] + (uint64_t)b * 4 + t] = c;
+        bits[py.woff[3] + (uint64_t)b * 4 + t] = w;
+        s3[t] = w;
+    }
+    __syncthreads();
+    if (t == 0) {
+        uint32_t w = 0, c = 0;
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            c += __popcll(s3[k]);
+            w |= nz_bytes(s3[k]) << (8 * k);
+        }
+        atomicAdd(cnt + py.coff[3] + b / 2, c);
+        reinterpret_cast<uint32_t *>(bits + py.woff[4])[b] = w;
+    }
+    __threadfence();
+    __syncthreads();
+    if (t == 0) s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    for (int l = 4; l < py.levels; ++l) {
+        const uint64_t *in = bits + py.woff[l];
+        const uint64_t nblk = py.words[l] / 8;
+        const bool has_next = l + 1 < py.levels;
+        uint64_t *out = has_next ? bits + py.woff[l + 1] : nullptr;
+        for (uint64_t j = t; j < nblk; j += blockDim.x) {
+            uint64_t w = 0;
+            uint32_t c = 0;
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                const uint64_t v = __ldcg(in + 8 * j + k);
+                c += __popcll(v);
+                w |= (uint64_t)nz_bytes(v) << (8 * k);
+            }
+            cnt[py.coff[l] + j] = c;
+            if (has_next) out[j] = w;
+        }
+        __syncthreads();
+    }
+    if (t == 0) *done = 0;
+}
+
+// ---------------------------------------------------------------------------
+// Single-pass exclusive scan (decoupled look-back).  Tile status words hold
+// (flag << 32 | value): flag 1 = tile aggregate, 2 = inclusive prefix.  The
+// look-back wait is bounded; on timeout the kernel records
+// kStatusScanTimeout and the host fails the build.
+// ---------------------------------------------------------------------------
+constexpr int kScanThreads = 256;
+constexpr int kScanItems = 8;
+constexpr uint64_t kScanTile = kScanThreads * kScanItems;
+constexpr int kSpinLimit = 1 << 22;
+
+__device__ __forceinline__ unsigned long long ld_relaxed(unsigned long long *p) {
+    return cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(*p).load(
+        cuda::memory_order_relaxed);
+}
+__device__ __forceinline__ void st_relaxed(unsigned long long *p, unsigned long long v) {
+    cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(*p).store(v, cuda::memory_order_relaxed);
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restrict__ in,
+                                                       uint32_t *__restrict__ out, uint64_t n,
+                                                       unsigned long long *__restrict__ scratch,
+                                                       uint32_t *__restrict__ status) {
+    __shared__ uint32_t s_tile, s_prefix;
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    if (t == 0) s_tile = atomicAdd(reinterpret_cast<unsigned int *>(scratch), 1u);
+    __syncthreads();
+    const uint64_t tile = s_tile;
+    unsigned long long *st = scratch + 1;
+    const uint64_t base = tile * kScanTile + (uint64_t)t * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        v[k] = base + k < n ? in[base + k] : 0u;
+        sum += v[k];
+    }
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += o;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < kScanThreads / 32 ? s_warp[lane] : 0u;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, w, d);
+            if (lane >= d) w += o;
+        }
+        if (lane < kScanThreads / 32) s_warp[lane] = w;  // inclusive warp totals
+    }
+    __syncthreads();
+    const uint32_t aggregate = s_warp[kScanThreads / 32 - 1];
+    if (warp == 0) {
+        uint32_t prefix = 0;
+        if (tile == 0) {
+            if (lane == 0) st_relaxed(st, (2ull << 32) | aggregate);
+        } else {
+            if (lane == 0) st_relaxed(st + tile, (1ull << 32) | aggregate);
+            int64_t j = (int64_t)tile - 1;
+            int spins = 0;
+            for (;;) {
+                const int64_t q = j - lane;
+                const unsigned long long s = q >= 0 ? ld_relaxed(st + q) : (2ull << 32);
+                const uint32_t flag = (uint32_t)(s >> 32);
+                if (__any_sync(0xFFFFFFFFu, flag == 0)) {
+                    if (++spins > kSpinLimit) {
+                        if (lane == 0) atomicOr(status, kStatusScanTimeout);
+                        break;
+                    }
+                    __nanosleep(64);
+                    continue;
+                }
+                const uint32_t m2 = __ballot_sync(0xFFFFFFFFu, flag == 2);
+                const int stop = m2 ? __ffs(m2) - 1 : 31;
+                uint32_t val = lane <= stop ? (uint32_t)s : 0u;
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) val += __shfl_xor_sync(0xFFFFFFFFu, val, d);
+                prefix += val;
+                if (m2) break;
+                j -= 32;
+            }
+            if (lane == 0) st_relaxed(st + tile, (2ull << 32) | (prefix + aggregate));
+        }
+        if (lane == 0) s_prefix = prefix;
+    }
+    __syncthreads();
+    uint32_t run = s_prefix + (warp ? s_warp[warp - 1] : 0u) + (incl - sum);
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        if (base + k < n) out[base + k] = run;
+        run += v[k];
+    }
+    const uint64_t last_tile = (n + kScanTile - 1) / kScanTile - 1;
+    if (tile == last_tile && t == kScanThreads - 1) out[n] = s_prefix + aggregate;
+}
+
+__global__ void k_level_totals(Pyramid py, const uint32_t *__restrict__ pre, uint32_t *__restrict__ totals) {
+    const int l = threadIdx.x;
+    if (l < py.levels) totals[l] = pre[py.coff[l + 1]] - pre[py.coff[l]];
+}
+
+struct KOff {
+    uint64_t v[kMaxLevels];
+};
+
+__global__ void __launch_bounds__(256) k_compact(Pyramid py, const uint64_t *__restrict__ bits,
+                                                 const uint32_t *__restrict__ pre, int l0, int l1,
+                                                 uint64_t *__restrict__ out, KOff koff) {
+    const uint64_t g = py.coff[l0] + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (g >= py.coff[l1]) return;
+    int l = l0;
+    while (g >= py.coff[l + 1]) ++l;
+    const uint64_t blk = g - py.coff[l];
+    uint64_t r = pre[g] - pre[py.coff[l]];
+    const uint64_t *w = bits + py.woff[l] + blk * 8;
+    uint64_t *o = out + koff.v[l];
+#pragma unroll 1
+    for (int k = 0; k < 8; ++k) {
+        uint64_t v = w[k];
+        while (v) {
+            o[r++] = blk * 512 + k * 64 + __ffsll((long long)v) - 1;
+            v &= v - 1;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Node emission.
+// ---------------------------------------------------------------------------
+struct NodeInfo {
+    uint64_t code;
+    uint64_t pc;  // parent code (level l+1)
+    int l;
+    bool real;
+    uint32_t child0;
+    uint32_t parent;
+    float o[3];
+    float w;
+};
+
+__device__ __forceinline__ uint32_t rank_of(const EmitParams &P, int l, uint64_t c) {
+    const uint64_t blk = c >> 9;
+    const uint64_t co = P.lv[l].coff;
+    uint32_t r = P.pre[co + blk] - P.pre[co];
+    const uint64_t *w = P.lv[l].bits + blk * 8;
+    const int wi = (int)((c >> 6) & 7);
+    for (int k = 0; k < wi; ++k) r += __popcll(w[k]);
+    r += __popcll(w[wi] & ((1ull << (c & 63)) - 1ull));
+    return r;
+}
+
+__device__ __forceinline__ bool bit_of(const uint64_t *bits, uint64_t c) {
+    return (bits[c >> 6] >> (c & 63)) & 1ull;
+}
+
+template <bool S>
+__device__ __forceinline__ void node_info(const EmitParams &P, const float go[3], uint32_t t, NodeInfo &ni) {
+    int l = 0;
+    while (l < P.T && t >= P.lv[l + 1].off) ++l;
+    const uint32_t i = t - P.lv[l].off;
+    ni.l = l;
+    if (l < P.T) {
+        ni.pc = P.lv[l].K1[i >> 3];
+        ni.code = (ni.pc << 3) | (i & 7);
+    } else {
+        ni.code = P.lv[l].K1[0];
+        ni.pc = ni.code >> 3;
+    }
+    ni.real = l >= 1 && bit_of(P.lv[l].bits, ni.code);
+    ni.child0 = ni.real ? P.lv[l - 1].off + 8u * rank_of(P, l, ni.code) : kNone;
+    if (l < P.T) {
+        const uint32_t pl = (l + 1 < P.T) ? 8u * rank_of(P, l + 2, ni.pc >> 3) + (uint32_t)(ni.pc & 7) : 0u;
+        ni.parent = P.lv[l + 1].off + pl;
+    } else {
+        ni.parent = kNone;
+    }
+    ni.w = P.lv[l].width;
+    const uint32_t x = compact3(ni.code), y = compact3(ni.code >> 1), z = compact3(ni.code >> 2);
+    ni.o[0] = Fp<S>::origin(go[0], ni.w, (float)x);
+    ni.o[1] = Fp<S>::origin(go[1], ni.w, (float)y);
+    ni.o[2] = Fp<S>::origin(go[2], ni.w, (float)z);
+}
+
+// Full 27-neighbourhood: the same-level node at offset (dx,dy,dz) exists iff
+// its parent group is a set bit of the next level.
+__device__ __forceinline__ uint32_t neighbor_of(const EmitParams &P, const NodeInfo &ni, uint32_t self, int j) {
+    if (j == 13) return self;
+    if (ni.l >= P.T) return kNone;
+    const int dx = j % 3 - 1, dy = (j / 3) % 3 - 1, dz = j / 9 - 1;
+    const int side = (int)P.lv[ni.l].side;
+    const int x = (int)compact3(ni.code) + dx, y = (int)compact3(ni.code >> 1) + dy,
+              z = (int)compact3(ni.code >> 2) + dz;
+    if (x < 0 || y < 0 || z < 0 || x >= side || y >= side || z >= side) return kNone;
+    const uint64_t c = morton3((uint32_t)x, (uint32_t)y, (uint32_t)z);
+    const int l1 = ni.l + 1;
+    if (!bit_of(P.lv[l1].bits, c >> 3)) return kNone;
+    const uint32_t g = (l1 < P.T) ? rank_of(P, l1, c >> 3) : 0u;
+    return P.lv[ni.l].off + 8u * g + (uint32_t)(c & 7);
+}
+
+// Corners (Morton-numbered) joined by edge e, in the reference's edge order
+// 02 23 31 10 46 67 75 54 04 26 37 15 (src/SVO.cu:610,638-663).
+__host__ __device__ constexpr int edge_corner(int e, int s) {
+    return (int)(((s ? 0x576445760132ull : 0x132057641320ull) >> (4 * e)) & 0xFull);
+}
+
+// Warp copy of nbytes (multiple of 8) from shared to global memory, in
+// 16-byte streaming stores.
+__device__ __forceinline__ void warp_copy_out(const uint4 *src, char *dst, uint32_t nbytes, int lane) {
+    const uint32_t nv = nbytes / 16;
+    uint4 *d4 = reinterpret_cast<uint4 *>(dst);
+    for (uint32_t v = lane; v < nv; v += 32) __stcs(d4 + v, src[v]);
+    if ((nbytes & 15) && lane == 0) {
+        const unsigned long long *s8 = reinterpret_cast<const unsigned long long *>(src);
+        __stcs(reinterpret_cast<unsigned long long *>(dst) + nv * 2, s8[nv * 2]);
+    }
+}
+
+__device__ __forceinline__ bool veq(const float *a, const float *b) {
+    return a[0] == b[0] && a[1] == b[1] && a[2] == b[2];
+}
+
+constexpr int kEmitWarps = 4;
+constexpr int kEmitBufBytes = 32 * 336;  // per warp
+
+template <bool S, bool FULL, bool VE>
+__global__ void __launch_bounds__(kEmitWarps * 32) k_emit(EmitParams P) {
+    extern __shared__ uint4 smem[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint4 *wbuf = smem + warp * (kEmitBufBytes / 16);
+    const float go[3] = {P.gp->origin[0], P.gp->origin[1], P.gp->origin[2]};
+    const uint64_t nwarps = (uint64_t)gridDim.x * kEmitWarps;
+    unsigned long long vdup = 0, edup = 0;
+    for (uint64_t base = ((uint64_t)blockIdx.x * kEmitWarps + warp) * 32; base < P.N; base += nwarps * 32) {
+        const uint32_t t = (uint32_t)(base + lane);
+        const bool valid = base + lane < P.N;
+        const uint32_t cnt = (uint32_t)(P.N - base < 32 ? P.N - base : 32);
+        NodeInfo ni;
+        if (valid) node_info<S>(P, go, t, ni);
+        uint32_t nb[27];
+#pragma unroll
+        for (int j = 0; j < 27; ++j) nb[j] = kNone;
+        if (valid) {
+            if (FULL) {
+#pragma unroll 1
+                for (int j = 0; j < 27; ++j) nb[j] = neighbor_of(P, ni, t, j);
+            } else if (ni.l == P.T && P.T >= 1) {
+                nb[13] = t;  // root self entry, src/SVO.cu:522-529,556-557
+            }
+        }
+        // ---- node records (21 u64 words each) ----
+        if (valid) {
+            unsigned long long *d = reinterpret_cast<unsigned long long *>(wbuf) + lane * 21;
+            const uint32_t leaf = (ni.l == 0 || !ni.real) ? 1u : 0u;
+            uint32_t ch[8];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) ch[k] = ni.real ? ni.child0 + k : kNone;
+            auto pk = [](uint32_t lo, uint32_t hi) { return ((unsigned long long)hi << 32) | lo; };
+            d[0] = pk((uint32_t)ni.code, leaf);
+            d[1] = pk(__float_as_uint(ni.o[0]), __float_as_uint(ni.o[1]));
+            d[2] = pk(__float_as_uint(ni.o[2]), __float_as_uint(ni.w));
+            d[3] = pk(ni.parent, ch[0]);
+            d[4] = pk(ch[1], ch[2]);
+            d[5] = pk(ch[3], ch[4]);
+            d[6] = pk(ch[5], ch[6]);
+            d[7] = pk(ch[7], nb[0]);
+#pragma unroll
+            for (int k = 0; k < 13; ++k) d[8 + k] = pk(nb[1 + 2 * k], nb[2 + 2 * k]);
+        }
+        __syncwarp();
+        warp_copy_out(wbuf, reinterpret_cast<char *>(P.nodes) + base * 168, cnt * 168, lane);
+        __syncwarp();
+        if (!VE) continue;
+        // ---- vertices: corner i = width * (i&1, i>>1&1, i>>2&1), src/SVO.cu:586-608 ----
+        float vp[8][3];
+        uint32_t vown[8];
+        if (valid) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) {
+                vp[i][0] = __fmul_rn(ni.w, (float)(i & 1));
+                vp[i][1] = __fmul_rn(ni.w, (float)((i >> 1) & 1));
+                vp[i][2] = __fmul_rn(ni.w, (float)((i >> 2) & 1));
+                uint32_t own = t;
+                if (FULL) {
+                    const int cx = i & 1, cy = (i >> 1) & 1, cz = (i >> 2) & 1;
+                    uint32_t best = kNone;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q) {
+                        const int s = (cx - 1 + (q & 1) + 1) + 3 * (cy - 1 + ((q >> 1) & 1) + 1) +
+                                      9 * (cz - 1 + ((q >> 2) & 1) + 1);
+                        best = min(best, nb[s]);
+                    }
+                    own = best;
+                }
+                vown[i] = own;
+                wbuf[lane * 8 + (i ^ (lane & 7))] =
+                    make_uint4(__float_as_uint(vp[i][0]), __float_as_uint(vp[i][1]),
+                               __float_as_uint(vp[i][2]), own);
+            }
+        }
+        __syncwarp();
+        {
+            const uint32_t nv = cnt * 8;
+            uint4 *d4 = reinterpret_cast<uint4 *>(P.verts + base * 8);
+            for (uint32_t v = lane; v < nv; v += 32) {
+                const uint32_t node = v >> 3, k = v & 7;
+                __stcs(d4 + v, wbuf[node * 8 + (k ^ (node & 7))]);
+            }
+        }
+        __syncwarp();
+        // ---- edges: 12 per node in the reference's order, src/SVO.cu:629-677 ----
+        float cp[8][3];
+        float pw = 0.0f;
+        float po[3] = {0.0f, 0.0f, 0.0f};
+        {
+            // previous node's width and origin (for the duplicate checks)
+            pw = __shfl_up_sync(0xFFFFFFFFu, valid ? ni.w : 0.0f, 1);
+#pragma unroll
+            for (int a = 0; a < 3; ++a) po[a] = __shfl_up_sync(0xFFFFFFFFu, valid ? ni.o[a] : 0.0f, 1);
+            if (lane == 0 && valid && t > 0) {
+                NodeInfo pn;
+                node_info<S>(P, go, t - 1, pn);
+                pw = pn.w;
+                po[0] = pn.o[0];
+                po[1] = pn.o[1];
+                po[2] = pn.o[2];
+            }
+        }
+        if (valid) {
+#pragma unroll
+            for (int c = 0; c < 8; ++c) {
+                if (c == 0) {
+                    cp[0][0] = ni.o[0];
+                    cp[0][1] = ni.o[1];
+                    cp[0][2] = ni.o[2];
+                } else {
+                    cp[c][0] = __fadd_rn(ni.o[0], (c & 1) ? ni.w : 0.0f);
+                    cp[c][1] = __fadd_rn(ni.o[1], (c & 2) ? ni.w : 0.0f);
+                    cp[c][2] = __fadd_rn(ni.o[2], (c & 4) ? ni.w : 0.0f);
+                }
+            }
+            uint32_t eown[12];
+#pragma unroll
+            for (int e = 0; e < 12; ++e) {
+                uint32_t own = t;
+                if (FULL) {
+                    const int a = edge_corner(e, 0), b = edge_corner(e, 1);
+                    uint32_t best = kNone;
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) {
+                        int d[3], qq = 0;
+#pragma unroll
+                        for (int ax = 0; ax < 3; ++ax) {
+                            const int ca = (a >> ax) & 1, cb = (b >> ax) & 1;
+                            if (ca != cb) {
+                                d[ax] = 0;
+                            } else {
+                                d[ax] = ca - 1 + ((q >> qq) & 1);
+                                ++qq;
+                            }
+                        }
+                        best = min(best, nb[(d[0] + 1) + 3 * (d[1] + 1) + 9 * (d[2] + 1)]);
+                    }
+                    own = best;
+                }
+                eown[e] = own;
+            }
+            // 84 words per node: edge e = p0 (3), p1 (3), owner
+            uint4 *d = wbuf + lane * 21;
+#pragma unroll
+            for (int j = 0; j < 21; ++j) {
+                uint32_t wv[4];
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int wi = 4 * j + q, e = wi / 7, f = wi % 7;
+                    wv[q] = f < 3   ? __float_as_uint(cp[edge_corner(e, 0)][f])
+                            : f < 6 ? __float_as_uint(cp[edge_corner(e, 1)][f - 3])
+                                    : eown[e];
+                }
+                d[j] = make_uint4(wv[0], wv[1], wv[2], wv[3]);
+            }
+            // consecutive duplicates (thrust::unique, src/SVO.cu:679-725)
+#pragma unroll
+            for (int i = 1; i < 8; ++i) vdup += veq(vp[i], vp[i - 1]);
+            if (t > 0) {
+                const float pv7[3] = {__fmul_rn(pw, 1.0f), __fmul_rn(pw, 1.0f), __fmul_rn(pw, 1.0f)};
+                vdup += veq(vp[0], pv7);
+            }
+#pragma unroll
+            for (int e = 1; e < 12; ++e) {
+                const float *a0 = cp[edge_corner(e - 1, 0)], *a1 = cp[edge_corner(e - 1, 1)];
+                const float *b0 = cp[edge_corner(e, 0)], *b1 = cp[edge_corner(e, 1)];
+                edup += (veq(a0, b0) && veq(a1, b1)) || (veq(a0, b1) && veq(a1, b0));
+            }
+            if (t > 0) {
+                // previous node's edge 11 = (corner 1, corner 5)
+                const float q1[3] = {__fadd_rn(po[0], pw), __fadd_rn(po[1], 0.0f), __fadd_rn(po[2], 0.0f)};
+                const float q5[3] = {__fadd_rn(po[0], pw), __fadd_rn(po[1], 0.0f), __fadd_rn(po[2], pw)};
+                const float *b0 = cp[0], *b1 = cp[2];
+                edup += (veq(q1, b0) && veq(q5, b1)) || (veq(q1, b1) && veq(q5, b0));
+            }
+        }
+        __syncwarp();
+        warp_copy_out(wbuf, reinterpret_cast<char *>(P.edges) + base * 336, cnt * 336, lane);
+        __syncwarp();
+    }
+    if (VE) {
+#pragma unroll
+        for (int d = 16; d > 0; d >>= 1) {
+            vdup += __shfl_xor_sync(0xFFFFFFFFu, vdup, d);
+            edup += __shfl_xor_sync(0xFFFFFFFFu, edup, d);
+        }
+        if (lane == 0 && vdup) atomicAdd(P.dups, vdup);
+        if (lane == 0 && edup) atomicAdd(P.dups + 1, edup);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Stable removal of consecutive duplicates (rare path).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool same(const svo_vertex &a, const svo_vertex &b) { return veq(a.pos, b.pos); }
+__device__ __forceinline__ bool same(const svo_edge &a, const svo_edge &b) {
+    return (veq(a.p0, b.p0) && veq(a.p1, b.p1)) || (veq(a.p0, b.p1) && veq(a.p1, b.p0));
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_unique_count(const T *__restrict__ in, uint64_t n,
+                                                      uint32_t *__restrict__ tile_counts) {
+    __shared__ uint32_t s[8];
+    const uint64_t t0 = (uint64_t)blockIdx.x * kUniqueTile;
+    uint32_t c = 0;
+    for (uint32_t k = threadIdx.x; k < kUniqueTile; k += blockDim.x) {
+        const uint64_t i = t0 + k;
+        if (i < n) c += (i == 0 || !same(in[i - 1], in[i]));
+    }
+    c = __reduce_add_sync(0xFFFFFFFFu, c);
+    if ((threadIdx.x & 31) == 0) s[threadIdx.x >> 5] = c;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t tot = 0;
+        for (int w = 0; w < 8; ++w) tot += s[w];
+        tile_counts[blockIdx.x] = tot;
+    }
+}
+
+template <class T>
+__global__ void __launch_bounds__(256) k_unique_scatter(const T *__restrict__ in, uint64_t n,
+                                                        const uint32_t *__restrict__ tile_pre,
+                                                        T *__restrict__ out) {
+    __shared__ uint32_t s_w[8];
+    const uint64_t t0 = (uint64_t)blockIdx.x * kUniqueTile;
+    uint32_t run = tile_pre[blockIdx.x];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (uint32_t k0 = 0; k0 < kUniqueTile; k0 += blockDim.x) {
+        const uint64_t i = t0 + k0 + threadIdx.x;
+        const bool keep = i < n && (i == 0 || !same(in[i - 1], in[i]));
+        const uint32_t m = __ballot_sync(0xFFFFFFFFu, keep);
+        if (lane == 0) s_w[warp] = __popc(m);
+        __syncthreads();
+        uint32_t before = 0, tot = 0;
+        for (int w = 0; w < 8; ++w) {
+            if (w < warp) before += s_w[w];
+            tot += s_w[w];
+        }
+        if (keep) out[run + before + __popc(m & ((1u << lane) - 1u))] = in[i];
+        run += tot;
+        __syncthreads();
+    }
+}
+
+template <class T>
+cudaError_t unique_impl(const T *in, uint64_t n, T *out, uint32_t *tile_counts, uint32_t *tile_pre,
+                        unsigned long long *scan_scratch, uint32_t *status, cudaStream_t st) {
+    const uint64_t tiles = (n + kUniqueTile - 1) / kUniqueTile;
+    if (tiles == 0) return cudaSuccess;
+    k_unique_count<T><<<(unsigned)tiles, 256, 0, st>>>(in, n, tile_counts);
+    cudaError_t e = launch_scan(tile_counts, tile_pre, tiles, scan_scratch, status, st);
+    if (e != cudaSuccess) return e;
+    k_unique_scatter<T><<<(unsigned)tiles, 256, 0, st>>>(in, n, tile_pre, out);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+cudaError_t launch_pyramid(const Pyramid &py, uint64_t *bits, uint32_t *cnt, uint32_t *done, cudaStream_t st) {
+    k_pyramid<<<py.ctas, 256, 0, st>>>(py, bits, cnt, done);
+    return cudaGetLastError();
+}
+
+size_t scan_scratch_words(uint64_t n) { return 1 + (n + kScanTile - 1) / kScanTile; }
+
+cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned long long *scratch,
+                        uint32_t *status, cudaStream_t st) {
+    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, scan_scratch_words(n) * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    if (tiles == 0) return cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
+    k_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, scratch, status);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_level_totals(const Pyramid &py, const uint32_t *pre, uint32_t *totals, cudaStream_t st) {
+    k_level_totals<<<1, 32, 0, st>>>(py, pre, totals);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact(const Pyramid &py, const uint64_t *bits, const uint32_t *pre, int l0, int l1,
+                           uint64_t *out, const uint64_t *koff, cudaStream_t st) {
+    const uint64_t nb = py.coff[l1] - py.coff[l0];
+    if (nb == 0) return cudaSuccess;
+    KOff k;
+    for (int l = 0; l < kMaxLevels; ++l) k.v[l] = koff[l];
+    k_compact<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(py, bits, pre, l0, l1, out, k);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_emit(const EmitParams &p, int num_sms, cudaStream_t st) {
+    if (p.N == 0) return cudaSuccess;
+    const uint64_t warps = (p.N + 31) / 32;
+    const unsigned blocks = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((warps + kEmitWarps - 1) / kEmitWarps, (uint64_t)num_sms * 12));
+    const size_t shmem = (size_t)kEmitWarps * kEmitBufBytes;
+    const bool s = (p.flags & SVO_FLAG_STRICT_FP) != 0, f = (p.flags & SVO_FLAG_FULL_NEIGHBORS) != 0,
+               ve = p.verts != nullptr;
+#define SVO_EMIT(S_, F_, V_) k_emit<S_, F_, V_><<<blocks, kEmitWarps * 32, shmem, st>>>(p)
+    if (s) {
+        if (f) { if (ve) SVO_EMIT(true, true, true); else SVO_EMIT(true, true, false); }
+        else { if (ve) SVO_EMIT(true, false, true); else SVO_EMIT(true, false, false); }
+    } else {
+        if (f) { if (ve) SVO_EMIT(false, true, true); else SVO_EMIT(false, true, false); }
+        else { if (ve) SVO_EMIT(false, false, true); else SVO_EMIT(false, false, false); }
+    }
+#undef SVO_EMIT
+    return cudaGetLastError();
+}
+
+cudaError_t launch_unique_vertices(const svo_vertex *in, uint64_t n, svo_vertex *out, uint32_t *tile_counts,
+                                   uint32_t *tile_pre, unsigned long long *scan_scratch, uint32_t *status,
+                                   cudaStream_t st) {
+    return unique_impl(in, n, out, tile_counts, tile_pre, scan_scratch, status, st);
+}
+
+cudaError_t launch_unique_edges(const svo_edge *in, uint64_t n, svo_edge *out, uint32_t *tile_counts,
+                                uint32_t *tile_pre, unsigned long long *scan_scratch, uint32_t *status,
+                                cudaStream_t st) {
+    return unique_impl(in, n, out, tile_counts, tile_pre, scan_scratch, status, st);
+}
+
+}  // namespace svo

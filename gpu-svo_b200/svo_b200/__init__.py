@@ -1,0 +1,311 @@
+"""Python binding (ctypes) of the B200 SVO library, libsvo_b200.so.
+
+The library is the product: CUDA kernels for sm_100a behind the C ABI in
+include/svo_b200.h.  This module only marshals arguments; it fails loudly when
+the shared library is missing (there is no CPU fallback).
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+LIB_PATH = os.path.join(PKG_ROOT, "lib", "libsvo_b200.so")
+CLI_PATH = os.path.join(PKG_ROOT, "bin", "svo_main")
+
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_CUDA = 2
+ERR_OUT_OF_MEMORY = 3
+ERR_EMPTY = 4
+ERR_DEGENERATE = 5
+ERR_IO = 6
+ERR_PARSE = 7
+ERR_UNSUPPORTED = 8
+ERR_DEVICE_TIMEOUT = 9
+
+FLAG_FULL_NEIGHBORS = 0x1
+FLAG_DEDUP = 0x2
+FLAG_STRICT_FP = 0x4
+FLAG_NO_VERT_EDGE = 0x8
+FLAG_NO_KEYS = 0x10
+
+NODE_DTYPE = np.dtype(
+    [
+        ("morton_code", "<u4"),
+        ("is_leaf", "u1"),
+        ("pad_", "u1", (3,)),
+        ("origin", "<f4", (3,)),
+        ("width", "<f4"),
+        ("parent", "<u4"),
+        ("childs", "<u4", (8,)),
+        ("neighbors", "<u4", (27,)),
+    ]
+)
+VERTEX_DTYPE = np.dtype([("pos", "<f4", (3,)), ("owner", "<u4")])
+EDGE_DTYPE = np.dtype([("p0", "<f4", (3,)), ("p1", "<f4", (3,)), ("owner", "<u4")])
+assert NODE_DTYPE.itemsize == 168 and VERTEX_DTYPE.itemsize == 16 and EDGE_DTYPE.itemsize == 28
+
+
+class SvoError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"svo error {code}: {msg}")
+        self.code = code
+
+
+class _Aabb(C.Structure):
+    _fields_ = [("min", C.c_float * 3), ("max", C.c_float * 3), ("width", C.c_float * 3)]
+
+
+class MeshDesc(C.Structure):
+    _fields_ = [
+        ("points", C.c_void_p),
+        ("n_points", C.c_int64),
+        ("tris", C.c_void_p),
+        ("n_tris", C.c_int64),
+        ("res", C.c_int * 3),
+        ("flags", C.c_uint32),
+    ]
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    """Loads libsvo_b200.so (build it with `make -C gpu-svo_b200`)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise FileNotFoundError(f"{LIB_PATH} is missing: build it with `make -C gpu-svo_b200`")
+        L = C.CDLL(LIB_PATH)
+        vp, i64, i64p = C.c_void_p, C.c_int64, C.POINTER(C.c_int64)
+        L.svo_last_error.restype = C.c_char_p
+        L.svo_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
+        L.svo_ctx_destroy.argtypes = [vp]
+        L.svo_ctx_destroy.restype = None
+        L.svo_load_obj.argtypes = [C.c_char_p, C.POINTER(vp), i64p, C.POINTER(vp), i64p]
+        L.svo_free_host.argtypes = [vp]
+        L.svo_free_host.restype = None
+        L.svo_bbox_cube.argtypes = [vp, i64, C.POINTER(_Aabb)]
+        L.svo_build.argtypes = [vp, vp, i64, vp, i64, C.c_int, C.c_int, C.c_int, C.c_uint32, vp, C.POINTER(vp)]
+        L.svo_build_batch.argtypes = [vp, C.POINTER(MeshDesc), C.c_int, vp, C.POINTER(vp), C.POINTER(C.c_int)]
+        L.svo_result_free.argtypes = [vp]
+        L.svo_result_free.restype = None
+        L.svo_result_depth.argtypes = [vp]
+        for name in ("num_nodes", "num_vertices", "num_edges", "num_keys"):
+            f = getattr(L, f"svo_result_{name}")
+            f.argtypes = [vp]
+            f.restype = i64
+        L.svo_result_level_counts.argtypes = [vp, vp, C.c_int]
+        L.svo_result_bbox.argtypes = [vp, C.POINTER(_Aabb)]
+        for name in ("nodes", "vertices", "edges", "keys"):
+            f = getattr(L, f"svo_result_{name}_device")
+            f.argtypes = [vp]
+            f.restype = vp
+            g = getattr(L, f"svo_result_copy_{name}")
+            g.argtypes = [vp, vp, i64]
+        L.svo_result_num_dedup.argtypes = [vp, C.c_int]
+        L.svo_result_num_dedup.restype = i64
+        L.svo_result_copy_dedup.argtypes = [vp, C.c_int, vp, i64]
+        L.svo_write_tree.argtypes = [vp, C.c_char_p]
+        L.svo_write_tree_nodes.argtypes = [vp, i64, C.c_char_p]
+        L.svo_write_voxels.argtypes = [vp, C.c_char_p]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != OK:
+        raise SvoError(rc, lib().svo_last_error().decode(errors="replace"))
+
+
+def load_obj(path: str):
+    """BaseModel::loadOBJ -> (points float32[n,3], tris int32[m,3])."""
+    L = lib()
+    pp, tp = C.c_void_p(), C.c_void_p()
+    npnt, ntri = C.c_int64(), C.c_int64()
+    _check(L.svo_load_obj(os.fsencode(path), C.byref(pp), C.byref(npnt), C.byref(tp), C.byref(ntri)))
+    try:
+        pts = np.ctypeslib.as_array(C.cast(pp, C.POINTER(C.c_float)), (max(1, npnt.value * 3),))[: npnt.value * 3]
+        tri = np.ctypeslib.as_array(C.cast(tp, C.POINTER(C.c_int32)), (max(1, ntri.value * 3),))[: ntri.value * 3]
+        return pts.reshape(-1, 3).copy(), tri.reshape(-1, 3).copy()
+    finally:
+        L.svo_free_host(pp)
+        L.svo_free_host(tp)
+
+
+def bbox_cube(points: np.ndarray) -> np.ndarray:
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    box = _Aabb()
+    _check(lib().svo_bbox_cube(pts.ctypes.data, pts.shape[0], C.byref(box)))
+    return np.array(list(box.min) + list(box.max) + list(box.width), dtype=np.float32)
+
+
+def write_tree_nodes(nodes: np.ndarray, path: str) -> None:
+    n = np.ascontiguousarray(nodes, dtype=NODE_DTYPE)
+    _check(lib().svo_write_tree_nodes(n.ctypes.data, n.shape[0], os.fsencode(path)))
+
+
+def _res3(res):
+    if isinstance(res, (int, np.integer)):
+        return (int(res),) * 3
+    return tuple(int(r) for r in res)
+
+
+def _ptr(a) -> int:
+    """Address of a numpy array, or of a torch tensor (host or CUDA)."""
+    if a is None:
+        return 0
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return a.ctypes.data
+
+
+class Context:
+    """svo_ctx: per-device state (memory pool, tuning)."""
+
+    def __init__(self, device: int = 0):
+        h = C.c_void_p()
+        _check(lib().svo_ctx_create(device, C.byref(h)))
+        self._h = h
+
+    @property
+    def handle(self):
+        return self._h
+
+    def close(self) -> None:
+        if self._h:
+            lib().svo_ctx_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def build(self, points, tris, res, flags: int = 0, stream: int = 0) -> "Result":
+        """svo_build.  points float32[n,3] and tris int32[m,3] (tris=None: soup),
+        numpy (host) or torch CUDA tensors (device)."""
+        if isinstance(points, np.ndarray):
+            points = np.ascontiguousarray(points, dtype=np.float32)
+        if isinstance(tris, np.ndarray):
+            tris = np.ascontiguousarray(tris, dtype=np.int32)
+        n_points = points.shape[0]
+        n_tris = 0 if tris is None else tris.shape[0]
+        rx, ry, rz = _res3(res)
+        h = C.c_void_p()
+        _check(lib().svo_build(self._h, _ptr(points), n_points, _ptr(tris), n_tris, rx, ry, rz, flags,
+                               stream or None, C.byref(h)))
+        return Result(h)
+
+    def build_batch(self, meshes, flags: int = 0, stream: int = 0):
+        """svo_build_batch over [(points, tris, res), ...]; returns (results, statuses)."""
+        keep = []
+        descs = (MeshDesc * len(meshes))()
+        for i, (pts, tri, res) in enumerate(meshes):
+            if isinstance(pts, np.ndarray):
+                pts = np.ascontiguousarray(pts, dtype=np.float32)
+            if isinstance(tri, np.ndarray):
+                tri = np.ascontiguousarray(tri, dtype=np.int32)
+            keep.append((pts, tri))
+            d = descs[i]
+            d.points = _ptr(pts)
+            d.n_points = pts.shape[0]
+            d.tris = _ptr(tri) if tri is not None else None
+            d.n_tris = 0 if tri is None else tri.shape[0]
+            d.res[:] = _res3(res)
+            d.flags = flags
+        outs = (C.c_void_p * len(meshes))()
+        st = (C.c_int * len(meshes))()
+        rc = lib().svo_build_batch(self._h, descs, len(meshes), stream or None, outs, st)
+        results = [Result(C.c_void_p(outs[i])) if st[i] == OK else None for i in range(len(meshes))]
+        return results, list(st), rc
+
+
+class Result:
+    """svo_result: device-resident octree of one build."""
+
+    def __init__(self, h: C.c_void_p):
+        self._h = h
+
+    def close(self) -> None:
+        if self._h:
+            lib().svo_result_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def depth(self) -> int:
+        return lib().svo_result_depth(self._h)
+
+    @property
+    def num_nodes(self) -> int:
+        return lib().svo_result_num_nodes(self._h)
+
+    @property
+    def num_vertices(self) -> int:
+        return lib().svo_result_num_vertices(self._h)
+
+    @property
+    def num_edges(self) -> int:
+        return lib().svo_result_num_edges(self._h)
+
+    @property
+    def num_keys(self) -> int:
+        return lib().svo_result_num_keys(self._h)
+
+    @property
+    def level_counts(self) -> np.ndarray:
+        out = np.zeros(64, dtype=np.int64)
+        n = lib().svo_result_level_counts(self._h, out.ctypes.data, 64)
+        return out[:n].copy()
+
+    @property
+    def bbox(self) -> np.ndarray:
+        box = _Aabb()
+        _check(lib().svo_result_bbox(self._h, C.byref(box)))
+        return np.array(list(box.min) + list(box.max) + list(box.width), dtype=np.float32)
+
+    def _copy(self, name: str, n: int, dtype) -> np.ndarray:
+        out = np.zeros(n, dtype=dtype)
+        _check(getattr(lib(), f"svo_result_copy_{name}")(self._h, out.ctypes.data, n))
+        return out
+
+    def nodes(self) -> np.ndarray:
+        return self._copy("nodes", self.num_nodes, NODE_DTYPE)
+
+    def vertices(self) -> np.ndarray:
+        return self._copy("vertices", self.num_vertices, VERTEX_DTYPE)
+
+    def edges(self) -> np.ndarray:
+        return self._copy("edges", self.num_edges, EDGE_DTYPE)
+
+    def keys(self) -> np.ndarray:
+        return self._copy("keys", self.num_keys, np.uint64)
+
+    def dedup(self, kind: int) -> np.ndarray:
+        n = lib().svo_result_num_dedup(self._h, kind)
+        out = np.zeros(max(n, 0), dtype=np.uint64)
+        _check(lib().svo_result_copy_dedup(self._h, kind, out.ctypes.data, out.shape[0]))
+        return out
+
+    def device_ptr(self, name: str) -> int:
+        return getattr(lib(), f"svo_result_{name}_device")(self._h) or 0
+
+    def write_tree(self, path: str) -> None:
+        _check(lib().svo_write_tree(self._h, os.fsencode(path)))
+
+    def write_voxels(self, path: str) -> None:
+        _check(lib().svo_write_voxels(self._h, os.fsencode(path)))

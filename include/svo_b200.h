@@ -1,0 +1,181 @@
+/*
+ * svo_b200.h -- C ABI of the B200-native sparse voxel octree builder.
+ *
+ * This is the drop-in boundary for GPU-SVO's build path.  Each entry point
+ * names the reference interface it replaces (paths relative to the GPU-SVO
+ * project root).  The reference itself is a C++ static library with no C
+ * entry points; these are the calls an FFI binding of its `SparseVoxelOctree`
+ * / `BaseModel` classes would make.  All functions return SVO_OK (0) or a
+ * status code; none of them exits the process (the reference's CUDA_CHECK /
+ * getLastCudaError call exit(), src/CUDAUtil.h:21-48).  svo_last_error()
+ * returns the calling thread's last error message.
+ *
+ * Pointers to mesh data may be host or device memory; the library detects
+ * which.  Result arrays live in device memory until copied out.
+ */
+#ifndef SVO_B200_H
+#define SVO_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes --------------------------------------------------------- */
+#define SVO_OK 0
+#define SVO_ERR_INVALID_ARGUMENT 1
+#define SVO_ERR_CUDA 2
+#define SVO_ERR_OUT_OF_MEMORY 3
+#define SVO_ERR_EMPTY 4       /* no surface voxels (the reference aborts) */
+#define SVO_ERR_DEGENERATE 5  /* input for which the reference's build is undefined */
+#define SVO_ERR_IO 6
+#define SVO_ERR_PARSE 7
+#define SVO_ERR_UNSUPPORTED 8
+#define SVO_ERR_DEVICE_TIMEOUT 9 /* a bounded device-side wait gave up */
+
+/* ---- build flags ---------------------------------------------------------- */
+/* Default (0): the reference's effective behaviour bit for bit, including its
+ * neighbour tables (only the root's self entry is ever stored,
+ * src/SVO.cu:535-542) and its vertex/edge arrays (src/SVO.cu:567-728). */
+#define SVO_FLAG_FULL_NEIGHBORS 0x1u /* real 27-neighbourhood per node (intended semantics),
+                                        vertex/edge owner = smallest sharing node index */
+#define SVO_FLAG_DEDUP 0x2u          /* also emit Morton-keyed unique vertex/edge/face keys */
+#define SVO_FLAG_STRICT_FP 0x4u      /* round every float op (no FMA contraction) */
+#define SVO_FLAG_NO_VERT_EDGE 0x8u   /* skip the per-node vertex/edge arrays */
+#define SVO_FLAG_NO_KEYS 0x10u       /* skip the sorted leaf-voxel key list */
+
+/* ---- records (byte layouts of the reference's types) --------------------- */
+/* SVONode, src/SVO.h:20-35 (168 bytes; pad_ is written as zero). */
+typedef struct svo_node {
+    uint32_t morton_code;
+    uint8_t is_leaf;
+    uint8_t pad_[3];
+    float origin[3];
+    float width;
+    uint32_t parent;
+    uint32_t childs[8];
+    uint32_t neighbors[27];
+} svo_node;
+
+/* thrust::pair<Eigen::Vector3f, uint32_t>, src/SVO.h:50 (16 bytes). */
+typedef struct svo_vertex {
+    float pos[3];
+    uint32_t owner;
+} svo_vertex;
+
+/* thrust::pair<thrust::pair<Vector3f, Vector3f>, uint32_t>, src/SVO.h:37,51 (28 bytes). */
+typedef struct svo_edge {
+    float p0[3];
+    float p1[3];
+    uint32_t owner;
+} svo_edge;
+
+/* AABox<Eigen::Vector3f>, src/BaseModel.h:10-22. */
+typedef struct svo_aabb {
+    float min[3];
+    float max[3];
+    float width[3];
+} svo_aabb;
+
+typedef struct svo_ctx svo_ctx;
+typedef struct svo_result svo_result;
+
+/* ---- context -------------------------------------------------------------- */
+/* Per-device state: stream-ordered memory pool, scratch, tuning.  Replaces the
+ * reference's process-global launch state (src/SVO.cu:15-18) and its
+ * per-call cudaMalloc/thrust allocations (src/SVO.cu:353-376). */
+int svo_ctx_create(int device, svo_ctx **out);
+void svo_ctx_destroy(svo_ctx *ctx);
+
+/* Thread-local message for the last non-zero status. */
+const char *svo_last_error(void);
+
+/* ---- mesh input ----------------------------------------------------------- */
+/* BaseModel::loadOBJ, src/BaseModel.cpp:3-25.  Same accepted lines and quirks
+ * (only "v " / "f " lines; `a/t/n` faces dropped; unterminated last line
+ * dropped).  A line of 255+ characters (the reference loops forever) and a
+ * face index outside the vertex list are SVO_ERR_PARSE.  *points (3 floats per
+ * vertex) and *tris (3 zero-based int32 per triangle) are malloc'd host
+ * arrays; release them with svo_free_host. */
+int svo_load_obj(const char *path, float **points, int64_t *n_points, int32_t **tris,
+                 int64_t *n_tris);
+void svo_free_host(void *p);
+
+/* BaseModel(filename) bounding box + createMeshBBCube, src/BaseModel.h:24-49,64-73.
+ * Host arrays only. */
+int svo_bbox_cube(const float *points, int64_t n_points, svo_aabb *out);
+
+/* ---- build ---------------------------------------------------------------- */
+/* SparseVoxelOctree::create(), src/SVO.cu:341-520 (with meshVoxelize,
+ * src/SVO.cu:37-206, and constructNodeAtrributes, src/SVO.cu:522-735), for
+ * the mesh a SparseVoxelOctree(filename, res_x, res_y, res_z) would hold
+ * (src/SVO.h:61-67): `points` are the model's vertices, `tris` its triangles
+ * (zero-based).  tris == NULL means a triangle soup: n_points = 3 * triangles.
+ * Resolutions up to 1024 reproduce the reference exactly; up to 4096 use
+ * 64-bit Morton codes (the reference's 32-bit codes are wrong above 1024).
+ * `stream` is a cudaStream_t (NULL = the legacy default stream).  On success
+ * *out owns the device arrays of the octree. */
+int svo_build(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t *tris,
+              int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags, void *stream,
+              svo_result **out);
+
+/* Many independent builds in one pass over the device (batched launches; each
+ * mesh's result equals its own svo_build).  descs[i] describes mesh i;
+ * out[i] receives its result.  Status of the first failing mesh is returned;
+ * per-mesh status in status_out (may be NULL). */
+typedef struct svo_mesh_desc {
+    const float *points;
+    int64_t n_points;
+    const int32_t *tris;
+    int64_t n_tris;
+    int res[3];
+    uint32_t flags;
+} svo_mesh_desc;
+int svo_build_batch(svo_ctx *ctx, const svo_mesh_desc *descs, int n, void *stream,
+                    svo_result **out, int *status_out);
+
+/* ---- results (SparseVoxelOctree's private members, src/SVO.h:41-51) ------- */
+void svo_result_free(svo_result *r);
+int svo_result_depth(const svo_result *r);                 /* treeDepth */
+int64_t svo_result_num_nodes(const svo_result *r);         /* numTreeNodes */
+int64_t svo_result_num_vertices(const svo_result *r);      /* nodeVertexArray.size() */
+int64_t svo_result_num_edges(const svo_result *r);         /* nodeEdgeArray.size() */
+int64_t svo_result_num_keys(const svo_result *r);          /* surface voxels */
+/* Node count of each level, finest first (depthNumNodes + the root level);
+ * returns the number of levels. */
+int svo_result_level_counts(const svo_result *r, int64_t *counts, int cap);
+int svo_result_bbox(const svo_result *r, svo_aabb *out);   /* modelBBox */
+/* Device pointers (valid until svo_result_free). */
+const svo_node *svo_result_nodes_device(const svo_result *r);
+const svo_vertex *svo_result_vertices_device(const svo_result *r);
+const svo_edge *svo_result_edges_device(const svo_result *r);
+const uint64_t *svo_result_keys_device(const svo_result *r);
+/* Copies to host memory (cap = capacity in elements; returns SVO_ERR_INVALID_ARGUMENT
+ * when too small). */
+int svo_result_copy_nodes(const svo_result *r, svo_node *dst, int64_t cap);
+int svo_result_copy_vertices(const svo_result *r, svo_vertex *dst, int64_t cap);
+int svo_result_copy_edges(const svo_result *r, svo_edge *dst, int64_t cap);
+int svo_result_copy_keys(const svo_result *r, uint64_t *dst, int64_t cap);
+/* Morton-keyed unique primitives (SVO_FLAG_DEDUP): kind 0 vertices, 1 edges,
+ * 2 faces.  Sorted u64 keys. */
+int64_t svo_result_num_dedup(const svo_result *r, int kind);
+int svo_result_copy_dedup(const svo_result *r, int kind, uint64_t *dst, int64_t cap);
+
+/* ---- output ---------------------------------------------------------------- */
+/* SparseVoxelOctree::writeTree, src/SVO.cu:737-753 with write_cube,
+ * src/IO.h:23-90: writes `path` byte-identical to the reference's file
+ * (the caller forms the name "<stem>_<depth>_tree.obj"). */
+int svo_write_tree(const svo_result *r, const char *path);
+/* The same writer over host node records (e.g. a copied node array). */
+int svo_write_tree_nodes(const svo_node *nodes, int64_t n, const char *path);
+/* SparseVoxelOctree::writeVoxel, src/SVO.cu:755-777: one cube per surface
+ * voxel, decoded from its key (the reference only calls it in NDEBUG builds). */
+int svo_write_voxels(const svo_result *r, const char *path);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SVO_B200_H */

@@ -1,0 +1,203 @@
+"""ctypes binding of the CPU oracle (liboracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the
+CPU legs of bench.py, as the checker or the timed CPU baseline.  The product
+(gpu-svo_b200/) never imports it.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "liboracle.so")
+
+FLAG_FULL_NEIGHBORS = 0x1
+FLAG_DEDUP = 0x2
+FLAG_STRICT_FP = 0x4
+FLAG_NO_VERT_EDGE = 0x8
+
+# SVONode (src/SVO.h:20-35), 168 bytes
+NODE_DTYPE = np.dtype(
+    [
+        ("morton_code", "<u4"),
+        ("is_leaf", "u1"),
+        ("pad_", "u1", (3,)),
+        ("origin", "<f4", (3,)),
+        ("width", "<f4"),
+        ("parent", "<u4"),
+        ("childs", "<u4", (8,)),
+        ("neighbors", "<u4", (27,)),
+    ]
+)
+VERTEX_DTYPE = np.dtype([("pos", "<f4", (3,)), ("owner", "<u4")])
+EDGE_DTYPE = np.dtype([("p0", "<f4", (3,)), ("p1", "<f4", (3,)), ("owner", "<u4")])
+assert NODE_DTYPE.itemsize == 168 and VERTEX_DTYPE.itemsize == 16 and EDGE_DTYPE.itemsize == 28
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"oracle error {code}: {msg}")
+        self.code = code
+
+
+_lib = None
+
+
+def build() -> None:
+    subprocess.run(["make", "-s", "-C", HERE], check=True)
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            build()
+        L = C.CDLL(LIB_PATH)
+        i64p = C.POINTER(C.c_int64)
+        L.oracle_last_error.restype = C.c_char_p
+        L.oracle_load_obj.argtypes = [C.c_char_p, C.POINTER(C.c_void_p), i64p, C.POINTER(C.c_void_p), i64p]
+        L.oracle_free.argtypes = [C.c_void_p]
+        L.oracle_bbox_cube.argtypes = [C.c_void_p, C.c_int64, C.c_void_p]
+        L.oracle_morton_encode.argtypes = [C.c_uint32] * 3
+        L.oracle_morton_encode.restype = C.c_uint64
+        L.oracle_morton_decode.argtypes = [C.c_uint64] + [C.POINTER(C.c_uint32)] * 3
+        L.oracle_build.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                   C.c_uint32, C.c_int, C.POINTER(C.c_void_p)]
+        L.oracle_voxelize.argtypes = [C.c_void_p, C.c_int64, C.c_void_p, C.c_int64, C.c_int, C.c_int, C.c_int,
+                                      C.c_uint32, C.c_int, C.POINTER(C.c_void_p), i64p]
+        for name in ("num_nodes", "num_vertices", "num_edges", "num_keys"):
+            f = getattr(L, f"oracle_result_{name}")
+            f.argtypes = [C.c_void_p]
+            f.restype = C.c_int64
+        L.oracle_result_depth.argtypes = [C.c_void_p]
+        L.oracle_result_level_counts.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+        for name in ("nodes", "vertices", "edges", "keys", "bbox"):
+            f = getattr(L, f"oracle_result_{name}")
+            f.argtypes = [C.c_void_p]
+            f.restype = C.c_void_p
+        L.oracle_result_num_dedup.argtypes = [C.c_void_p, C.c_int]
+        L.oracle_result_num_dedup.restype = C.c_int64
+        L.oracle_result_dedup.argtypes = [C.c_void_p, C.c_int]
+        L.oracle_result_dedup.restype = C.c_void_p
+        L.oracle_tables.argtypes = [C.c_void_p] * 4
+        L.oracle_result_free.argtypes = [C.c_void_p]
+        L.oracle_write_tree.argtypes = [C.c_void_p, C.c_char_p]
+        _lib = L
+    return _lib
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise OracleError(rc, lib().oracle_last_error().decode())
+
+
+def _copy(ptr: int, n: int, dtype) -> np.ndarray:
+    if n == 0:
+        return np.zeros(0, dtype=dtype)
+    buf = (C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr)
+    return np.frombuffer(bytes(buf), dtype=dtype).copy()
+
+
+def load_obj(path: str):
+    """BaseModel::loadOBJ -> (points float32[n,3], tris int32[m,3])."""
+    L = lib()
+    pp, tp = C.c_void_p(), C.c_void_p()
+    npnt, ntri = C.c_int64(), C.c_int64()
+    _check(L.oracle_load_obj(path.encode(), C.byref(pp), C.byref(npnt), C.byref(tp), C.byref(ntri)))
+    pts = _copy(pp.value, npnt.value * 3, np.float32).reshape(-1, 3)
+    tri = _copy(tp.value, ntri.value * 3, np.int32).reshape(-1, 3)
+    L.oracle_free(pp)
+    L.oracle_free(tp)
+    return pts, tri
+
+
+def bbox_cube(points: np.ndarray) -> np.ndarray:
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    out = np.zeros(9, dtype=np.float32)
+    _check(lib().oracle_bbox_cube(pts.ctypes.data, pts.shape[0], out.ctypes.data))
+    return out
+
+
+def morton_encode(x: int, y: int, z: int) -> int:
+    return int(lib().oracle_morton_encode(x, y, z))
+
+
+def tables() -> dict:
+    out = {"neighbor_LUTparent": np.zeros(216, np.int16), "neighbor_LUTchild": np.zeros(216, np.int16),
+           "d_vertSharedLUT": np.zeros(64, np.int16), "d_edgeSharedLUT": np.zeros(48, np.int16)}
+    lib().oracle_tables(*(a.ctypes.data for a in out.values()))
+    return out
+
+
+def morton_decode(code: int):
+    x, y, z = C.c_uint32(), C.c_uint32(), C.c_uint32()
+    lib().oracle_morton_decode(code, C.byref(x), C.byref(y), C.byref(z))
+    return x.value, y.value, z.value
+
+
+def _res3(res):
+    if isinstance(res, int):
+        return (res, res, res)
+    return tuple(int(r) for r in res)
+
+
+def voxelize(points, tris, res, flags: int = 0, threads: int = 0) -> np.ndarray:
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    tri = np.ascontiguousarray(tris, dtype=np.int32)
+    rx, ry, rz = _res3(res)
+    cp, n = C.c_void_p(), C.c_int64()
+    L = lib()
+    _check(L.oracle_voxelize(pts.ctypes.data, pts.shape[0], tri.ctypes.data, tri.shape[0], rx, ry, rz,
+                             flags, threads, C.byref(cp), C.byref(n)))
+    out = _copy(cp.value, n.value, np.uint64)
+    L.oracle_free(cp)
+    return out
+
+
+class Result:
+    """Outputs of the oracle's create(), copied into numpy arrays."""
+
+    def __init__(self, handle):
+        L = lib()
+        self.depth = L.oracle_result_depth(handle)
+        lc = np.zeros(64, dtype=np.int64)
+        n = L.oracle_result_level_counts(handle, lc.ctypes.data, 64)
+        self.level_counts = lc[:n].copy()
+        self.nodes = _copy(L.oracle_result_nodes(handle), L.oracle_result_num_nodes(handle), NODE_DTYPE)
+        self.vertices = _copy(L.oracle_result_vertices(handle), L.oracle_result_num_vertices(handle), VERTEX_DTYPE)
+        self.edges = _copy(L.oracle_result_edges(handle), L.oracle_result_num_edges(handle), EDGE_DTYPE)
+        self.keys = _copy(L.oracle_result_keys(handle), L.oracle_result_num_keys(handle), np.uint64)
+        self.bbox = _copy(L.oracle_result_bbox(handle), 9, np.float32)
+        self.dedup = [
+            _copy(L.oracle_result_dedup(handle, k), max(0, L.oracle_result_num_dedup(handle, k)), np.uint64)
+            for k in range(3)
+        ]
+        self._handle = handle
+
+    def write_tree(self, path: str) -> None:
+        _check(lib().oracle_write_tree(self._handle, path.encode()))
+
+    def close(self) -> None:
+        if self._handle:
+            lib().oracle_result_free(self._handle)
+            self._handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def build_svo(points, tris, res, flags: int = 0, threads: int = 0) -> Result:
+    pts = np.ascontiguousarray(points, dtype=np.float32)
+    tri = np.ascontiguousarray(tris, dtype=np.int32)
+    rx, ry, rz = _res3(res)
+    h = C.c_void_p()
+    _check(lib().oracle_build(pts.ctypes.data, pts.shape[0], tri.ctypes.data, tri.shape[0], rx, ry, rz,
+                              flags, threads, C.byref(h)))
+    return Result(h.value)

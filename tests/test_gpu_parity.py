@@ -1,0 +1,124 @@
+"""GPU build (C ABI, sm_100a kernels) against the oracle, bit for bit."""
+import numpy as np
+import pytest
+
+from conftest import random_mesh
+from parity import assert_same
+
+pytestmark = pytest.mark.gpu
+
+
+def _both(ctx, oracle_mod, v, f, res, flags=0):
+    g = ctx.build(v, f, res, flags)
+    o = oracle_mod.build_svo(v, f, res, flags)
+    return g, o
+
+
+@pytest.mark.parametrize("seed", range(4))
+@pytest.mark.parametrize("res", [2, 3, 5, 8, 16, 33, 64])
+def test_random_blobs(gpu_ctx, oracle_mod, seed, res):
+    v, f = random_mesh(seed, 60)
+    g, o = _both(gpu_ctx, oracle_mod, v, f, res)
+    assert_same(g, o)
+
+
+@pytest.mark.parametrize("kind", ["grid", "sliver"])
+@pytest.mark.parametrize("res", [8, 32, 128])
+def test_hard_triangles(gpu_ctx, oracle_mod, kind, res):
+    v, f = random_mesh(11, 200, kind)
+    g, o = _both(gpu_ctx, oracle_mod, v, f, res)
+    assert_same(g, o)
+
+
+@pytest.mark.parametrize("res", [16, 64, 128, 256])
+def test_bunny(gpu_ctx, oracle_mod, bunny_path, res):
+    v, f = oracle_mod.load_obj(bunny_path)
+    g, o = _both(gpu_ctx, oracle_mod, v, f, res)
+    assert_same(g, o)
+
+
+def test_icosphere_l5(gpu_ctx, oracle_mod):
+    from svo_b200 import meshgen
+
+    v, f, res = meshgen.icosphere_l5()
+    g, o = _both(gpu_ctx, oracle_mod, v, f, res)
+    assert g.num_nodes == 221177 and g.depth == 8
+    assert_same(g, o)
+
+
+@pytest.mark.parametrize("flags", ["strict", "full", "full_strict", "no_ve"])
+def test_modes(gpu_ctx, oracle_mod, bunny_path, flags, svo_mod):
+    fl = {"strict": svo_mod.FLAG_STRICT_FP, "full": svo_mod.FLAG_FULL_NEIGHBORS,
+          "full_strict": svo_mod.FLAG_FULL_NEIGHBORS | svo_mod.FLAG_STRICT_FP,
+          "no_ve": svo_mod.FLAG_NO_VERT_EDGE}[flags]
+    v, f = oracle_mod.load_obj(bunny_path)
+    g, o = _both(gpu_ctx, oracle_mod, v, f, 64, fl)
+    assert_same(g, o, check_ve=flags != "no_ve")
+    if flags == "no_ve":
+        assert g.num_vertices == 0 and g.num_edges == 0
+
+
+def test_anisotropic(gpu_ctx, oracle_mod):
+    v, f = random_mesh(4, 80)
+    g, o = _both(gpu_ctx, oracle_mod, v, f, (16, 32, 8))
+    assert_same(g, o)
+
+
+def test_soup_equals_indexed(gpu_ctx, oracle_mod):
+    v, f = random_mesh(6, 100)
+    a = gpu_ctx.build(v, f, 32)
+    b = gpu_ctx.build(v[f].reshape(-1, 3), None, 32)
+    o = oracle_mod.build_svo(v[f].reshape(-1, 3), np.arange(300, dtype=np.int32).reshape(-1, 3), 32)
+    assert_same(b, o)
+    # the soup has the same vertices, so the same bbox and tree
+    assert a.nodes().tobytes() == b.nodes().tobytes()
+
+
+def test_device_input(gpu_ctx, oracle_mod, bunny_path):
+    import torch
+
+    v, f = oracle_mod.load_obj(bunny_path)
+    dv = torch.from_numpy(v).cuda()
+    df = torch.from_numpy(f).cuda()
+    g = gpu_ctx.build(dv, df, 64)
+    o = oracle_mod.build_svo(v, f, 64)
+    assert_same(g, o)
+
+
+def test_far_offset_duplicates(gpu_ctx, oracle_mod, bunny_path):
+    """Far from the origin the edge corners absorb the node width: the
+    consecutive-unique pass (src/SVO.cu:718-722) then really removes edges."""
+    v, f = oracle_mod.load_obj(bunny_path)
+    v = (v * 0.01 + np.float32(3.0e5)).astype(np.float32)
+    g, o = _both(gpu_ctx, oracle_mod, v, f, 64)
+    assert len(o.edges) < 12 * len(o.nodes)
+    assert_same(g, o)
+
+
+def test_repeat_builds_identical(gpu_ctx, bunny_path, oracle_mod):
+    v, f = oracle_mod.load_obj(bunny_path)
+    a = gpu_ctx.build(v, f, 128)
+    b = gpu_ctx.build(v, f, 128)
+    assert a.nodes().tobytes() == b.nodes().tobytes()
+    assert a.edges().tobytes() == b.edges().tobytes()
+
+
+def test_errors(gpu_ctx, svo_mod):
+    pts = np.array([[0, 0, 0], [1, 1, 1], [0.5, 0.2, 0.1]], dtype=np.float32)
+    cases = [
+        (pts, np.zeros((0, 3), np.int32), 8, svo_mod.ERR_EMPTY),
+        (pts, np.array([[0, 1, 2]], np.int32), 1, svo_mod.ERR_DEGENERATE),
+        (pts, np.array([[0, 1, 3]], np.int32), 8, svo_mod.ERR_INVALID_ARGUMENT),
+        (pts, np.array([[0, 1, 2]], np.int32), 0, svo_mod.ERR_UNSUPPORTED),
+        (pts, np.array([[0, 1, 2]], np.int32), 4096, svo_mod.ERR_UNSUPPORTED),
+    ]
+    bad = pts.copy()
+    bad[1, 1] = np.nan
+    cases.append((bad, np.array([[0, 1, 2]], np.int32), 8, svo_mod.ERR_INVALID_ARGUMENT))
+    for p, f, res, code in cases:
+        with pytest.raises(svo_mod.SvoError) as e:
+            gpu_ctx.build(p, f, res)
+        assert e.value.code == code, (res, e.value)
+    # the context stays usable after errors
+    r = gpu_ctx.build(pts, np.array([[0, 1, 2]], np.int32), 8)
+    assert r.depth == 4

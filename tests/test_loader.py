@@ -1,0 +1,85 @@
+"""OBJ loading (src/BaseModel.cpp:3-25): the oracle's reading of the
+reference, and the product loader against the oracle."""
+import numpy as np
+import pytest
+
+
+def _write(tmp_path, name, text):
+    p = tmp_path / name
+    p.write_bytes(text.encode() if isinstance(text, str) else text)
+    return str(p)
+
+
+CASES = {
+    "plain": "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 0 0 1\nf 1 2 3\nf 1 3 4\n",
+    "double_slash": "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1//7 2//8 3//9\n",
+    "tex": "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1/5 2/6 3/7\n",
+    # a/t/n faces match none of the reference's patterns and are dropped
+    "tex_normal": "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1/1/1 2/2/2 3/3/3\nf 1 2 3\n",
+    # quads keep their first triangle
+    "quad": "v 0 0 0\nv 1 0 0\nv 0 1 0\nv 1 1 0\nf 1 2 4 3\n",
+    # vn / vt / comments / tabs after v are ignored
+    "other_lines": "# c\nvn 1 0 0\nvt 0 0\nv\t5 5 5\nv 0 0 0\nv 1 0 0\nv 0 1 0\n\nf 1 2 3\n",
+    # unterminated last line is dropped
+    "unterminated": "v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\nv 9 9 9",
+    "crlf": "v 0 0 0\r\nv 1 0 0\r\nv 0 1 0\r\nf 1 2 3\r\n",
+    "short_v": "v 1 2\nv 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 3\n",
+    "exp_floats": "v 1e-3 -2.5E+2 +7\nv 0.1 0.2 0.30000001\nv 3 nan 4\nf 1 2 3\n",
+    "spaces": "v   1   2   3\nv 0 0 0\nv 1 1 1\nf  1  2  3\n",
+    "line_254": "v 1 2 3" + " " * 247 + "\nv 0 0 0\nv 1 1 1\nf 1 2 3\n",
+}
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_oracle_loader_cases(tmp_path, oracle_mod, name):
+    path = _write(tmp_path, name + ".obj", CASES[name])
+    pts, tri = oracle_mod.load_obj(path)
+    if name == "tex_normal":
+        assert tri.tolist() == [[0, 1, 2]]
+    if name == "quad":
+        assert tri.tolist() == [[0, 1, 3]]
+    if name == "other_lines":
+        assert pts.shape == (3, 3) and tri.shape == (1, 3)
+    if name == "unterminated":
+        assert pts.shape == (3, 3) and tri.shape == (1, 3)
+    if name == "short_v":
+        assert pts.shape == (3, 3)
+    if name == "exp_floats":
+        assert pts[0].tolist() == [np.float32(1e-3), -250.0, 7.0]
+        assert np.isnan(pts[2, 1])
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_product_loader_matches_oracle(tmp_path, oracle_mod, svo_mod, name):
+    path = _write(tmp_path, name + ".obj", CASES[name])
+    p0, t0 = oracle_mod.load_obj(path)
+    p1, t1 = svo_mod.load_obj(path)
+    assert p0.tobytes() == p1.tobytes()
+    assert np.array_equal(t0, t1)
+
+
+@pytest.mark.parametrize("text,code", [
+    ("v 0 0 0\n" + "v " + "1 " * 130 + "\n", 7),          # 255+ characters: reference never returns
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 1 2 9\n", 7),           # index past the vertex list
+    ("v 0 0 0\nv 1 0 0\nv 0 1 0\nf 0 1 2\n", 7),           # index 0 -> -1
+])
+def test_loader_errors(tmp_path, oracle_mod, svo_mod, text, code):
+    path = _write(tmp_path, "bad.obj", text)
+    with pytest.raises(oracle_mod.OracleError) as e0:
+        oracle_mod.load_obj(path)
+    with pytest.raises(svo_mod.SvoError) as e1:
+        svo_mod.load_obj(path)
+    assert e0.value.code == code and e1.value.code == code
+
+
+def test_missing_file(oracle_mod, svo_mod, tmp_path):
+    with pytest.raises(svo_mod.SvoError) as e:
+        svo_mod.load_obj(str(tmp_path / "nope.obj"))
+    assert e.value.code == svo_mod.ERR_IO
+
+
+def test_bunny(bunny_path, oracle_mod, svo_mod):
+    p0, t0 = oracle_mod.load_obj(bunny_path)
+    p1, t1 = svo_mod.load_obj(bunny_path)
+    assert p0.shape == (14290, 3) and t0.shape == (28576, 3)
+    assert p0.tobytes() == p1.tobytes() and np.array_equal(t0, t1)
