@@ -1,0 +1,373 @@
+#!/usr/bin/env python3
+"""Benchmark of the octree build path: one step = one full SVO build
+(voxelize -> octree levels -> node records + vertex/edge arrays, bit-exact
+with the reference's semantics) of a seeded synthetic mesh.
+
+Default workload: 1,000,000-triangle torus + sliver soup at resolution 512
+(svo_b200.meshgen.torus_slivers).  `value` is whole-job triangles/s with the
+mesh already resident in HBM; `e2e` is the same metric through the C ABI with
+pinned host buffers (host->device copy of the mesh and device->host copy of
+the whole octree -- nodes, vertices, edges, keys -- inside the timed region).
+
+  python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
+
+Multi-GPU (torchrun): replicas only -- every rank builds the same workload
+independently (one build does not shard), no collective on the data path;
+value = triangles of all ranks / max over ranks of the device time.
+
+--impl reference times the CPU restatement of the reference's build
+(oracle/, all host threads) on a bounded sample of the same workload.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "gpu-svo_b200"))
+
+PEAKS_PATH = os.path.join(ROOT, "MEASURED_PEAKS.json")
+FALLBACK_HBM_GBS = 6650.0
+L2_FLUSH_BYTES = 256 << 20
+# Algorithmic bytes of one node in the emission kernel: node record 168 B,
+# 8 vertices x 16 B, 12 edges x 28 B written; one 8-byte group code read per
+# 8 sibling nodes.
+EMIT_BYTES_PER_NODE = 168 + 8 * 16 + 12 * 28 + 1
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5"], default="torus_slivers")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    return ap.parse_args()
+
+
+def workload(name: str):
+    from svo_b200 import meshgen
+
+    if name == "torus_slivers":
+        pts, tris, res = meshgen.torus_slivers()
+        return pts, tris, res, "torus_slivers_1M_res512"
+    pts, tris, res = meshgen.icosphere_l5()
+    return pts, tris, res, "icosphere_l5_res128"
+
+
+def n_triangles(pts, tris) -> int:
+    return pts.shape[0] // 3 if tris is None else tris.shape[0]
+
+
+# ---------------------------------------------------------------------------
+# distributed plumbing (replicas)
+# ---------------------------------------------------------------------------
+def dist_setup(n_gpus: int):
+    import torch
+    import torch.distributed as dist
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world > 1 and not dist.is_initialized():
+        import datetime
+
+        backend = "nccl" if torch.cuda.is_available() else "gloo"
+        if backend == "nccl":
+            torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group(backend, timeout=datetime.timedelta(seconds=120))
+    rank = dist.get_rank() if dist.is_initialized() else 0
+    return rank, world
+
+
+def dist_max(x: float) -> float:
+    import torch
+    import torch.distributed as dist
+
+    if not dist.is_initialized():
+        return x
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def dist_barrier() -> None:
+    import torch.distributed as dist
+
+    if dist.is_initialized():
+        dist.barrier()
+
+
+def dist_done() -> None:
+    import torch.distributed as dist
+
+    if dist.is_initialized():
+        dist.destroy_process_group()
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.dev = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self) -> dict:
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower() == "active":
+                    reasons.add(n)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU legs (the oracle: CPU restatement of the reference's build)
+# ---------------------------------------------------------------------------
+def cpu_sample(pts, tris, stride: int):
+    """Every stride-th triangle of the workload (a bounded sample)."""
+    if tris is None:
+        soup = pts.reshape(-1, 3, 3)[::stride].reshape(-1, 3)
+        return soup, np.arange(soup.shape[0], dtype=np.int32).reshape(-1, 3)
+    return pts, tris[::stride]
+
+
+def time_cpu_build(pts, tris, res, threads: int) -> float:
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    oracle.build()
+    t = time.perf_counter()
+    r = oracle.build_svo(pts, tris, res, flags=0, threads=threads)
+    dt = time.perf_counter() - t
+    r.close()
+    return dt
+
+
+def run_reference(args, rank: int):
+    if rank != 0:
+        return
+    pts, tris, res, wname = workload(args.workload)
+    stride = 16 if args.workload == "torus_slivers" else 1
+    spts, stris = cpu_sample(pts, tris, stride)
+    nt = stris.shape[0]
+    threads = os.cpu_count() or 1
+    for _ in range(args.warmup):
+        time_cpu_build(spts, stris, res, threads)
+    times = [time_cpu_build(spts, stris, res, threads) for _ in range(args.steps)]
+    total = sum(times)
+    value = nt * len(times) / total
+    sample = (f"every {stride}th triangle of {wname} ({nt} triangles), res {res}, full build "
+              f"(voxels, levels, nodes, vertex/edge arrays)")
+    line = {
+        "impl": "reference", "metric": "tris/s", "value": value, "unit": "tris/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": wname, "triangles": nt, "resolution": res},
+        "cpu_baseline": {"value": value, "unit": "tris/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "tris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": "the reference has no CPU build path and cannot be built here (Eigen 3.4 is fetched at "
+                "configure time); this times the CPU restatement of its algorithm (oracle/)",
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ---------------------------------------------------------------------------
+# our arm
+# ---------------------------------------------------------------------------
+def run_ours(args, rank: int, world: int):
+    import torch
+
+    import svo_b200 as S
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    sid = stream.cuda_stream
+    pts, tris, res, wname = workload(args.workload)
+    nt = n_triangles(pts, tris)
+    ctx = S.Context(dev)
+    d_pts = torch.from_numpy(pts).cuda()
+    d_tris = torch.from_numpy(tris).cuda() if tris is not None else None
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+
+    def step(flags=0):
+        flush.fill_(1)  # L2 flush before each step, outside the timed span
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        r = ctx.build(d_pts, d_tris, res, flags, sid)
+        e1.record(stream)
+        e1.synchronize()
+        ms = e0.elapsed_time(e1)
+        return ms, r
+
+    for _ in range(args.warmup):
+        _, r = step()
+        r.close()
+    dist_barrier()
+    torch.cuda.synchronize()
+    launches0 = S.kernel_launches()
+    step_ms = []
+    info = {}
+    with ClockSampler(dev) as clocks:
+        for _ in range(args.steps):
+            ms, r = step()
+            step_ms.append(ms)
+            info = {"nodes": r.num_nodes, "vertices": r.num_vertices, "edges": r.num_edges, "keys": r.num_keys,
+                    "depth": r.depth}
+            r.close()
+    torch.cuda.synchronize()
+    launches = S.kernel_launches() - launches0
+    dist_barrier()
+    total_ms = dist_max(sum(step_ms))
+    value = world * nt * args.steps / (total_ms / 1e3)
+    nodes_per_s = world * info["nodes"] * args.steps / (total_ms / 1e3)
+
+    # per-stage device times (separate steps, with events inside the library)
+    stage = {}
+    for _ in range(3):
+        _, r = step(S.FLAG_TIMINGS)
+        for k, v in r.timings().items():
+            stage.setdefault(k, []).append(v)
+        r.close()
+    stage = {k: statistics.median(v) for k, v in stage.items()}
+    emit_ms = stage.get("emit", 0.0)
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    emit_bytes = EMIT_BYTES_PER_NODE * info["nodes"]
+    achieved = emit_bytes / (emit_ms / 1e3) / 1e9 if emit_ms > 0 else None
+    traffic = None
+    tpath = os.path.join(ROOT, "profiles", "emit_traffic_per_node.json")
+    if os.path.exists(tpath):
+        traffic = json.load(open(tpath))["dram_bytes_per_node"] * info["nodes"]
+    roofline = {
+        "kernel": "k_emit (node records + vertex/edge arrays)",
+        "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+        "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+        "peak_source": "measured" if peaks else "fallback",
+        "algorithmic_bytes": emit_bytes, "launch_ms": emit_ms,
+        "stage_ms": stage,
+        "build_bytes_alg": 36 * nt + 8 * info["keys"] + EMIT_BYTES_PER_NODE * info["nodes"],
+    }
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        h_pts = torch.from_numpy(pts).pin_memory()
+        h_tris = torch.from_numpy(tris).pin_memory() if tris is not None else None
+        nb = [info["nodes"] * 168, info["vertices"] * 16, info["edges"] * 28, info["keys"] * 8]
+        out = [torch.empty(max(b, 1), dtype=torch.uint8).pin_memory() for b in nb]
+        lib = S.lib()
+
+        def e2e_step():
+            flush.fill_(1)
+            torch.cuda.synchronize()
+            t = time.perf_counter()
+            r = ctx.build(h_pts.numpy(), None if h_tris is None else h_tris.numpy(), res, 0, sid)
+            for fn, buf, n in ((lib.svo_result_copy_nodes, out[0], info["nodes"]),
+                               (lib.svo_result_copy_vertices, out[1], info["vertices"]),
+                               (lib.svo_result_copy_edges, out[2], info["edges"]),
+                               (lib.svo_result_copy_keys, out[3], info["keys"])):
+                S._check(fn(r.handle, buf.data_ptr(), n))
+            dt = time.perf_counter() - t
+            r.close()
+            return dt
+
+        e2e_step()
+        dist_barrier()
+        ts = [e2e_step() for _ in range(max(2, min(args.steps, 5)))]
+        tmax = dist_max(sum(ts))
+        e2e = {"value": world * nt * len(ts) / tmax, "unit": "tris/s",
+               "h2d_bytes_per_step": int(h_pts.numel() * 4 + (0 if h_tris is None else h_tris.numel() * 4)),
+               "d2h_bytes_per_step": int(sum(nb)), "ms_per_step": 1e3 * tmax / len(ts),
+               "timer": "host wall clock around svo_build + svo_result_copy_* (synchronous calls)"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        stride = 16 if args.workload == "torus_slivers" else 1
+        spts, stris = cpu_sample(pts, tris, stride)
+        threads = os.cpu_count() or 1
+        dt = time_cpu_build(spts, stris, res, threads)
+        cpu = {"value": stris.shape[0] / dt, "unit": "tris/s", "cores": threads, "kind": "port",
+               "sample": f"every {stride}th triangle ({stris.shape[0]}), res {res}, one full oracle build"}
+
+    if rank == 0:
+        line = {
+            "metric": "tris/s", "value": value, "unit": "tris/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": dist_max(sum(step_ms)) / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": wname, "triangles": nt, "resolution": res, "parallelism": f"replicas{world}",
+                       "l2_flush": "256 MiB device write before every step, outside the timed span",
+                       **info},
+            "nodes_per_s": nodes_per_s,
+            "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
+def main():
+    args = parse_args()
+    rank, world = dist_setup(args.gpus)
+    try:
+        if args.impl == "reference":
+            run_reference(args, rank)
+        else:
+            run_ours(args, rank, world)
+    finally:
+        dist_done()
+
+
+if __name__ == "__main__":
+    main()

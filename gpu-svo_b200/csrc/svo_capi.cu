@@ -7,6 +7,7 @@
 // vertices and edges -> one small read of the duplicate counters.
 // The reference's equivalent (src/SVO.cu:341-735) synchronises with the host
 // at least six times per level and reallocates its node array per level.
+#include <atomic>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -40,6 +41,8 @@ struct svo_result {
     uint64_t *keys = nullptr;
     uint64_t n_dedup[3] = {0, 0, 0};
     uint64_t *dedup[3] = {nullptr, nullptr, nullptr};
+    int n_timings = 0;
+    float timings[9] = {};
 };
 
 namespace {
@@ -109,6 +112,46 @@ T *pool_alloc(cudaMemPool_t pool, cudaStream_t st, size_t count, cudaError_t &er
     return static_cast<T *>(p);
 }
 
+// CUDA events at stage boundaries (SVO_FLAG_TIMINGS).
+struct StageTimer {
+    enum { kStart, kBbox, kVox, kPyr, kScan, kCompact0, kCompact, kEmit, kUnique, kDedup, kN };
+    bool on = false;
+    cudaEvent_t ev[kN] = {};
+    bool rec[kN] = {};
+    explicit StageTimer(bool enable) : on(enable) {
+        if (!on) return;
+        for (auto &e : ev) cudaEventCreate(&e);
+    }
+    ~StageTimer() {
+        if (!on) return;
+        for (auto &e : ev) cudaEventDestroy(e);
+    }
+    void mark(int i, cudaStream_t st) {
+        if (!on) return;
+        cudaEventRecord(ev[i], st);
+        rec[i] = true;
+    }
+    float span(int a, int b) const {
+        float ms = 0.0f;
+        if (on && rec[a] && rec[b]) cudaEventElapsedTime(&ms, ev[a], ev[b]);
+        return ms;
+    }
+    void store(svo_result *r) const {
+        if (!on) return;
+        cudaEventSynchronize(ev[kDedup]);
+        r->n_timings = 9;
+        r->timings[0] = span(kStart, kDedup);
+        r->timings[1] = span(kStart, kBbox);
+        r->timings[2] = span(kBbox, kVox);
+        r->timings[3] = span(kVox, kPyr);
+        r->timings[4] = span(kPyr, kScan);
+        r->timings[5] = span(kCompact0, kCompact);
+        r->timings[6] = span(kCompact, kEmit);
+        r->timings[7] = span(kEmit, kUnique);
+        r->timings[8] = span(kUnique, kDedup);
+    }
+};
+
 // Device-side meta block read back by the host after the count phase.
 struct Meta {
     GridParams gp;
@@ -176,7 +219,10 @@ int build_one(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t
     SVO_TRY(cudaMemsetAsync(d_meta, 0, sizeof(Meta), st), "memset");
     SVO_TRY(cudaMemsetAsync(d_done, 0, 4, st), "memset");
     GridParams *d_gp = &d_meta->gp;
+    StageTimer tm((flags & SVO_FLAG_TIMINGS) != 0);
+    tm.mark(StageTimer::kStart, st);
     SVO_TRY(launch_bbox(d_pts, n_points, rx, ry, rz, d_mm, d_gp, st), "bbox");
+    tm.mark(StageTimer::kBbox, st);
     const bool strict = (flags & SVO_FLAG_STRICT_FP) != 0;
     Meta meta;
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -185,9 +231,12 @@ int build_one(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t
         SVO_TRY(launch_voxelize(d_pts, d_tris, nt, d_gp, rx, ry, rz, strict, reinterpret_cast<uint32_t *>(d_bits),
                                 ctx->tune, d_big, big_cap, d_meta->counters, ctx->num_sms, st),
                 "voxelize");
+        tm.mark(StageTimer::kVox, st);
         SVO_TRY(launch_pyramid(py, d_bits, d_cnt, d_done, st), "pyramid");
+        tm.mark(StageTimer::kPyr, st);
         SVO_TRY(launch_scan(d_cnt, d_pre, py.total_blocks, d_scan, &d_meta->gp.status, st), "scan");
         SVO_TRY(launch_level_totals(py, d_pre, d_meta->totals, st), "totals");
+        tm.mark(StageTimer::kScan, st);
         SVO_TRY(cudaMemcpyAsync(&meta, d_meta, sizeof(Meta), cudaMemcpyDeviceToHost, st), "read meta");
         SVO_TRY(cudaStreamSynchronize(st), "count phase");
         if (meta.counters[0] <= big_cap) break;
@@ -262,11 +311,13 @@ int build_one(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t
     auto check = [&](cudaError_t e, const char *what) {
         if (e != cudaSuccess && rc == SVO_OK) rc = cuda_fail(e, what);
     };
+    tm.mark(StageTimer::kCompact0, st);
     check(launch_compact(py, d_bits, d_pre, 1, T + 1, d_K, koff, st), "compact levels");
     if (want_keys) {
         uint64_t k0[kMaxLevels] = {};
         check(launch_compact(py, d_bits, d_pre, 0, 1, r->keys, k0, st), "compact keys");
     }
+    tm.mark(StageTimer::kCompact, st);
     EmitParams P{};
     P.T = T;
     P.N = (uint32_t)N;
@@ -294,6 +345,7 @@ int build_one(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t
     P.edges = ve ? r->edges : nullptr;
     P.dups = d_meta->dups;
     check(launch_emit(P, ctx->num_sms, st), "emit");
+    tm.mark(StageTimer::kEmit, st);
     check(cudaMemcpyAsync(&meta.top_code, d_K + koff[T], 8, cudaMemcpyDeviceToHost, st), "read top");
     check(cudaMemcpyAsync(meta.dups, d_meta->dups, 16, cudaMemcpyDeviceToHost, st), "read dups");
     check(cudaStreamSynchronize(st), "emit phase");
@@ -336,7 +388,10 @@ int build_one(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t
             }
         }
     }
+    tm.mark(StageTimer::kUnique, st);
     if (rc == SVO_OK && (flags & SVO_FLAG_DEDUP)) rc = build_dedup(ctx->pool, st, P, r->n_dedup, r->dedup, ctx->num_sms);
+    tm.mark(StageTimer::kDedup, st);
+    if (rc == SVO_OK) tm.store(r);
     S.release();
     if (rc != SVO_OK) {
         svo_result_free(r);
@@ -455,6 +510,12 @@ int svo_result_copy_edges(const svo_result *r, svo_edge *dst, int64_t cap) {
 int svo_result_copy_keys(const svo_result *r, uint64_t *dst, int64_t cap) {
     return copy_out(r, dst, r ? r->keys : nullptr, r ? r->n_keys : 0, cap, sizeof(uint64_t), "keys");
 }
+int svo_result_timings(const svo_result *r, float *ms, int cap) {
+    if (!r) return 0;
+    for (int i = 0; i < r->n_timings && i < cap; ++i) ms[i] = r->timings[i];
+    return r->n_timings;
+}
+
 int64_t svo_result_num_dedup(const svo_result *r, int kind) {
     return (r && kind >= 0 && kind < 3) ? (int64_t)r->n_dedup[kind] : -1;
 }
@@ -484,3 +545,10 @@ int svo_write_voxels(const svo_result *r, const char *path) {
 namespace svo::host {
 void set_error(const char *msg) { g_err = msg; }
 }  // namespace svo::host
+
+namespace svo {
+static std::atomic<int64_t> g_launches{0};
+void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+}  // namespace svo
+
+extern "C" int64_t svo_kernel_launches(void) { return svo::g_launches.load(std::memory_order_relaxed); }

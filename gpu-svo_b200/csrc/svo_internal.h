@@ -9,6 +9,9 @@
 
 namespace svo {
 
+// Counts kernel launches (svo_kernel_launches).
+void count_launches(int n);
+
 constexpr int kMaxLevels = 24;
 constexpr int kMaxRes = 2048;
 

@@ -638,9 +638,11 @@ cudaError_t unique_impl(const T *in, uint64_t n, T *out, uint32_t *tile_counts, 
     const uint64_t tiles = (n + kUniqueTile - 1) / kUniqueTile;
     if (tiles == 0) return cudaSuccess;
     k_unique_count<T><<<(unsigned)tiles, 256, 0, st>>>(in, n, tile_counts);
+    count_launches(1);
     cudaError_t e = launch_scan(tile_counts, tile_pre, tiles, scan_scratch, status, st);
     if (e != cudaSuccess) return e;
     k_unique_scatter<T><<<(unsigned)tiles, 256, 0, st>>>(in, n, tile_pre, out);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -648,6 +650,7 @@ cudaError_t unique_impl(const T *in, uint64_t n, T *out, uint32_t *tile_counts, 
 
 cudaError_t launch_pyramid(const Pyramid &py, uint64_t *bits, uint32_t *cnt, uint32_t *done, cudaStream_t st) {
     k_pyramid<<<py.ctas, 256, 0, st>>>(py, bits, cnt, done);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -660,11 +663,13 @@ cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned 
     if (e != cudaSuccess) return e;
     if (tiles == 0) return cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
     k_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, scratch, status);
+    count_launches(1);
     return cudaGetLastError();
 }
 
 cudaError_t launch_level_totals(const Pyramid &py, const uint32_t *pre, uint32_t *totals, cudaStream_t st) {
     k_level_totals<<<1, 32, 0, st>>>(py, pre, totals);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -675,6 +680,7 @@ cudaError_t launch_compact(const Pyramid &py, const uint64_t *bits, const uint32
     KOff k;
     for (int l = 0; l < kMaxLevels; ++l) k.v[l] = koff[l];
     k_compact<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(py, bits, pre, l0, l1, out, k);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -695,6 +701,7 @@ cudaError_t launch_emit(const EmitParams &p, int num_sms, cudaStream_t st) {
         else { if (ve) SVO_EMIT(false, false, true); else SVO_EMIT(false, false, false); }
     }
 #undef SVO_EMIT
+    count_launches(1);
     return cudaGetLastError();
 }
 

@@ -412,8 +412,10 @@ __global__ void k_index_range(const int32_t *__restrict__ idx, int64_t n, int32_
 
 cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaStream_t st) {
     k_index_init<<<1, 1, 0, st>>>(mm);
+    count_launches(1);
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8));
     k_index_range<<<blocks, 256, 0, st>>>(idx, n, mm);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -426,7 +428,9 @@ cudaError_t launch_bbox(const float *pts, int64_t n, int rx, int ry, int rz, uin
     int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
     blocks = std::max(blocks, 1);
     k_bbox_reduce<<<blocks, 256, 0, st>>>(pts, n, mm_scratch, gp);
+    count_launches(1);
     k_grid_setup<<<1, 32, 0, st>>>(mm_scratch, rx, ry, rz, gp);
+    count_launches(1);
     return cudaGetLastError();
 }
 
@@ -440,19 +444,19 @@ cudaError_t launch_voxelize(const float *pts, const int32_t *tris, int64_t nt, c
     if (nt > 0) {
         const int64_t want = (nt + 255) / 256;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * 16));
-        if (strict)
+        const int bblocks = num_sms * 2;
+        if (strict) {
             k_voxelize<true><<<blocks, 256, 0, st>>>(pts, tris, nt, gp, rx, ry, rz, bm, tune, big, big_cap,
                                                     counters);
-        else
-            k_voxelize<false><<<blocks, 256, 0, st>>>(pts, tris, nt, gp, rx, ry, rz, bm, tune, big, big_cap,
-                                                     counters);
-        const int bblocks = num_sms * 2;
-        if (strict)
             k_voxelize_big<true><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters,
                                                          big_cap, counters + 1);
-        else
+        } else {
+            k_voxelize<false><<<blocks, 256, 0, st>>>(pts, tris, nt, gp, rx, ry, rz, bm, tune, big, big_cap,
+                                                     counters);
             k_voxelize_big<false><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters,
                                                           big_cap, counters + 1);
+        }
+        count_launches(2);
     }
     return cudaGetLastError();
 }

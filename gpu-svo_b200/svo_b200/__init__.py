@@ -31,6 +31,8 @@ FLAG_DEDUP = 0x2
 FLAG_STRICT_FP = 0x4
 FLAG_NO_VERT_EDGE = 0x8
 FLAG_NO_KEYS = 0x10
+FLAG_TIMINGS = 0x20
+TIMING_STAGES = ("total", "bbox", "voxelize", "pyramid", "scan", "compact", "emit", "unique", "dedup")
 
 NODE_DTYPE = np.dtype(
     [
@@ -106,6 +108,8 @@ def lib() -> C.CDLL:
             f.restype = vp
             g = getattr(L, f"svo_result_copy_{name}")
             g.argtypes = [vp, vp, i64]
+        L.svo_result_timings.argtypes = [vp, vp, C.c_int]
+        L.svo_kernel_launches.restype = i64
         L.svo_result_num_dedup.argtypes = [vp, C.c_int]
         L.svo_result_num_dedup.restype = i64
         L.svo_result_copy_dedup.argtypes = [vp, C.c_int, vp, i64]
@@ -141,6 +145,11 @@ def bbox_cube(points: np.ndarray) -> np.ndarray:
     box = _Aabb()
     _check(lib().svo_bbox_cube(pts.ctypes.data, pts.shape[0], C.byref(box)))
     return np.array(list(box.min) + list(box.max) + list(box.width), dtype=np.float32)
+
+
+def kernel_launches() -> int:
+    """Kernels launched by the library in this process so far."""
+    return int(lib().svo_kernel_launches())
 
 
 def write_tree_nodes(nodes: np.ndarray, path: str) -> None:
@@ -294,6 +303,12 @@ class Result:
 
     def keys(self) -> np.ndarray:
         return self._copy("keys", self.num_keys, np.uint64)
+
+    def timings(self) -> dict:
+        """Per-stage device ms of a build made with FLAG_TIMINGS."""
+        ms = np.zeros(16, dtype=np.float32)
+        n = lib().svo_result_timings(self._h, ms.ctypes.data, 16)
+        return {TIMING_STAGES[i]: float(ms[i]) for i in range(n)}
 
     def dedup(self, kind: int) -> np.ndarray:
         n = lib().svo_result_num_dedup(self._h, kind)

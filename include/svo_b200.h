@@ -45,6 +45,7 @@ extern "C" {
 #define SVO_FLAG_STRICT_FP 0x4u      /* round every float op (no FMA contraction) */
 #define SVO_FLAG_NO_VERT_EDGE 0x8u   /* skip the per-node vertex/edge arrays */
 #define SVO_FLAG_NO_KEYS 0x10u       /* skip the sorted leaf-voxel key list */
+#define SVO_FLAG_TIMINGS 0x20u       /* record per-stage device times (svo_result_timings) */
 
 /* ---- records (byte layouts of the reference's types) --------------------- */
 /* SVONode, src/SVO.h:20-35 (168 bytes; pad_ is written as zero). */
@@ -92,6 +93,10 @@ void svo_ctx_destroy(svo_ctx *ctx);
 /* Thread-local message for the last non-zero status. */
 const char *svo_last_error(void);
 
+/* Process-wide number of CUDA kernels this library has launched (for
+ * accounting in benchmarks; no counterpart in the reference). */
+int64_t svo_kernel_launches(void);
+
 /* ---- mesh input ----------------------------------------------------------- */
 /* BaseModel::loadOBJ, src/BaseModel.cpp:3-25.  Same accepted lines and quirks
  * (only "v " / "f " lines; `a/t/n` faces dropped; unterminated last line
@@ -113,8 +118,10 @@ int svo_bbox_cube(const float *points, int64_t n_points, svo_aabb *out);
  * the mesh a SparseVoxelOctree(filename, res_x, res_y, res_z) would hold
  * (src/SVO.h:61-67): `points` are the model's vertices, `tris` its triangles
  * (zero-based).  tris == NULL means a triangle soup: n_points = 3 * triangles.
- * Resolutions up to 1024 reproduce the reference exactly; up to 4096 use
- * 64-bit Morton codes (the reference's 32-bit codes are wrong above 1024).
+ * Resolutions up to 1024 reproduce the reference exactly; 1025..2048 use
+ * 64-bit Morton codes (the reference's 32-bit codes are wrong above 1024;
+ * svo_node.morton_code then holds the low 32 bits, svo_result_copy_keys the
+ * full codes).
  * `stream` is a cudaStream_t (NULL = the legacy default stream).  On success
  * *out owns the device arrays of the octree. */
 int svo_build(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t *tris,
@@ -158,6 +165,15 @@ int svo_result_copy_nodes(const svo_result *r, svo_node *dst, int64_t cap);
 int svo_result_copy_vertices(const svo_result *r, svo_vertex *dst, int64_t cap);
 int svo_result_copy_edges(const svo_result *r, svo_edge *dst, int64_t cap);
 int svo_result_copy_keys(const svo_result *r, uint64_t *dst, int64_t cap);
+/* Per-stage device times in ms of a build made with SVO_FLAG_TIMINGS, from
+ * CUDA events on the build stream: [0] first to last event (includes the
+ * host round trip that sizes the outputs), [1] bounding cube, [2] voxelize,
+ * [3] bitmap pyramid, [4] block-count scan, [5] level code lists,
+ * [6] node/vertex/edge emission, [7] duplicate removal, [8] dedup keys.
+ * Returns the number of entries (9), or 0 without timings.  No counterpart in
+ * the reference (it has no instrumentation). */
+int svo_result_timings(const svo_result *r, float *ms, int cap);
+
 /* Morton-keyed unique primitives (SVO_FLAG_DEDUP): kind 0 vertices, 1 edges,
  * 2 faces.  Sorted u64 keys. */
 int64_t svo_result_num_dedup(const svo_result *r, int kind);

@@ -65,12 +65,15 @@ def test_anisotropic(gpu_ctx, oracle_mod):
 
 
 def test_soup_equals_indexed(gpu_ctx, oracle_mod):
-    v, f = random_mesh(6, 100)
+    from svo_b200 import meshgen
+
+    v, f = meshgen.jittered_icosphere(3, np.random.default_rng(6))
+    soup = v[f].reshape(-1, 3)
     a = gpu_ctx.build(v, f, 32)
-    b = gpu_ctx.build(v[f].reshape(-1, 3), None, 32)
-    o = oracle_mod.build_svo(v[f].reshape(-1, 3), np.arange(300, dtype=np.int32).reshape(-1, 3), 32)
+    b = gpu_ctx.build(soup, None, 32)
+    o = oracle_mod.build_svo(soup, np.arange(soup.shape[0], dtype=np.int32).reshape(-1, 3), 32)
     assert_same(b, o)
-    # the soup has the same vertices, so the same bbox and tree
+    # every vertex is referenced: same bbox, so the same tree as the indexed mesh
     assert a.nodes().tobytes() == b.nodes().tobytes()
 
 
