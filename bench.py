@@ -50,6 +50,7 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5"], default="torus_slivers")
+    ap.add_argument("--res", type=int, default=0, help="override the workload's resolution")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     return ap.parse_args()
@@ -234,6 +235,8 @@ def run_ours(args, rank: int, world: int):
     stream = torch.cuda.current_stream()
     sid = stream.cuda_stream
     pts, tris, res, wname = workload(args.workload)
+    if args.res:
+        res, wname = args.res, f"{wname.rsplit('_res', 1)[0]}_res{args.res}"
     nt = n_triangles(pts, tris)
     ctx = S.Context(dev)
     d_pts = torch.from_numpy(pts).cuda()
