@@ -236,6 +236,11 @@ int svo_bbox_cube(const float *pts, int64_t n, svo_aabb *out) {
     return SVO_OK;
 }
 
+int svo_write_voxel_keys(const uint64_t *keys, int64_t n, const float origin[3], float width, const char *path) {
+    if ((!keys && n > 0) || !origin || !path) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    return svo::host::write_voxels(keys, n, origin, width, path);
+}
+
 int svo_write_tree_nodes(const svo_node *nodes, int64_t n, const char *path) {
     if ((!nodes && n > 0) || !path) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
     return write_cubes(

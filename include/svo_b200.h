@@ -189,6 +189,10 @@ int svo_write_tree_nodes(const svo_node *nodes, int64_t n, const char *path);
 /* SparseVoxelOctree::writeVoxel, src/SVO.cu:755-777: one cube per surface
  * voxel, decoded from its key (the reference only calls it in NDEBUG builds). */
 int svo_write_voxels(const svo_result *r, const char *path);
+/* The same writer over host keys: cube i at origin + width * (x, y, z) of
+ * keys[i], computed on the host (src/SVO.cu:766-775). */
+int svo_write_voxel_keys(const uint64_t *keys, int64_t n, const float origin[3], float width,
+                         const char *path);
 
 #ifdef __cplusplus
 }
