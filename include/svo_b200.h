@@ -143,6 +143,25 @@ typedef struct svo_mesh_desc {
 int svo_build_batch(svo_ctx *ctx, const svo_mesh_desc *descs, int n, void *stream,
                     svo_result **out, int *status_out);
 
+/* Sorted surface-voxel Morton keys of a mesh (the first stage of svo_build:
+ * same bounding cube, same voxel test, same key list as svo_result_copy_keys)
+ * without allocating any device memory.  No counterpart in the reference.
+ * It exists for callers that cannot let a library call cudaMalloc or cudaFree
+ * -- applications that hand out all device memory from their own arena, or
+ * that must not have an allocation synchronise the device in the middle of
+ * their stream work.  Inputs (points, tris; tris == NULL means a soup) and the
+ * output `keys` (capacity keys_cap, count in *n_keys) are device memory the
+ * caller owns; the only other memory used is a fixed 3 MiB scratch array
+ * compiled into the library, which every GPU that loads the library holds
+ * until the process exits.  Resolutions above 256 on any axis are rejected
+ * with SVO_ERR_UNSUPPORTED (the scratch holds a 256^3 bitmap).  The first call
+ * on a device looks up the scratch array's device address (make it before any
+ * stream capture).  All calls share the one scratch array: calls whose work
+ * overlaps on the GPU race, so serialise them.  Synchronises `stream`. */
+int svo_voxelize_keys_noalloc(const float *points, int64_t n_points, const int32_t *tris,
+                              int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags,
+                              uint64_t *keys, int64_t keys_cap, int64_t *n_keys, void *stream);
+
 /* ---- results (SparseVoxelOctree's private members, src/SVO.h:41-51) ------- */
 void svo_result_free(svo_result *r);
 int svo_result_depth(const svo_result *r);                 /* treeDepth */
