@@ -430,6 +430,23 @@ int svo_ctx_create(int device, svo_ctx **out) {
 
 void svo_ctx_destroy(svo_ctx *ctx) { delete ctx; }
 
+int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t) {
+    if (!ctx || !t) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    if (t->warp_max == 0) return fail(SVO_ERR_INVALID_ARGUMENT, "warp_max must be positive");
+    ctx->tune.serial_max = t->serial_max;
+    ctx->tune.warp_max = t->warp_max;
+    ctx->tune.split = t->split;
+    return SVO_OK;
+}
+
+int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t) {
+    if (!ctx || !t) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    t->serial_max = ctx->tune.serial_max;
+    t->warp_max = ctx->tune.warp_max;
+    t->split = ctx->tune.split;
+    return SVO_OK;
+}
+
 int svo_build(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t *tris, int64_t n_tris,
               int res_x, int res_y, int res_z, uint32_t flags, void *stream, svo_result **out) {
     if (!ctx || !out) return fail(SVO_ERR_INVALID_ARGUMENT, "null context or output");

@@ -15,10 +15,11 @@ void count_launches(int n);
 constexpr int kMaxLevels = 24;
 constexpr int kMaxRes = 2048;
 
-// Voxelizer work-split thresholds (bbox volume in voxels).
+// Voxelizer work split.
 struct VoxTuning {
-    uint32_t serial_max = 64;    // tested by one thread
-    uint32_t warp_max = 8192;    // tested by one warp; larger -> CTA queue
+    uint32_t serial_max = 64;    // grid-bbox voxels tested by one thread, row by row
+    uint32_t warp_max = 256;     // 4x4x4 bricks per queue entry (one warp walks one entry)
+    uint32_t split = 0;          // cull 2x2x2 sub-bricks of surviving bricks too
 };
 
 // Occupancy bitmap pyramid: level 0 is the voxel grid (one bit per Morton

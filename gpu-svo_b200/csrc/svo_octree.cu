@@ -267,24 +267,27 @@ struct KOff {
     uint64_t v[kMaxLevels];
 };
 
+// One thread per 64-bit word of levels [l0, l1): its first rank is the
+// block prefix plus the popcounts of the preceding words of its block.
 __global__ void __launch_bounds__(256) k_compact(Pyramid py, const uint64_t *__restrict__ bits,
                                                  const uint32_t *__restrict__ pre, int l0, int l1,
                                                  uint64_t *__restrict__ out, KOff koff) {
-    const uint64_t g = py.coff[l0] + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (g >= py.coff[l1]) return;
+    const uint64_t gw = py.woff[l0] + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (gw >= py.woff[l1 - 1] + py.words[l1 - 1]) return;
     int l = l0;
-    while (g >= py.coff[l + 1]) ++l;
-    const uint64_t blk = g - py.coff[l];
-    uint64_t r = pre[g] - pre[py.coff[l]];
-    const uint64_t *w = bits + py.woff[l] + blk * 8;
-    uint64_t *o = out + koff.v[l];
-#pragma unroll 1
-    for (int k = 0; k < 8; ++k) {
-        uint64_t v = w[k];
-        while (v) {
-            o[r++] = blk * 512 + k * 64 + __ffsll((long long)v) - 1;
-            v &= v - 1;
-        }
+    while (l + 1 < l1 && gw >= py.woff[l + 1]) ++l;
+    uint64_t v = bits[gw];
+    if (!v) return;
+    const uint64_t w = gw - py.woff[l];
+    const uint64_t blk = w >> 3;
+    uint64_t r = pre[py.coff[l] + blk] - pre[py.coff[l]];
+    const uint64_t *bw = bits + py.woff[l] + blk * 8;
+    for (int k = 0; k < (int)(w & 7); ++k) r += __popcll(bw[k]);
+    uint64_t *o = out + koff.v[l] + r;
+    const uint64_t base = w * 64;
+    while (v) {
+        *o++ = base + __ffsll((long long)v) - 1;
+        v &= v - 1;
     }
 }
 
@@ -675,11 +678,11 @@ cudaError_t launch_level_totals(const Pyramid &py, const uint32_t *pre, uint32_t
 
 cudaError_t launch_compact(const Pyramid &py, const uint64_t *bits, const uint32_t *pre, int l0, int l1,
                            uint64_t *out, const uint64_t *koff, cudaStream_t st) {
-    const uint64_t nb = py.coff[l1] - py.coff[l0];
-    if (nb == 0) return cudaSuccess;
+    const uint64_t nw = py.woff[l1 - 1] + py.words[l1 - 1] - py.woff[l0];
+    if (nw == 0) return cudaSuccess;
     KOff k;
     for (int l = 0; l < kMaxLevels; ++l) k.v[l] = koff[l];
-    k_compact<<<(unsigned)((nb + 255) / 256), 256, 0, st>>>(py, bits, pre, l0, l1, out, k);
+    k_compact<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(py, bits, pre, l0, l1, out, k);
     count_launches(1);
     return cudaGetLastError();
 }

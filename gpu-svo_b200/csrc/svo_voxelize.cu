@@ -7,17 +7,28 @@
 // arithmetic is the reference's, operation for operation (svo_device.cuh Fp).
 //
 // Work split: a triangle whose grid bbox has at most `serial_max` voxels is
-// tested by its own thread; up to `warp_max` voxels by its warp (row segments
-// spread over the lanes); larger ones are cut into entries of at most
-// kEntryItems row segments that whole CTAs take from a queue.
+// tested by its own thread, row by row.  Larger ones go to a queue of entries
+// (triangle, at most `warp_max` 4x4x4 bricks aligned to the grid) that
+// warps take one at a time; a brick is 64 consecutive Morton codes, two
+// bitmap words.  Without a queue (the allocation-free entry point) the
+// triangle's own warp walks its bricks in place.
+//
+// Brick culling is exact.  Every predicate of the voxel test is monotone in
+// each grid coordinate separately (each is built from rounded products,
+// sums and fmas of p = coordinate * unit, and IEEE rounding is monotone), so
+// over a brick an edge test is largest at the corner picked by the signs of
+// its two coefficients, and n.p is smallest/largest at the corners picked by
+// the signs of n.  A brick is skipped only when one predicate, evaluated at
+// its best corner with the voxel test's own arithmetic, already fails; every
+// other brick is split and tested again, and the voxels of surviving
+// sub-bricks are tested one per lane.  Triangles with any non-finite setup
+// value are never culled.
 #include "svo_internal.h"
 
 namespace svo {
 
 namespace {
 
-constexpr int kSeg = 16;            // voxels per row segment (one work item)
-constexpr uint32_t kEntryItems = 2048;  // row segments per big-triangle entry
 
 __device__ __forceinline__ uint32_t f2ord(float f) {
     uint32_t b = __float_as_uint(f);
@@ -31,21 +42,37 @@ __device__ __forceinline__ float ord2f(uint32_t o) {
 // Bounding box of all vertices (exact min/max through an order-preserving
 // integer map), then the bounding cube on one thread.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ void bbox_take(float v, int a, uint32_t lo[3], uint32_t hi[3], bool &bad) {
+    bad |= !isfinite(v);
+    const uint32_t o = f2ord(v);
+    lo[a] = min(lo[a], o);
+    hi[a] = max(hi[a], o);
+}
+
+// When pts is 16-byte aligned, 4 points (12 floats, 3 float4) per step; the
+// component of float k is k % 3, the same in every 12-float group.
 __global__ void k_bbox_reduce(const float *__restrict__ pts, int64_t n, uint32_t *__restrict__ mm,
                               GridParams *__restrict__ gp) {
     uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
     bool bad = false;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-         i += (int64_t)gridDim.x * blockDim.x) {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            float v = __ldg(pts + 3 * i + a);
-            bad |= !isfinite(v);
-            uint32_t o = f2ord(v);
-            lo[a] = min(lo[a], o);
-            hi[a] = max(hi[a], o);
+    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    int64_t done = 0;
+    if ((reinterpret_cast<uintptr_t>(pts) & 15) == 0) {
+        const float4 *p4 = reinterpret_cast<const float4 *>(pts);
+        const int64_t groups = n / 4;
+        for (int64_t gi = tid; gi < groups; gi += nth) {
+            const float4 a = __ldcs(p4 + 3 * gi), b = __ldcs(p4 + 3 * gi + 1), c = __ldcs(p4 + 3 * gi + 2);
+            bbox_take(a.x, 0, lo, hi, bad); bbox_take(a.y, 1, lo, hi, bad); bbox_take(a.z, 2, lo, hi, bad);
+            bbox_take(a.w, 0, lo, hi, bad); bbox_take(b.x, 1, lo, hi, bad); bbox_take(b.y, 2, lo, hi, bad);
+            bbox_take(b.z, 0, lo, hi, bad); bbox_take(b.w, 1, lo, hi, bad); bbox_take(c.x, 2, lo, hi, bad);
+            bbox_take(c.y, 0, lo, hi, bad); bbox_take(c.z, 1, lo, hi, bad); bbox_take(c.w, 2, lo, hi, bad);
         }
+        done = groups * 4;
     }
+    for (int64_t i = done + tid; i < n; i += nth)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) bbox_take(__ldg(pts + 3 * i + a), a, lo, hi, bad);
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         lo[a] = __reduce_min_sync(0xFFFFFFFFu, lo[a]);
@@ -104,6 +131,7 @@ struct Tri {
     float d1, d2;
     float ea[9], eb[9], ed[9];  // edge test k of plane p at 3p+k: XY, YZ, ZX
     int lo[3], hi[3];
+    int cull;                   // all setup values finite: brick culling allowed
 };
 
 __device__ __forceinline__ int f2i_rz(float f) { return __float2int_rz(f); }
@@ -178,6 +206,11 @@ __device__ __forceinline__ void tri_setup(const GridParams &g, const int res[3],
                                         cmaxf(0.0f, __fmul_rn(u[j], a1)));
         }
     }
+    bool fin = isfinite(t.n[0]) && isfinite(t.n[1]) && isfinite(t.n[2]) && isfinite(t.d1) && isfinite(t.d2) &&
+               isfinite(u[0]) && isfinite(u[1]) && isfinite(u[2]);
+#pragma unroll
+    for (int k = 0; k < 9; ++k) fin = fin && isfinite(t.ea[k]) && isfinite(t.eb[k]) && isfinite(t.ed[k]);
+    t.cull = fin ? 1 : 0;
 }
 
 // Per-row state: everything of the voxel test that depends only on (y, z).
@@ -209,19 +242,16 @@ template <bool S>
 __device__ __forceinline__ bool voxel_test(const Tri &t, const GridParams &g, const Row &r, int x) {
     const float px = __fmul_rn((float)x, g.unit[0]);
     const float nd = Fp<S>::dot3_head(t.n[0], px, r.inner);
-    if (__fmul_rn(__fadd_rn(nd, t.d1), __fadd_rn(nd, t.d2)) > 0.0f) return false;
+    bool ok = !(__fmul_rn(__fadd_rn(nd, t.d1), __fadd_rn(nd, t.d2)) > 0.0f);
 #pragma unroll
     for (int k = 0; k < 3; ++k) {
         const float f = S ? __fadd_rn(__fmul_rn(t.ea[k], px), r.xyb[k]) : __fmaf_rn(t.ea[k], px, r.xyb[k]);
-        if (__fadd_rn(f, t.ed[k]) < 0.0f) return false;
-    }
-#pragma unroll
-    for (int k = 0; k < 3; ++k) {
+        ok &= !(__fadd_rn(f, t.ed[k]) < 0.0f);
         const float q = __fmul_rn(t.eb[6 + k], px);
-        const float f = S ? __fadd_rn(r.zxp[k], q) : __fmaf_rn(t.ea[6 + k], r.zxp[k], q);
-        if (__fadd_rn(f, t.ed[6 + k]) < 0.0f) return false;
+        const float h = S ? __fadd_rn(r.zxp[k], q) : __fmaf_rn(t.ea[6 + k], r.zxp[k], q);
+        ok &= !(__fadd_rn(h, t.ed[6 + k]) < 0.0f);
     }
-    return true;
+    return ok;
 }
 
 // OR-accumulates hits of consecutive voxels that share a bitmap word.
@@ -255,15 +285,157 @@ __device__ __forceinline__ void row_segment(const Tri &t, const GridParams &g, i
         if (voxel_test<S>(t, g, r, x)) sink.add(spread3((uint32_t)x) | r.syz);
 }
 
-// Work item i of a triangle: row segment (y, z, x0..x1).
-__device__ __forceinline__ void item_coords(const Tri &t, uint32_t segs, uint32_t ny, uint32_t i, int &y,
-                                            int &z, int &x0, int &x1) {
-    const uint32_t row = i / segs, s = i - row * segs;
-    const uint32_t zr = row / ny;
-    y = t.lo[1] + (int)(row - zr * ny);
-    z = t.lo[2] + (int)zr;
-    x0 = t.lo[0] + (int)s * kSeg;
-    x1 = min(x0 + kSeg - 1, t.hi[0]);
+// The full voxel test at one voxel (the same arithmetic as row_prep +
+// voxel_test, src/SVO.cu:156-177), without early exits.
+template <bool S>
+__device__ __forceinline__ bool voxel_pass(const Tri &t, const GridParams &g, int x, int y, int z) {
+    const float px = __fmul_rn((float)x, g.unit[0]);
+    const float py = __fmul_rn((float)y, g.unit[1]);
+    const float pz = __fmul_rn((float)z, g.unit[2]);
+    const float nd = Fp<S>::dot3_head(t.n[0], px, Fp<S>::dot3_tail(t.n[1], t.n[2], py, pz));
+    bool ok = !(__fmul_rn(__fadd_rn(nd, t.d1), __fadd_rn(nd, t.d2)) > 0.0f);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        ok &= !(__fadd_rn(Fp<S>::dot2(t.ea[k], t.eb[k], px, py), t.ed[k]) < 0.0f);
+        ok &= !(__fadd_rn(Fp<S>::dot2(t.ea[3 + k], t.eb[3 + k], py, pz), t.ed[3 + k]) < 0.0f);
+        ok &= !(__fadd_rn(Fp<S>::dot2(t.ea[6 + k], t.eb[6 + k], pz, px), t.ed[6 + k]) < 0.0f);
+    }
+    return ok;
+}
+
+// True when no voxel of the box lo..hi (inclusive) can pass: one predicate
+// fails at its most favourable corner (see the comment at the top).
+template <bool S>
+__device__ __forceinline__ bool brick_reject(const Tri &t, const GridParams &g, const int lo[3], const int hi[3]) {
+    float pl[3], ph[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        pl[a] = __fmul_rn((float)lo[a], g.unit[a]);
+        ph[a] = __fmul_rn((float)hi[a], g.unit[a]);
+    }
+#pragma unroll
+    for (int p = 0; p < 3; ++p) {
+        const int i = p == 0 ? 0 : (p == 1 ? 1 : 2);
+        const int j = p == 0 ? 1 : (p == 1 ? 2 : 0);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            const float a = t.ea[3 * p + k], b = t.eb[3 * p + k];
+            const float pi = a >= 0.0f ? ph[i] : pl[i];
+            const float pj = b >= 0.0f ? ph[j] : pl[j];
+            if (__fadd_rn(Fp<S>::dot2(a, b, pi, pj), t.ed[3 * p + k]) < 0.0f) return true;
+        }
+    }
+    // n.p at its smallest and largest corners
+    const float x0 = t.n[0] >= 0.0f ? pl[0] : ph[0], x1 = t.n[0] >= 0.0f ? ph[0] : pl[0];
+    const float y0 = t.n[1] >= 0.0f ? pl[1] : ph[1], y1 = t.n[1] >= 0.0f ? ph[1] : pl[1];
+    const float z0 = t.n[2] >= 0.0f ? pl[2] : ph[2], z1 = t.n[2] >= 0.0f ? ph[2] : pl[2];
+    const float nd0 = Fp<S>::dot3_head(t.n[0], x0, Fp<S>::dot3_tail(t.n[1], t.n[2], y0, z0));
+    const float nd1 = Fp<S>::dot3_head(t.n[0], x1, Fp<S>::dot3_tail(t.n[1], t.n[2], y1, z1));
+    const float dlo = t.d1 <= t.d2 ? t.d1 : t.d2, dhi = t.d1 <= t.d2 ? t.d2 : t.d1;
+    {  // everything above the slab: both factors positive from the smallest n.p on
+        const float sa = __fadd_rn(nd0, dlo), sb = __fadd_rn(nd0, dhi);
+        if (sa > 0.0f && __fmul_rn(sa, sb) > 0.0f) return true;
+    }
+    {  // everything below: both factors negative up to the largest n.p
+        const float sa = __fadd_rn(nd1, dlo), sb = __fadd_rn(nd1, dhi);
+        if (sb < 0.0f && __fmul_rn(sa, sb) > 0.0f) return true;
+    }
+    return false;
+}
+
+// Bricks [b0, b1) of triangle t (the same t in every lane), chunks of 32
+// bricks taken with stride `step` starting at b0 + first.  Three rounds, each
+// with one item per lane: 32 bricks (4^3); the 8 sub-bricks (2^3) of 4
+// surviving bricks; the 8 voxels of 4 surviving sub-bricks.  A 2^3 sub-brick
+// is 8 consecutive Morton codes, one byte of a bitmap word.
+template <bool S>
+__device__ __forceinline__ void warp_bricks(const Tri &t, const GridParams &g, uint32_t *__restrict__ bm,
+                                            uint32_t b0, uint32_t b1, uint32_t first, uint32_t step,
+                                            bool split) {
+    const int lane = threadIdx.x & 31, grp = lane >> 3, sub = lane & 7;
+    const int bx0 = t.lo[0] >> 2, by0 = t.lo[1] >> 2, bz0 = t.lo[2] >> 2;
+    const uint32_t nbx = (uint32_t)((t.hi[0] >> 2) - bx0 + 1), nby = (uint32_t)((t.hi[1] >> 2) - by0 + 1);
+    for (uint32_t c = b0 + first; c < b1; c += step) {
+        const uint32_t j = c + lane;
+        bool live = false;
+        int bx = 0, by = 0, bz = 0;
+        if (j < b1) {
+            const uint32_t jy = j / nbx, jz = jy / nby;
+            bx = bx0 + (int)(j - jy * nbx);
+            by = by0 + (int)(jy - jz * nby);
+            bz = bz0 + (int)jz;
+            int lo[3] = {max(4 * bx, t.lo[0]), max(4 * by, t.lo[1]), max(4 * bz, t.lo[2])};
+            int hi[3] = {min(4 * bx + 3, t.hi[0]), min(4 * by + 3, t.hi[1]), min(4 * bz + 3, t.hi[2])};
+            live = !t.cull || !brick_reject<S>(t, g, lo, hi);
+        }
+        uint32_t m = __ballot_sync(0xFFFFFFFFu, live);
+        while (m && !split) {
+            // one surviving brick at a time, 2 voxels per lane, one ballot per bitmap word
+            const int src = __ffs(m) - 1;
+            m &= m - 1;
+            const int sx = __shfl_sync(0xFFFFFFFFu, bx, src), sy = __shfl_sync(0xFFFFFFFFu, by, src),
+                      sz = __shfl_sync(0xFFFFFFFFu, bz, src);
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int lm = lane + 32 * h;  // local Morton index in the brick
+                const int x = 4 * sx + ((lm & 1) | ((lm >> 2) & 2));
+                const int y = 4 * sy + (((lm >> 1) & 1) | ((lm >> 3) & 2));
+                const int z = 4 * sz + (((lm >> 2) & 1) | ((lm >> 4) & 2));
+                const bool in = x >= t.lo[0] && x <= t.hi[0] && y >= t.lo[1] && y <= t.hi[1] && z >= t.lo[2] &&
+                                z <= t.hi[2];
+                const uint32_t w = __ballot_sync(0xFFFFFFFFu, in && voxel_pass<S>(t, g, x, y, z));
+                if (lane == h && w) atomicOr(bm + ((morton3((uint32_t)sx, (uint32_t)sy, (uint32_t)sz) << 1) | h), w);
+            }
+        }
+        while (m) {
+            // up to 4 surviving bricks: lane = (brick, sub-brick)
+            int src = 0;
+            const int nsv = min(4, __popc(m));
+            for (int i = 0; i < nsv; ++i) {
+                const int s_ = __ffs(m) - 1;
+                m &= m - 1;
+                if (i == grp) src = s_;
+            }
+            const int sx = __shfl_sync(0xFFFFFFFFu, bx, src), sy = __shfl_sync(0xFFFFFFFFu, by, src),
+                      sz = __shfl_sync(0xFFFFFFFFu, bz, src);
+            const int x2 = 4 * sx + 2 * (sub & 1), y2 = 4 * sy + ((sub >> 1) & 1) * 2, z2 = 4 * sz + ((sub >> 2) & 1) * 2;
+            bool slive = false;
+            if (grp < nsv) {
+                int lo[3] = {max(x2, t.lo[0]), max(y2, t.lo[1]), max(z2, t.lo[2])};
+                int hi[3] = {min(x2 + 1, t.hi[0]), min(y2 + 1, t.hi[1]), min(z2 + 1, t.hi[2])};
+                slive = lo[0] <= hi[0] && lo[1] <= hi[1] && lo[2] <= hi[2] && (!t.cull || !brick_reject<S>(t, g, lo, hi));
+            }
+            uint32_t m2 = __ballot_sync(0xFFFFFFFFu, slive);
+            while (m2) {
+                // up to 4 surviving sub-bricks: lane = (sub-brick, voxel)
+                int src2 = 0;
+                const int n2 = min(4, __popc(m2));
+                for (int i = 0; i < n2; ++i) {
+                    const int s_ = __ffs(m2) - 1;
+                    m2 &= m2 - 1;
+                    if (i == grp) src2 = s_;
+                }
+                const int vx = __shfl_sync(0xFFFFFFFFu, x2, src2), vy = __shfl_sync(0xFFFFFFFFu, y2, src2),
+                          vz = __shfl_sync(0xFFFFFFFFu, z2, src2);
+                const int x = vx + (sub & 1), y = vy + ((sub >> 1) & 1), z = vz + ((sub >> 2) & 1);
+                const bool in = grp < n2 && x >= t.lo[0] && x <= t.hi[0] && y >= t.lo[1] && y <= t.hi[1] &&
+                                z >= t.lo[2] && z <= t.hi[2];
+                const uint32_t w = __ballot_sync(0xFFFFFFFFu, in && voxel_pass<S>(t, g, x, y, z));
+                if (sub == 0 && grp < n2) {
+                    const uint32_t bits = (w >> (8 * grp)) & 0xFFu;
+                    if (bits) {
+                        const uint64_t code = morton3((uint32_t)vx, (uint32_t)vy, (uint32_t)vz);
+                        atomicOr(bm + (code >> 5), bits << (code & 31));
+                    }
+                }
+            }
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t brick_count(const Tri &t) {
+    return (uint32_t)((t.hi[0] >> 2) - (t.lo[0] >> 2) + 1) * (uint32_t)((t.hi[1] >> 2) - (t.lo[1] >> 2) + 1) *
+           (uint32_t)((t.hi[2] >> 2) - (t.lo[2] >> 2) + 1);
 }
 
 __device__ __forceinline__ void load_tri(const float *__restrict__ pts, const int32_t *__restrict__ tris,
@@ -290,13 +462,16 @@ __device__ __forceinline__ void shfl_tri(Tri &dst, const Tri &src, int lane) {
     for (int i = 0; i < (int)(sizeof(Tri) / 4); ++i) d[i] = __shfl_sync(0xFFFFFFFFu, s[i], lane);
 }
 
-template <bool S>
-__global__ void __launch_bounds__(256) k_voxelize(const float *__restrict__ pts,
-                                                  const int32_t *__restrict__ tris, int64_t nt,
-                                                  const GridParams *__restrict__ gpp, int rx, int ry,
-                                                  int rz, uint32_t *__restrict__ bm, VoxTuning tune,
-                                                  uint4 *__restrict__ big, uint32_t big_cap,
-                                                  uint32_t *__restrict__ big_count) {
+// One thread per triangle: setup, then either its own serial test
+// (grid bbox <= serial_max voxels) or queue entries of <= warp_max bricks.  INPLACE (no queue given): the triangle's warp walks its bricks
+// right here instead.
+template <bool S, bool INPLACE>
+__global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(const float *__restrict__ pts,
+                                                     const int32_t *__restrict__ tris, int64_t nt,
+                                                     const GridParams *__restrict__ gpp, int rx, int ry,
+                                                     int rz, uint32_t *__restrict__ bm, VoxTuning tune,
+                                                     uint4 *__restrict__ big, uint32_t big_cap,
+                                                     uint32_t *__restrict__ big_count) {
     const GridParams g = *gpp;
     const int res[3] = {rx, ry, rz};
     const int lane = threadIdx.x & 31;
@@ -306,85 +481,71 @@ __global__ void __launch_bounds__(256) k_voxelize(const float *__restrict__ pts,
     for (int64_t base = warp0; base < nt; base += stride) {
         const int64_t tid = base + lane;
         Tri t;
-        uint32_t items = 0;
-        uint64_t vol = 0;
+        uint32_t nb = 0;
         int tier = -1;
         if (tid < nt) {
             float p[3][3];
             load_tri(pts, tris, tid, p);
             tri_setup<S>(g, res, p[0], p[1], p[2], t);
-            const uint32_t nx = t.hi[0] - t.lo[0] + 1, ny = t.hi[1] - t.lo[1] + 1, nz = t.hi[2] - t.lo[2] + 1;
-            vol = (uint64_t)nx * ny * nz;
-            items = ((nx + kSeg - 1) / kSeg) * ny * nz;
-            tier = vol <= (uint64_t)tune.serial_max ? 0 : (vol <= (uint64_t)tune.warp_max ? 1 : 2);
+            const uint64_t vol = (uint64_t)(t.hi[0] - t.lo[0] + 1) * (uint64_t)(t.hi[1] - t.lo[1] + 1) *
+                                 (uint64_t)(t.hi[2] - t.lo[2] + 1);
+            nb = brick_count(t);
+            tier = vol <= (uint64_t)tune.serial_max ? 0 : 1;
         }
         if (tier == 0) {
             for (int z = t.lo[2]; z <= t.hi[2]; ++z)
                 for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
             sink.flush();
-        } else if (tier == 2) {
-            const uint32_t ne = (items + kEntryItems - 1) / kEntryItems;
+        } else if (!INPLACE && tier == 1) {
+            const uint32_t eb = tune.warp_max;
+            const uint32_t ne = (nb + eb - 1) / eb;
             const uint32_t at = atomicAdd(big_count, ne);
             if (at + ne <= big_cap) {
                 for (uint32_t e = 0; e < ne; ++e)
-                    big[at + e] = make_uint4((uint32_t)tid, e * kEntryItems, min(items, (e + 1) * kEntryItems), 0);
+                    big[at + e] = make_uint4((uint32_t)tid, e * eb, min(nb, (e + 1) * eb), 0);
             }
         }
-        // warp-cooperative triangles, one at a time
-        uint32_t coop = __ballot_sync(0xFFFFFFFFu, tier == 1);
-        while (coop) {
-            const int src = __ffs(coop) - 1;
-            coop &= coop - 1;
-            Tri w;
-            shfl_tri(w, t, src);
-            const uint32_t witems = __shfl_sync(0xFFFFFFFFu, items, src);
-            const uint32_t segs = (w.hi[0] - w.lo[0] + 1 + kSeg - 1) / kSeg;
-            const uint32_t wny = w.hi[1] - w.lo[1] + 1;
-            for (uint32_t i = lane; i < witems; i += 32) {
-                int y, z, x0, x1;
-                item_coords(w, segs, wny, i, y, z, x0, x1);
-                row_segment<S>(w, g, y, z, x0, x1, sink);
-                sink.flush();
+        if (INPLACE) {
+            uint32_t coop = __ballot_sync(0xFFFFFFFFu, tier == 1);
+            while (coop) {
+                const int src = __ffs(coop) - 1;
+                coop &= coop - 1;
+                Tri w;
+                shfl_tri(w, t, src);
+                const uint32_t wnb = __shfl_sync(0xFFFFFFFFu, nb, src);
+                warp_bricks<S>(w, g, bm, 0, wnb, 0, 32, tune.split != 0);
             }
         }
     }
 }
 
-// Big triangles: CTAs take entries (triangle, range of row segments) from a
-// queue and spread the segments over their threads.
+// Queued triangles: each warp takes an entry (triangle, brick range) and
+// walks its bricks.
 template <bool S>
-__global__ void __launch_bounds__(256) k_voxelize_big(const float *__restrict__ pts,
-                                                      const int32_t *__restrict__ tris,
-                                                      const GridParams *__restrict__ gpp, int rx,
-                                                      int ry, int rz, uint32_t *__restrict__ bm,
-                                                      const uint4 *__restrict__ big,
-                                                      const uint32_t *__restrict__ big_count,
-                                                      uint32_t big_cap, uint32_t *__restrict__ cursor) {
-    __shared__ uint32_t s_e;
+__global__ void __launch_bounds__(256, 4) k_voxelize_bricks(const float *__restrict__ pts,
+                                                            const int32_t *__restrict__ tris,
+                                                            const GridParams *__restrict__ gpp, int rx,
+                                                            int ry, int rz, uint32_t *__restrict__ bm,
+                                                            const uint4 *__restrict__ big,
+                                                            const uint32_t *__restrict__ big_count,
+                                                            uint32_t big_cap, uint32_t *__restrict__ cursor,
+                                                            bool split) {
     const GridParams g = *gpp;
     const int res[3] = {rx, ry, rz};
-    const uint32_t n = min(*big_count, big_cap);
-    if (*big_count > big_cap) return;  // reported by the host; the build is retried
-    HitSink sink{bm};
+    const int lane = threadIdx.x & 31;
+    const uint32_t n = *big_count;
+    if (n > big_cap) return;  // reported by the host; the build is retried
     for (;;) {
-        if (threadIdx.x == 0) s_e = atomicAdd(cursor, 1u);
-        __syncthreads();
-        const uint32_t e = s_e;
-        __syncthreads();
+        uint32_t e = 0;
+        if (lane == 0) e = atomicAdd(cursor, 1u);
+        e = __shfl_sync(0xFFFFFFFFu, e, 0);
         if (e >= n) return;
         const uint4 ent = big[e];
         float p[3][3];
         load_tri(pts, tris, ent.x, p);
         Tri t;
         tri_setup<S>(g, res, p[0], p[1], p[2], t);
-        const uint32_t segs = (t.hi[0] - t.lo[0] + 1 + kSeg - 1) / kSeg;
-        const uint32_t ny = t.hi[1] - t.lo[1] + 1;
-        for (uint32_t i = ent.y + threadIdx.x; i < ent.z; i += blockDim.x) {
-            int y, z, x0, x1;
-            item_coords(t, segs, ny, i, y, z, x0, x1);
-            row_segment<S>(t, g, y, z, x0, x1, sink);
-            sink.flush();
-        }
+        warp_bricks<S>(t, g, bm, ent.y, ent.z, 0, 32, split);
     }
 }
 
@@ -425,7 +586,7 @@ cudaError_t launch_bbox(const float *pts, int64_t n, int rx, int ry, int rz, uin
     if (e == cudaSuccess) e = cudaMemsetAsync(mm_scratch + 3, 0, 3 * sizeof(uint32_t), st);
     if (e == cudaSuccess) e = cudaMemsetAsync(gp, 0, sizeof(GridParams), st);
     if (e != cudaSuccess) return e;
-    int blocks = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
+    int blocks = (int)std::min<int64_t>((n / 4 + 255) / 256, 148 * 4);
     blocks = std::max(blocks, 1);
     k_bbox_reduce<<<blocks, 256, 0, st>>>(pts, n, mm_scratch, gp);
     count_launches(1);
@@ -444,19 +605,26 @@ cudaError_t launch_voxelize(const float *pts, const int32_t *tris, int64_t nt, c
     if (nt > 0) {
         const int64_t want = (nt + 255) / 256;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * 16));
-        const int bblocks = num_sms * 2;
+        const bool inplace = big == nullptr || big_cap == 0;
+#define SVO_VOX(S_, I_) \
+    k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(pts, tris, nt, gp, rx, ry, rz, bm, tune, big, big_cap, counters)
         if (strict) {
-            k_voxelize<true><<<blocks, 256, 0, st>>>(pts, tris, nt, gp, rx, ry, rz, bm, tune, big, big_cap,
-                                                    counters);
-            k_voxelize_big<true><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters,
-                                                         big_cap, counters + 1);
+            if (inplace) SVO_VOX(true, true); else SVO_VOX(true, false);
         } else {
-            k_voxelize<false><<<blocks, 256, 0, st>>>(pts, tris, nt, gp, rx, ry, rz, bm, tune, big, big_cap,
-                                                     counters);
-            k_voxelize_big<false><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters,
-                                                          big_cap, counters + 1);
+            if (inplace) SVO_VOX(false, true); else SVO_VOX(false, false);
         }
-        count_launches(2);
+#undef SVO_VOX
+        count_launches(1);
+        if (!inplace) {
+            const int bblocks = num_sms * 4;
+            if (strict)
+                k_voxelize_bricks<true><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters, big_cap,
+                                                                counters + 1, tune.split != 0);
+            else
+                k_voxelize_bricks<false><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters,
+                                                                 big_cap, counters + 1, tune.split != 0);
+            count_launches(1);
+        }
     }
     return cudaGetLastError();
 }

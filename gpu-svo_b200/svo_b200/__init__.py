@@ -61,6 +61,10 @@ class _Aabb(C.Structure):
     _fields_ = [("min", C.c_float * 3), ("max", C.c_float * 3), ("width", C.c_float * 3)]
 
 
+class Tuning(C.Structure):
+    _fields_ = [("serial_max", C.c_uint32), ("warp_max", C.c_uint32), ("split", C.c_uint32)]
+
+
 class MeshDesc(C.Structure):
     _fields_ = [
         ("points", C.c_void_p),
@@ -87,6 +91,8 @@ def lib() -> C.CDLL:
         L.svo_ctx_create.argtypes = [C.c_int, C.POINTER(vp)]
         L.svo_ctx_destroy.argtypes = [vp]
         L.svo_ctx_destroy.restype = None
+        L.svo_ctx_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.svo_ctx_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.svo_load_obj.argtypes = [C.c_char_p, C.POINTER(vp), i64p, C.POINTER(vp), i64p]
         L.svo_free_host.argtypes = [vp]
         L.svo_free_host.restype = None
@@ -194,6 +200,17 @@ class Context:
             self.close()
         except Exception:
             pass
+
+    @property
+    def tuning(self) -> tuple:
+        t = Tuning()
+        _check(lib().svo_ctx_get_tuning(self._h, C.byref(t)))
+        return (t.serial_max, t.warp_max, t.split)
+
+    @tuning.setter
+    def tuning(self, value) -> None:
+        t = Tuning(int(value[0]), int(value[1]), int(value[2]) if len(value) > 2 else 0)
+        _check(lib().svo_ctx_set_tuning(self._h, C.byref(t)))
 
     def build(self, points, tris, res, flags: int = 0, stream: int = 0) -> "Result":
         """svo_build.  points float32[n,3] and tris int32[m,3] (tris=None: soup),

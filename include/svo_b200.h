@@ -90,6 +90,19 @@ typedef struct svo_result svo_result;
 int svo_ctx_create(int device, svo_ctx **out);
 void svo_ctx_destroy(svo_ctx *ctx);
 
+/* Voxelizer work split: triangles whose grid bbox has at most serial_max
+ * voxels are tested by one thread; larger ones are cut into queue entries of
+ * at most warp_max 4x4x4 bricks, one warp per entry.  Results do not depend on
+ * these values, only the speed.  No counterpart in the reference
+ * (one thread per triangle there, src/SVO.cu:37-188). */
+typedef struct svo_tuning {
+    uint32_t serial_max;
+    uint32_t warp_max;
+    uint32_t split; /* also cull the 2x2x2 sub-bricks of surviving bricks */
+} svo_tuning;
+int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t);
+int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t);
+
 /* Thread-local message for the last non-zero status. */
 const char *svo_last_error(void);
 
