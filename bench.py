@@ -49,7 +49,7 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5"], default="torus_slivers")
+    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5", "heightfield"], default="torus_slivers")
     ap.add_argument("--res", type=int, default=0, help="override the workload's resolution")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -62,6 +62,9 @@ def workload(name: str):
     if name == "torus_slivers":
         pts, tris, res = meshgen.torus_slivers()
         return pts, tris, res, "torus_slivers_1M_res512"
+    if name == "heightfield":
+        pts, tris, res = meshgen.heightfield()
+        return pts, tris, res, "heightfield_5M_res2048"
     pts, tris, res = meshgen.icosphere_l5()
     return pts, tris, res, "icosphere_l5_res128"
 

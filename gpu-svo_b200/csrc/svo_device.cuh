@@ -39,16 +39,26 @@ __host__ __device__ __forceinline__ uint64_t morton3(uint32_t x, uint32_t y, uin
 // Floating-point model.  The reference's voxel test and node origins are
 // Eigen 3.4 expressions compiled by nvcc with --fmad=true.  Eigen evaluates a
 // 3-term dot as a0*b0 + (a1*b1 + a2*b2) and a 2-term dot as a0*b0 + a1*b1;
-// nvcc fuses each single-use product into the add/sub consuming it.  Every
-// operation here is an explicit round-to-nearest intrinsic, so the compiler
-// cannot re-fuse or reorder anything: STRICT=false reproduces the fused
-// pattern, STRICT=true rounds every operation.
+// nvcc fuses products into the adds consuming them.  Which product it fuses
+// was measured on nvcc 12.9 with the reference's loop structure: the first
+// one, except in the squared norm's inner sum and in the first two ZX edge
+// tests of the voxel loop (see tri_setup / voxel_test).  Every operation here
+// is an explicit round-to-nearest intrinsic, so the compiler cannot re-fuse
+// or reorder anything: STRICT=false reproduces the fused pattern,
+// STRICT=true rounds every operation.
 // ---------------------------------------------------------------------------
 template <bool STRICT>
 struct Fp {
     static __device__ __forceinline__ float dot2(float a0, float a1, float b0, float b1) {
         return STRICT ? __fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1))
                       : __fmaf_rn(a0, b0, __fmul_rn(a1, b1));
+    }
+    // a0*b0 + a1*b1 inside the voxel loop when only the second product varies
+    // with x: nvcc hoists the first product out of the loop, then fuses the
+    // second (the ZX projection test).
+    static __device__ __forceinline__ float dot2_late(float a0, float a1, float b0, float b1) {
+        return STRICT ? __fadd_rn(__fmul_rn(a0, b0), __fmul_rn(a1, b1))
+                      : __fmaf_rn(a1, b1, __fmul_rn(a0, b0));
     }
     // a1*b1 + a2*b2 (inner part of a 3-term dot)
     static __device__ __forceinline__ float dot3_tail(float a1, float a2, float b1, float b2) {

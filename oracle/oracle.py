@@ -84,6 +84,8 @@ def lib() -> C.CDLL:
         L.oracle_result_dedup.argtypes = [C.c_void_p, C.c_int]
         L.oracle_result_dedup.restype = C.c_void_p
         L.oracle_tables.argtypes = [C.c_void_p] * 4
+        L.oracle_fp_eval.argtypes = [C.c_int, C.c_int, C.c_void_p, C.c_int64, C.c_void_p]
+        L.oracle_set_fp_sites.argtypes = [C.c_void_p, C.c_int]
         L.oracle_result_free.argtypes = [C.c_void_p]
         L.oracle_write_tree.argtypes = [C.c_void_p, C.c_char_p]
         _lib = L
@@ -130,6 +132,26 @@ def tables() -> dict:
     out = {"neighbor_LUTparent": np.zeros(216, np.int16), "neighbor_LUTchild": np.zeros(216, np.int16),
            "d_vertSharedLUT": np.zeros(64, np.int16), "d_edgeSharedLUT": np.zeros(48, np.int16)}
     lib().oracle_tables(*(a.ctypes.data for a in out.values()))
+    return out
+
+
+FP_ARITY = {0: (4, 1), 1: (6, 1), 2: (4, 1), 3: (3, 1), 4: (3, 3), 5: (14, 1), 6: (14, 14)}
+FP_SITES = ("cross", "sq_inner", "sq_outer", "d12_inner", "d12_outer", "d_edge", "plane_inner", "plane_outer",
+            "loop_xy0", "loop_xy1", "loop_xy2", "loop_yz0", "loop_yz1", "loop_yz2", "loop_zx0", "loop_zx1", "loop_zx2")
+
+
+def set_fp_sites(choice) -> None:
+    """Contraction choice per site (0 first product, 1 second, 2 none)."""
+    arr = (C.c_int * len(choice))(*choice)
+    lib().oracle_set_fp_sites(arr, len(choice))
+
+
+def fp_eval(op: int, strict: bool, operands: np.ndarray) -> np.ndarray:
+    """The oracle's float model for one expression shape (see oracle_fp_eval)."""
+    k_in, k_out = FP_ARITY[op]
+    a = np.ascontiguousarray(operands, dtype=np.float32).reshape(-1, k_in)
+    out = np.zeros((a.shape[0], k_out), dtype=np.float32)
+    _check(lib().oracle_fp_eval(op, int(strict), a.ctypes.data, a.shape[0], out.ctypes.data))
     return out
 
 

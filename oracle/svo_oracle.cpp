@@ -101,12 +101,48 @@ inline void demorton(uint64_t c, uint32_t &x, uint32_t &y, uint32_t &z) {
 //   * cross(a,b) = (a1*b2 - a2*b1, a2*b0 - a0*b2, a0*b1 - a1*b0).
 //   * normalized() = v / sqrt(squaredNorm) when squaredNorm > 0, else v.
 // nvcc then fuses each single-use product into the add/sub that consumes it;
-// "reference" mode below states which product becomes the FMA (the left
-// operand of the add, the minuend of the sub); a GPU probe test checks this
-// against nvcc's own contraction of the same expressions.  "strict" mode
+// "reference" mode below states which product becomes the FMA: the left
+// operand of the add, the minuend of the sub -- except inside the voxel loop,
+// where a product that does not depend on the loop's x is hoisted first and
+// the other one is fused (dot2_late).  A GPU probe test checks this against
+// nvcc's own contraction of the same expressions in the same loop structure.  "strict" mode
 // rounds every operation (what a non-contracting compiler would produce).
 // ---------------------------------------------------------------------------
 namespace fp {
+// Contraction sites of the reference's arithmetic.  Choice per site: 0 fuse
+// the first product of the sum, 1 fuse the second, 2 no fusion.  Strict mode
+// never fuses.  The defaults are the pattern nvcc 12.9 produces for the
+// reference's expressions in their loop structure (tests/fp_probe.cu):
+// everything fuses its first product except the inner sum of the squared
+// norm (c1*c1 + c2*c2 fuses c2*c2) and the first two ZX edge tests in the
+// voxel loop (a*p.z is hoisted out of the x loop, b*p.x is fused); the third
+// ZX test fuses a*p.z.  oracle_set_fp_sites changes them (used only to search
+// for the pattern).
+enum Site {
+    kCross, kSqInner, kSqOuter, kD12Inner, kD12Outer, kDEdge, kPlaneInner, kPlaneOuter,
+    kLoopXY, kLoopYZ = kLoopXY + 3, kLoopZX = kLoopYZ + 3, kNumSites = kLoopZX + 3
+};
+int g_site[kNumSites] = {0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 0};
+
+inline float dot2s(int site, bool strict, float a0, float a1, float b0, float b1) {
+    const int c = strict ? 2 : g_site[site];
+    if (c == 0) return std::fmaf(a0, b0, a1 * b1);
+    if (c == 1) return std::fmaf(a1, b1, a0 * b0);
+    return a0 * b0 + a1 * b1;
+}
+inline float dot3s(int inner, int outer, bool strict, float a0, float a1, float a2, float b0, float b1,
+                   float b2) {
+    const float t = dot2s(inner, strict, a1, a2, b1, b2);
+    const int c = strict ? 2 : g_site[outer];
+    return c == 2 ? a0 * b0 + t : std::fmaf(a0, b0, t);
+}
+// a*b - c*d
+inline float diffs(int site, bool strict, float a, float b, float c, float d) {
+    const int k = strict ? 2 : g_site[site];
+    if (k == 0) return std::fmaf(a, b, -(c * d));
+    if (k == 1) return std::fmaf(-c, d, a * b);
+    return a * b - c * d;
+}
 inline float dot2(bool strict, float a0, float a1, float b0, float b1) {
     if (strict) return a0 * b0 + a1 * b1;
     return std::fmaf(a0, b0, a1 * b1);
@@ -115,7 +151,6 @@ inline float dot3(bool strict, float a0, float a1, float a2, float b0, float b1,
     if (strict) return a0 * b0 + (a1 * b1 + a2 * b2);
     return std::fmaf(a0, b0, std::fmaf(a1, b1, a2 * b2));
 }
-// a*b - c*d (one component of a cross product)
 inline float diffprod(bool strict, float a, float b, float c, float d) {
     if (strict) return a * b - c * d;
     return std::fmaf(a, b, -(c * d));
@@ -180,10 +215,10 @@ void tri_setup(bool strict, const Grid &g, const float *p0, const float *p1, con
     }
     // n = e0.cross(e1).normalized()   (src/SVO.cu:69)
     float c[3];
-    c[0] = fp::diffprod(strict, e0[1], e1[2], e0[2], e1[1]);
-    c[1] = fp::diffprod(strict, e0[2], e1[0], e0[0], e1[2]);
-    c[2] = fp::diffprod(strict, e0[0], e1[1], e0[1], e1[0]);
-    float sq = fp::dot3(strict, c[0], c[1], c[2], c[0], c[1], c[2]);
+    c[0] = fp::diffs(fp::kCross, strict, e0[1], e1[2], e0[2], e1[1]);
+    c[1] = fp::diffs(fp::kCross, strict, e0[2], e1[0], e0[0], e1[2]);
+    c[2] = fp::diffs(fp::kCross, strict, e0[0], e1[1], e0[1], e1[0]);
+    float sq = fp::dot3s(fp::kSqInner, fp::kSqOuter, strict, c[0], c[1], c[2], c[0], c[1], c[2]);
     if (sq > 0.0f) {
         float r = std::sqrt(sq);
         for (int i = 0; i < 3; ++i) s.n[i] = c[i] / r;
@@ -206,8 +241,8 @@ void tri_setup(bool strict, const Grid &g, const float *p0, const float *p1, con
         a[i] = cc[i] - v0[i];
         b[i] = (u[i] - cc[i]) - v0[i];
     }
-    s.d1 = fp::dot3(strict, n[0], n[1], n[2], a[0], a[1], a[2]);
-    s.d2 = fp::dot3(strict, n[0], n[1], n[2], b[0], b[1], b[2]);
+    s.d1 = fp::dot3s(fp::kD12Inner, fp::kD12Outer, strict, n[0], n[1], n[2], a[0], a[1], a[2]);
+    s.d2 = fp::dot3s(fp::kD12Inner, fp::kD12Outer, strict, n[0], n[1], n[2], b[0], b[1], b[2]);
     // projection tests (src/SVO.cu:96-149).  For the projection onto axes
     // (i, j) the edge normal is (-e[j], e[i]), negated when n on the third
     // axis is negative.
@@ -232,7 +267,7 @@ void tri_setup(bool strict, const Grid &g, const float *p0, const float *p1, con
             }
             pl.nn[k][0] = ne0;
             pl.nn[k][1] = ne1;
-            float dt = fp::dot2(strict, ne0, ne1, vs[k][pl.i], vs[k][pl.j]);
+            float dt = fp::dot2s(fp::kDEdge, strict, ne0, ne1, vs[k][pl.i], vs[k][pl.j]);
             pl.dd[k] = ((-1.0f * dt) + cmax(0.0f, u[pl.i] * ne0)) + cmax(0.0f, u[pl.j] * ne1);
         }
     }
@@ -241,14 +276,18 @@ void tri_setup(bool strict, const Grid &g, const float *p0, const float *p1, con
 // src/SVO.cu:156-177 for one voxel
 inline bool voxel_hit(bool strict, const Grid &g, const TriSetup &s, int x, int y, int z) {
     const float p[3] = {(float)x * g.unit[0], (float)y * g.unit[1], (float)z * g.unit[2]};
-    const float nDOTp = fp::dot3(strict, s.n[0], s.n[1], s.n[2], p[0], p[1], p[2]);
+    const float nDOTp =
+        fp::dot3s(fp::kPlaneInner, fp::kPlaneOuter, strict, s.n[0], s.n[1], s.n[2], p[0], p[1], p[2]);
     if ((nDOTp + s.d1) * (nDOTp + s.d2) > 0.0f) return false;
     for (int k = 0; k < 3; ++k)
-        if (fp::dot2(strict, s.nxy[k][0], s.nxy[k][1], p[0], p[1]) + s.dxy[k] < 0.0f) return false;
+        if (fp::dot2s(fp::kLoopXY + k, strict, s.nxy[k][0], s.nxy[k][1], p[0], p[1]) + s.dxy[k] < 0.0f)
+            return false;
     for (int k = 0; k < 3; ++k)
-        if (fp::dot2(strict, s.nyz[k][0], s.nyz[k][1], p[1], p[2]) + s.dyz[k] < 0.0f) return false;
+        if (fp::dot2s(fp::kLoopYZ + k, strict, s.nyz[k][0], s.nyz[k][1], p[1], p[2]) + s.dyz[k] < 0.0f)
+            return false;
     for (int k = 0; k < 3; ++k)
-        if (fp::dot2(strict, s.nzx[k][0], s.nzx[k][1], p[2], p[0]) + s.dzx[k] < 0.0f) return false;
+        if (fp::dot2s(fp::kLoopZX + k, strict, s.nzx[k][0], s.nzx[k][1], p[2], p[0]) + s.dzx[k] < 0.0f)
+            return false;
     return true;
 }
 
@@ -708,6 +747,94 @@ extern "C" {
 const char *oracle_last_error(void) { return g_err.c_str(); }
 
 void oracle_free(void *p) { std::free(p); }
+
+// The oracle's floating-point model on batches of operands, for comparing it
+// with what nvcc makes of the same expressions.  op (operands -> results):
+//   0 dot2 (a0,a1,b0,b1)            1 dot3 (a0,a1,a2,b0,b1,b2)
+//   2 a*b-c*d (a,b,c,d)             3 origin o+w*x (o,w,x)
+//   4 normalize (c0,c1,c2) -> 3     5 voxel test: tri (9), voxel (x,y,z),
+//                                     unit, res -> 1.0 / 0.0 (grid origin 0)
+//   6 triangle setup, same operands -> n (3), d1, d2, dxy (3), dyz (3), dzx (3)
+int oracle_set_fp_sites(const int *choice, int n) {
+    for (int i = 0; i < n && i < fp::kNumSites; ++i) fp::g_site[i] = choice[i];
+    return fp::kNumSites;
+}
+
+int oracle_fp_eval(int op, int strict, const float *in, int64_t n, float *out) {
+    const bool st = strict != 0;
+    for (int64_t i = 0; i < n; ++i) {
+        switch (op) {
+            case 0: {
+                const float *a = in + 4 * i;
+                out[i] = fp::dot2(st, a[0], a[1], a[2], a[3]);
+                break;
+            }
+            case 1: {
+                const float *a = in + 6 * i;
+                out[i] = fp::dot3(st, a[0], a[1], a[2], a[3], a[4], a[5]);
+                break;
+            }
+            case 2: {
+                const float *a = in + 4 * i;
+                out[i] = fp::diffprod(st, a[0], a[1], a[2], a[3]);
+                break;
+            }
+            case 3: {
+                const float *a = in + 3 * i;
+                out[i] = fp::origin(st, a[0], a[1], a[2]);
+                break;
+            }
+            case 4: {
+                const float *c = in + 3 * i;
+                const float sq = fp::dot3(st, c[0], c[1], c[2], c[0], c[1], c[2]);
+                for (int k = 0; k < 3; ++k) out[3 * i + k] = sq > 0.0f ? c[k] / std::sqrt(sq) : c[k];
+                break;
+            }
+            case 5: {
+                const float *a = in + 14 * i;
+                Grid g;
+                const int res = (int)a[13];
+                for (int k = 0; k < 3; ++k) {
+                    g.res[k] = res;
+                    g.origin[k] = 0.0f;
+                    g.unit[k] = a[12];
+                }
+                TriSetup ts;
+                tri_setup(st, g, a, a + 3, a + 6, ts);
+                const int x = (int)a[9], y = (int)a[10], z = (int)a[11];
+                const bool inside = x >= ts.lo[0] && x <= ts.hi[0] && y >= ts.lo[1] && y <= ts.hi[1] &&
+                                    z >= ts.lo[2] && z <= ts.hi[2];
+                out[i] = inside && voxel_hit(st, g, ts, x, y, z) ? 1.0f : 0.0f;
+                break;
+            }
+            case 6: {
+                const float *a = in + 14 * i;
+                Grid g;
+                const int res = (int)a[13];
+                for (int k = 0; k < 3; ++k) {
+                    g.res[k] = res;
+                    g.origin[k] = 0.0f;
+                    g.unit[k] = a[12];
+                }
+                TriSetup ts;
+                tri_setup(st, g, a, a + 3, a + 6, ts);
+                float *o = out + 14 * i;
+                for (int k = 0; k < 3; ++k) o[k] = ts.n[k];
+                o[3] = ts.d1;
+                o[4] = ts.d2;
+                for (int k = 0; k < 3; ++k) {
+                    o[5 + k] = ts.dxy[k];
+                    o[8 + k] = ts.dyz[k];
+                    o[11 + k] = ts.dzx[k];
+                }
+                break;
+            }
+            default:
+                return fail(ORACLE_ERR_INVALID_ARGUMENT, "unknown op");
+        }
+    }
+    return ORACLE_OK;
+}
 
 void oracle_tables(int16_t *nbr_parent, int16_t *nbr_child, int16_t *vert_shared,
                    int16_t *edge_shared) {

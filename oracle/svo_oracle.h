@@ -94,6 +94,10 @@ void oracle_morton_decode(uint64_t code, uint32_t *x, uint32_t *y, uint32_t *z);
 void oracle_tables(int16_t *nbr_parent, int16_t *nbr_child, int16_t *vert_shared,
                    int16_t *edge_shared);
 
+/* The floating-point model on operand batches (see svo_oracle.cpp for ops). */
+int oracle_set_fp_sites(const int *choice, int n);
+int oracle_fp_eval(int op, int strict, const float *in, int64_t n, float *out);
+
 /* Full create(): voxelize, octree levels, neighbours, vertex/edge arrays.
  * n_threads <= 0 means all hardware threads. */
 int oracle_build(const float *points, int64_t n_points, const int32_t *tris, int64_t n_tris,
