@@ -136,269 +136,640 @@ struct StageTimer {
         if (on && rec[a] && rec[b]) cudaEventElapsedTime(&ms, ev[a], ev[b]);
         return ms;
     }
-    void store(svo_result *r) const {
-        if (!on) return;
-        cudaEventSynchronize(ev[kDedup]);
-        r->n_timings = 9;
-        r->timings[0] = span(kStart, kDedup);
-        r->timings[1] = span(kStart, kBbox);
-        r->timings[2] = span(kBbox, kVox);
-        r->timings[3] = span(kVox, kPyr);
-        r->timings[4] = span(kPyr, kScan);
-        r->timings[5] = span(kCompact0, kCompact);
-        r->timings[6] = span(kCompact, kEmit);
-        r->timings[7] = span(kEmit, kUnique);
-        r->timings[8] = span(kUnique, kDedup);
+};
+
+// ---------------------------------------------------------------------------
+// Batches.  Phase A (svo_batch_create) runs for every mesh at once: bounding
+// cube, voxelization, bitmap pyramid, one scan over all block counts, level
+// totals, then one small device->host read.  Phase B (svo_batch_emit) writes
+// the octrees of any subset of the meshes in one compaction launch and one
+// emission launch.  svo_build is a batch of one.
+// ---------------------------------------------------------------------------
+struct MeshHost {
+    const float *h_pts = nullptr;      // caller's pointers
+    const int32_t *h_tris = nullptr;
+    int64_t n_pts = 0, n_tris = 0;     // n_tris: triangles (soup: n_pts / 3)
+    int res[3] = {0, 0, 0};
+    const float *d_pts = nullptr;      // device copies or the caller's device pointers
+    const int32_t *d_tris = nullptr;
+    bool tris_on_device = false;
+    Pyramid py;
+    uint64_t bits_off = 0, cnt_off = 0;  // into the batch's bitmap / count buffers
+    int status = SVO_OK;
+    std::string error;
+    GridParams gp{};
+    uint32_t totals[kMaxLevels] = {};
+    int T = -1;
+    uint64_t n_l[kMaxLevels] = {}, off[kMaxLevels + 1] = {};
+    uint64_t N = 0;
+    bool emitted = false;
+};
+
+// Layout of the small per-batch meta block (device), read back after phase A.
+struct MetaLayout {
+    size_t counters = 0, gp = 0, totals = 0, mm = 0, done = 0, imm = 0, bytes = 0;
+    explicit MetaLayout(int n) {
+        auto take = [&](size_t b) {
+            const size_t o = (bytes + 255) / 256 * 256;
+            bytes = o + b;
+            return o;
+        };
+        counters = take(4 * sizeof(uint32_t));
+        gp = take(sizeof(GridParams) * n);
+        totals = take(sizeof(uint32_t) * kMaxLevels * n);
+        mm = take(sizeof(uint32_t) * 8 * n);
+        done = take(sizeof(uint32_t) * n);
+        imm = take(sizeof(int32_t) * 2 * n);
     }
 };
 
-// Device-side meta block read back by the host after the count phase.
-struct Meta {
-    GridParams gp;
-    uint32_t totals[kMaxLevels];
-    uint32_t counters[2];  // big-triangle entries, queue cursor
-    unsigned long long dups[2];
-    uint64_t top_code;
+__global__ void k_meta_init(uint32_t *mm, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    for (int a = 0; a < 3; ++a) {
+        mm[8 * i + a] = 0xFFFFFFFFu;
+        mm[8 * i + 3 + a] = 0u;
+    }
+}
+
+// top_codes[i] = *ptrs[i] (the single code of each mesh's top level)
+__global__ void k_gather_top(const uint64_t *const *ptrs, int n, uint64_t *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = *ptrs[i];
+}
+
+}  // namespace
+
+struct svo_batch {
+    svo_ctx *ctx = nullptr;
+    cudaStream_t st = nullptr;
+    uint32_t flags = 0;
+    std::vector<MeshHost> m;
+    std::vector<int> live;                  // meshes with device work
+    std::vector<void *> allocs;             // phase A buffers (pool)
+    uint64_t *bits = nullptr;
+    uint32_t *cnt = nullptr, *pre = nullptr;
+    unsigned char *meta = nullptr;
+    MeshDev *d_mesh = nullptr;
+    std::vector<MeshDev> h_mesh;
+    uint64_t total_blocks = 0;
+    float timings_a[5] = {};                // total, bbox, voxelize, pyramid, scan
+    bool timed = false;
 };
 
-int build_one(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t *tris, int64_t n_tris,
-              int rx, int ry, int rz, uint32_t flags, cudaStream_t st, svo_result **out) {
-    *out = nullptr;
-    if (!points || n_points <= 0) return fail(SVO_ERR_EMPTY, "mesh has no vertices");
-    if (n_tris < 0 || (!tris && n_points % 3 != 0))
-        return fail(SVO_ERR_INVALID_ARGUMENT, "triangle soup needs 3 points per triangle");
-    const int64_t nt = tris ? n_tris : n_points / 3;
-    if (nt > 0x7FFFFFFF) return fail(SVO_ERR_UNSUPPORTED, "more than 2^31-1 triangles");
-    const int res[3] = {rx, ry, rz};
-    for (int a = 0; a < 3; ++a)
-        if (res[a] < 1 || res[a] > kMaxRes)
-            return fail(SVO_ERR_UNSUPPORTED, "resolution %d outside [1, %d]", res[a], kMaxRes);
+namespace {
+
+template <class T>
+T *batch_alloc(svo_batch *b, size_t count, cudaError_t &err) {
+    T *p = pool_alloc<T>(b->ctx->pool, b->st, count, err);
+    if (p) b->allocs.push_back(p);
+    return p;
+}
+
+void batch_release(svo_batch *b) {
+    for (void *p : b->allocs) cudaFreeAsync(p, b->st);
+    b->allocs.clear();
+}
+
+int mesh_error(MeshHost &mh, int code, const char *msg) {
+    mh.status = code;
+    mh.error = msg;
+    return code;
+}
+
+template <class T>
+cudaError_t upload(T *dst, const std::vector<T> &src, cudaStream_t st) {
+    if (src.empty()) return cudaSuccess;
+    return cudaMemcpyAsync(dst, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+}
+
+// Phase A.  Returns SVO_OK when the batch itself works (individual meshes
+// may still carry an error status).
+int batch_phase_a(svo_batch *b) {
+    svo_ctx *ctx = b->ctx;
+    cudaStream_t st = b->st;
     SVO_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
-
-    Scratch S{ctx->pool, st};
-    // ---- mesh on the device ----
-    const float *d_pts = points;
-    const int32_t *d_tris = tris;
-    if (!is_device_ptr(points)) {
-        float *p = S.get<float>((size_t)n_points * 3);
-        if (!p) return cuda_fail(S.err, "alloc points");
-        SVO_TRY(cudaMemcpyAsync(p, points, (size_t)n_points * 12, cudaMemcpyHostToDevice, st), "copy points");
-        d_pts = p;
+    cudaError_t err = cudaSuccess;
+    // ---- validation and mesh data on the device ----
+    std::vector<int> idx_check;  // meshes whose device-side indices need a range check
+    for (int i = 0; i < (int)b->m.size(); ++i) {
+        MeshHost &mh = b->m[i];
+        if (!mh.h_pts || mh.n_pts <= 0) {
+            mesh_error(mh, SVO_ERR_EMPTY, "mesh has no vertices");
+            continue;
+        }
+        if (mh.n_tris < 0 || (!mh.h_tris && mh.n_pts % 3 != 0)) {
+            mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "triangle soup needs 3 points per triangle");
+            continue;
+        }
+        if (!mh.h_tris) mh.n_tris = mh.n_pts / 3;
+        if (mh.n_tris > 0x7FFFFFFF) {
+            mesh_error(mh, SVO_ERR_UNSUPPORTED, "more than 2^31-1 triangles");
+            continue;
+        }
+        bool bad_res = false;
+        for (int a = 0; a < 3; ++a) bad_res |= mh.res[a] < 1 || mh.res[a] > kMaxRes;
+        if (bad_res) {
+            char msg[96];
+            snprintf(msg, sizeof(msg), "resolution outside [1, %d]", kMaxRes);
+            mesh_error(mh, SVO_ERR_UNSUPPORTED, msg);
+            continue;
+        }
+        if (mh.h_tris && mh.n_tris > 0) {
+            mh.tris_on_device = is_device_ptr(mh.h_tris);
+            if (!mh.tris_on_device) {
+                bool ok = true;
+                for (int64_t k = 0; k < 3 * mh.n_tris && ok; ++k)
+                    ok = mh.h_tris[k] >= 0 && mh.h_tris[k] < mh.n_pts;
+                if (!ok) {
+                    mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "triangle index out of range");
+                    continue;
+                }
+            }
+        }
+        if (is_device_ptr(mh.h_pts)) {
+            mh.d_pts = mh.h_pts;
+        } else {
+            float *p = batch_alloc<float>(b, (size_t)mh.n_pts * 3, err);
+            if (!p) return cuda_fail(err, "alloc points");
+            SVO_TRY(cudaMemcpyAsync(p, mh.h_pts, (size_t)mh.n_pts * 12, cudaMemcpyHostToDevice, st), "copy points");
+            mh.d_pts = p;
+        }
+        if (mh.h_tris && mh.n_tris > 0) {
+            if (mh.tris_on_device) {
+                mh.d_tris = mh.h_tris;
+                idx_check.push_back(i);
+            } else {
+                int32_t *p = batch_alloc<int32_t>(b, (size_t)mh.n_tris * 3, err);
+                if (!p) return cuda_fail(err, "alloc tris");
+                SVO_TRY(cudaMemcpyAsync(p, mh.h_tris, (size_t)mh.n_tris * 12, cudaMemcpyHostToDevice, st),
+                        "copy tris");
+                mh.d_tris = p;
+            }
+        }
+        b->live.push_back(i);
     }
-    if (tris && nt > 0 && !is_device_ptr(tris)) {
-        // validate indices on the host while they are here
-        for (int64_t i = 0; i < 3 * nt; ++i)
-            if (tris[i] < 0 || tris[i] >= n_points)
-                return fail(SVO_ERR_INVALID_ARGUMENT, "triangle index %d out of range", tris[i]);
-        int32_t *p = S.get<int32_t>((size_t)nt * 3);
-        if (!p) return cuda_fail(S.err, "alloc tris");
-        SVO_TRY(cudaMemcpyAsync(p, tris, (size_t)nt * 12, cudaMemcpyHostToDevice, st), "copy tris");
-        d_tris = p;
-    } else if (tris && nt > 0) {
-        std::vector<int32_t> mm(2);
-        int32_t *d_mm = S.get<int32_t>(2);
-        if (!d_mm) return cuda_fail(S.err, "alloc");
-        SVO_TRY(launch_index_range(d_tris, nt * 3, d_mm, st), "index range");
-        SVO_TRY(cudaMemcpyAsync(mm.data(), d_mm, 8, cudaMemcpyDeviceToHost, st), "copy");
-        SVO_TRY(cudaStreamSynchronize(st), "sync");
-        if (mm[0] < 0 || mm[1] >= n_points)
-            return fail(SVO_ERR_INVALID_ARGUMENT, "triangle index out of range");
+    const int n = (int)b->live.size();
+    if (n == 0) return SVO_OK;
+    const MetaLayout ml(n);
+    b->meta = batch_alloc<unsigned char>(b, ml.bytes, err);
+    if (!b->meta) return cuda_fail(err, "alloc meta");
+    if (!idx_check.empty()) {  // device-side index ranges, one read for all meshes
+        int32_t *imm = reinterpret_cast<int32_t *>(b->meta + ml.imm);
+        for (size_t k = 0; k < idx_check.size(); ++k) {
+            const MeshHost &mh = b->m[idx_check[k]];
+            SVO_TRY(launch_index_range(mh.d_tris, mh.n_tris * 3, imm + 2 * k, st), "index range");
+        }
+        std::vector<int32_t> h(2 * idx_check.size());
+        SVO_TRY(cudaMemcpyAsync(h.data(), imm, h.size() * 4, cudaMemcpyDeviceToHost, st), "read");
+        SVO_TRY(cudaStreamSynchronize(st), "index check");
+        std::vector<int> keep;
+        for (size_t k = 0; k < idx_check.size(); ++k) {
+            MeshHost &mh = b->m[idx_check[k]];
+            if (h[2 * k] < 0 || h[2 * k + 1] >= mh.n_pts) mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "triangle index out of range");
+        }
+        for (int i : b->live)
+            if (b->m[i].status == SVO_OK) keep.push_back(i);
+        if ((int)keep.size() != n) {
+            b->live = keep;
+            return batch_phase_a(b);  // rebuild the tables without the rejected meshes
+        }
     }
-
-    const Pyramid py = make_pyramid(rx, ry, rz);
-    Meta *d_meta = S.get<Meta>(1);
-    uint32_t *d_mm = S.get<uint32_t>(8);
-    uint64_t *d_bits = S.get<uint64_t>(py.total_words);
-    uint32_t *d_cnt = S.get<uint32_t>(py.total_blocks);
-    uint32_t *d_pre = S.get<uint32_t>(py.total_blocks + 1);
-    unsigned long long *d_scan = S.get<unsigned long long>(scan_scratch_words(py.total_blocks));
-    uint32_t *d_done = S.get<uint32_t>(1);
-    uint32_t big_cap = (uint32_t)std::min<int64_t>(std::max<int64_t>(2 * nt, 1 << 16), 0x7FFFFFFF);
-    uint4 *d_big = S.get<uint4>(big_cap);
-    if (S.err != cudaSuccess) return cuda_fail(S.err, "scratch allocation");
-    SVO_TRY(cudaMemsetAsync(d_meta, 0, sizeof(Meta), st), "memset");
-    SVO_TRY(cudaMemsetAsync(d_done, 0, 4, st), "memset");
-    GridParams *d_gp = &d_meta->gp;
-    StageTimer tm((flags & SVO_FLAG_TIMINGS) != 0);
-    tm.mark(StageTimer::kStart, st);
-    SVO_TRY(launch_bbox(d_pts, n_points, rx, ry, rz, d_mm, d_gp, st), "bbox");
-    tm.mark(StageTimer::kBbox, st);
-    const bool strict = (flags & SVO_FLAG_STRICT_FP) != 0;
-    Meta meta;
+    // ---- layout ----
+    uint64_t words = 0, blocks = 0, tris = 0;
+    uint32_t ctas = 0, bblocks = 0;
+    std::vector<uint64_t> tri_off(n + 1);
+    std::vector<uint32_t> cta_off(n + 1), bbox_off(n + 1);
+    for (int k = 0; k < n; ++k) {
+        MeshHost &mh = b->m[b->live[k]];
+        mh.py = make_pyramid(mh.res[0], mh.res[1], mh.res[2]);
+        mh.bits_off = words;
+        mh.cnt_off = blocks;
+        words += (mh.py.total_words + 31) / 32 * 32;
+        blocks += mh.py.total_blocks;
+        tri_off[k] = tris;
+        cta_off[k] = ctas;
+        bbox_off[k] = bblocks;
+        tris += (uint64_t)mh.n_tris;
+        ctas += mh.py.ctas;
+        bblocks += bbox_blocks(mh.n_pts);
+    }
+    tri_off[n] = tris;
+    cta_off[n] = ctas;
+    bbox_off[n] = bblocks;
+    b->total_blocks = blocks;
+    b->bits = batch_alloc<uint64_t>(b, words, err);
+    b->cnt = batch_alloc<uint32_t>(b, blocks, err);
+    b->pre = batch_alloc<uint32_t>(b, blocks + 1, err);
+    unsigned long long *scan = batch_alloc<unsigned long long>(b, scan_scratch_words(blocks), err);
+    b->d_mesh = batch_alloc<MeshDev>(b, n, err);
+    uint64_t *d_tri_off = batch_alloc<uint64_t>(b, n + 1, err);
+    uint32_t *d_cta_off = batch_alloc<uint32_t>(b, n + 1, err);
+    uint32_t *d_bbox_off = batch_alloc<uint32_t>(b, n + 1, err);
+    uint32_t big_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(2 * tris, 1 << 16), 0x7FFFFFFFu);
+    uint4 *big = batch_alloc<uint4>(b, big_cap, err);
+    if (err != cudaSuccess) return cuda_fail(err, "batch scratch");
+    GridParams *gp = reinterpret_cast<GridParams *>(b->meta + ml.gp);
+    uint32_t *totals = reinterpret_cast<uint32_t *>(b->meta + ml.totals);
+    uint32_t *mm = reinterpret_cast<uint32_t *>(b->meta + ml.mm);
+    uint32_t *done = reinterpret_cast<uint32_t *>(b->meta + ml.done);
+    uint32_t *counters = reinterpret_cast<uint32_t *>(b->meta + ml.counters);
+    b->h_mesh.assign(n, MeshDev{});
+    for (int k = 0; k < n; ++k) {
+        const MeshHost &mh = b->m[b->live[k]];
+        MeshDev &d = b->h_mesh[k];
+        d.pts = mh.d_pts;
+        d.tris = mh.d_tris;
+        d.n_pts = mh.n_pts;
+        d.n_tris = mh.n_tris;
+        for (int a = 0; a < 3; ++a) d.res[a] = mh.res[a];
+        d.gp = gp + k;
+        d.mm = mm + 8 * k;
+        d.bits = b->bits + mh.bits_off;
+        d.cnt = b->cnt + mh.cnt_off;
+        d.pre = b->pre + mh.cnt_off;
+        d.totals = totals + kMaxLevels * k;
+        d.done = done + k;
+        d.py = mh.py;
+    }
+    SVO_TRY(upload(b->d_mesh, b->h_mesh, st), "upload meshes");
+    SVO_TRY(upload(d_tri_off, tri_off, st), "upload");
+    SVO_TRY(upload(d_cta_off, cta_off, st), "upload");
+    SVO_TRY(upload(d_bbox_off, bbox_off, st), "upload");
+    const BatchDev bd{b->d_mesh, n, d_tri_off, d_cta_off, d_bbox_off};
+    const bool strict = (b->flags & SVO_FLAG_STRICT_FP) != 0;
+    StageTimer tm((b->flags & SVO_FLAG_TIMINGS) != 0);
     for (int attempt = 0; attempt < 2; ++attempt) {
-        SVO_TRY(cudaMemsetAsync(d_bits, 0, py.total_words * 8, st), "memset bitmap");
-        SVO_TRY(cudaMemsetAsync(d_cnt, 0, py.total_blocks * 4, st), "memset counts");
-        SVO_TRY(launch_voxelize(d_pts, d_tris, nt, d_gp, rx, ry, rz, strict, reinterpret_cast<uint32_t *>(d_bits),
-                                ctx->tune, d_big, big_cap, d_meta->counters, ctx->num_sms, st),
+        tm.mark(StageTimer::kStart, st);
+        SVO_TRY(cudaMemsetAsync(b->meta, 0, ml.imm, st), "memset meta");
+        k_meta_init<<<(n + 127) / 128, 128, 0, st>>>(mm, n);
+        count_launches(1);
+        SVO_TRY(launch_bbox(bd, bblocks, st), "bbox");
+        tm.mark(StageTimer::kBbox, st);
+        SVO_TRY(cudaMemsetAsync(b->bits, 0, words * 8, st), "memset bitmaps");
+        SVO_TRY(cudaMemsetAsync(b->cnt, 0, blocks * 4, st), "memset counts");
+        SVO_TRY(launch_voxelize(bd, (int64_t)tris, strict, ctx->tune, big, big_cap, counters, ctx->num_sms, st),
                 "voxelize");
         tm.mark(StageTimer::kVox, st);
-        SVO_TRY(launch_pyramid(py, d_bits, d_cnt, d_done, st), "pyramid");
+        SVO_TRY(launch_pyramid(bd, ctas, st), "pyramid");
         tm.mark(StageTimer::kPyr, st);
-        SVO_TRY(launch_scan(d_cnt, d_pre, py.total_blocks, d_scan, &d_meta->gp.status, st), "scan");
-        SVO_TRY(launch_level_totals(py, d_pre, d_meta->totals, st), "totals");
+        SVO_TRY(launch_scan(b->cnt, b->pre, blocks, scan, counters + 2, st), "scan");
+        SVO_TRY(launch_level_totals(bd, st), "totals");
         tm.mark(StageTimer::kScan, st);
-        SVO_TRY(cudaMemcpyAsync(&meta, d_meta, sizeof(Meta), cudaMemcpyDeviceToHost, st), "read meta");
+        std::vector<unsigned char> h(ml.imm);
+        SVO_TRY(cudaMemcpyAsync(h.data(), b->meta, ml.imm, cudaMemcpyDeviceToHost, st), "read meta");
         SVO_TRY(cudaStreamSynchronize(st), "count phase");
-        if (meta.counters[0] <= big_cap) break;
-        // more big-triangle entries than the queue holds: grow it and redo
-        big_cap = meta.counters[0];
-        d_big = S.get<uint4>(big_cap);
-        if (!d_big) return cuda_fail(S.err, "big-triangle queue");
-    }
-    if (meta.gp.status & kStatusNonFinite) return fail(SVO_ERR_INVALID_ARGUMENT, "non-finite vertex coordinate");
-    if (meta.gp.status & kStatusScanTimeout) return fail(SVO_ERR_DEVICE_TIMEOUT, "scan look-back timed out");
-    if (meta.counters[0] > big_cap) return fail(SVO_ERR_CUDA, "big-triangle queue overflow");
-
-    // ---- level structure (src/SVO.cu:383-495) ----
-    const uint32_t C0 = meta.totals[0];
-    if (C0 == 0) return fail(SVO_ERR_EMPTY, "no surface voxels");
-    if (C0 == 1) return fail(SVO_ERR_DEGENERATE, "a single surface voxel: the reference's build is undefined");
-    int T = -1;
-    for (int l = 0; l < py.levels; ++l)
-        if (meta.totals[l] == 1) {
-            T = l;
-            break;
+        const uint32_t *hc = reinterpret_cast<const uint32_t *>(h.data() + ml.counters);
+        if (hc[2] & kStatusScanTimeout) return fail(SVO_ERR_DEVICE_TIMEOUT, "scan look-back timed out");
+        if (hc[0] > big_cap) {  // more big-triangle entries than the queue holds: grow it, redo
+            big_cap = hc[0];
+            big = batch_alloc<uint4>(b, big_cap, err);
+            if (!big) return cuda_fail(err, "big-triangle queue");
+            continue;
         }
-    if (T < 0) return fail(SVO_ERR_CUDA, "octree levels did not converge");
-    uint64_t off[kMaxLevels + 1] = {};
-    uint64_t n_l[kMaxLevels] = {};
-    for (int l = 0; l <= T; ++l) {
-        n_l[l] = l < T ? 8ull * meta.totals[l + 1] : 1ull;
-        off[l + 1] = off[l] + n_l[l];
+        for (int k = 0; k < n; ++k) {
+            MeshHost &mh = b->m[b->live[k]];
+            std::memcpy(&mh.gp, h.data() + ml.gp + sizeof(GridParams) * k, sizeof(GridParams));
+            std::memcpy(mh.totals, h.data() + ml.totals + sizeof(uint32_t) * kMaxLevels * k, sizeof(mh.totals));
+        }
+        break;
     }
-    const uint64_t N = off[T + 1];
-    if (N >= 0xFFFFFFFFull) return fail(SVO_ERR_UNSUPPORTED, "more than 2^32-2 nodes");
+    if (tm.on) {
+        b->timed = true;
+        b->timings_a[0] = tm.span(StageTimer::kStart, StageTimer::kScan);
+        b->timings_a[1] = tm.span(StageTimer::kStart, StageTimer::kBbox);
+        b->timings_a[2] = tm.span(StageTimer::kBbox, StageTimer::kVox);
+        b->timings_a[3] = tm.span(StageTimer::kVox, StageTimer::kPyr);
+        b->timings_a[4] = tm.span(StageTimer::kPyr, StageTimer::kScan);
+    }
+    // ---- level structure per mesh (src/SVO.cu:383-495) ----
+    for (int k = 0; k < n; ++k) {
+        MeshHost &mh = b->m[b->live[k]];
+        if (mh.gp.status & kStatusNonFinite) {
+            mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "non-finite vertex coordinate");
+            continue;
+        }
+        const uint32_t C0 = mh.totals[0];
+        if (C0 == 0) {
+            mesh_error(mh, SVO_ERR_EMPTY, "no surface voxels");
+            continue;
+        }
+        if (C0 == 1) {
+            mesh_error(mh, SVO_ERR_DEGENERATE, "a single surface voxel: the reference's build is undefined");
+            continue;
+        }
+        mh.T = -1;
+        for (int l = 0; l < mh.py.levels; ++l)
+            if (mh.totals[l] == 1) {
+                mh.T = l;
+                break;
+            }
+        if (mh.T < 0) {
+            mesh_error(mh, SVO_ERR_CUDA, "octree levels did not converge");
+            continue;
+        }
+        for (int l = 0; l <= mh.T; ++l) {
+            mh.n_l[l] = l < mh.T ? 8ull * mh.totals[l + 1] : 1ull;
+            mh.off[l + 1] = mh.off[l] + mh.n_l[l];
+        }
+        mh.N = mh.off[mh.T + 1];
+        if (mh.N >= 0xFFFFFFFFull) mesh_error(mh, SVO_ERR_UNSUPPORTED, "more than 2^32-2 nodes");
+    }
+    return SVO_OK;
+}
 
-    svo_result *r = new svo_result();
-    r->device = ctx->device;
-    r->stream = st;
-    r->pool = ctx->pool;
-    r->depth = T + 1;
-    for (int l = 0; l <= T; ++l) r->level_counts.push_back((int64_t)n_l[l]);
-    for (int a = 0; a < 3; ++a) {
-        r->bbox.min[a] = meta.gp.bbox[a];
-        r->bbox.max[a] = meta.gp.bbox[3 + a];
-        r->bbox.width[a] = meta.gp.bbox[6 + a];
-        r->unit[a] = meta.gp.unit[a];
-    }
-    r->n_nodes = N;
+// Bytes of the outputs of one mesh.
+uint64_t output_bytes(const MeshHost &mh, uint32_t flags) {
+    uint64_t b = mh.N * sizeof(svo_node);
+    if (!(flags & SVO_FLAG_NO_VERT_EDGE)) b += mh.N * (8 * sizeof(svo_vertex) + 12 * sizeof(svo_edge));
+    if (!(flags & SVO_FLAG_NO_KEYS)) b += (uint64_t)mh.totals[0] * 8;
+    return b;
+}
+
+// Phase B for meshes [first, first + count).
+int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *status_out) {
+    svo_ctx *ctx = b->ctx;
+    cudaStream_t st = b->st;
+    const uint32_t flags = b->flags;
     const bool ve = !(flags & SVO_FLAG_NO_VERT_EDGE);
     const bool want_keys = !(flags & SVO_FLAG_NO_KEYS);
-    cudaError_t err = cudaSuccess;
-    r->nodes = pool_alloc<svo_node>(ctx->pool, st, N, err);
-    if (ve) {
-        r->verts = pool_alloc<svo_vertex>(ctx->pool, st, N * 8, err);
-        r->edges = pool_alloc<svo_edge>(ctx->pool, st, N * 12, err);
-        r->n_verts = N * 8;
-        r->n_edges = N * 12;
+    SVO_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    std::vector<int> wave;   // batch mesh indices emitted now
+    std::vector<int> dev_k;  // their index in b->live
+    for (int i = first; i < first + count; ++i) {
+        out[i - first] = nullptr;
+        MeshHost &mh = b->m[i];
+        if (mh.status == SVO_OK && mh.emitted) mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "mesh already emitted");
+        if (mh.status != SVO_OK) continue;
+        wave.push_back(i);
+        dev_k.push_back((int)(std::find(b->live.begin(), b->live.end(), i) - b->live.begin()));
     }
-    if (want_keys) {
-        r->keys = pool_alloc<uint64_t>(ctx->pool, st, C0, err);
-        r->n_keys = C0;
-    }
-    uint64_t koff[kMaxLevels] = {};
-    uint64_t ktot = 0;
-    for (int l = 1; l <= T; ++l) {
-        koff[l] = ktot;
-        ktot += meta.totals[l];
-    }
-    uint64_t *d_K = S.get<uint64_t>(ktot + 1);
-    if (err != cudaSuccess || S.err != cudaSuccess) {
-        svo_result_free(r);
-        return cuda_fail(err != cudaSuccess ? err : S.err, "output allocation");
-    }
+    const int n = (int)wave.size();
+    std::vector<svo_result *> res(n, nullptr);
     int rc = SVO_OK;
     auto check = [&](cudaError_t e, const char *what) {
         if (e != cudaSuccess && rc == SVO_OK) rc = cuda_fail(e, what);
     };
-    tm.mark(StageTimer::kCompact0, st);
-    check(launch_compact(py, d_bits, d_pre, 1, T + 1, d_K, koff, st), "compact levels");
-    if (want_keys) {
-        uint64_t k0[kMaxLevels] = {};
-        check(launch_compact(py, d_bits, d_pre, 0, 1, r->keys, k0, st), "compact keys");
-    }
-    tm.mark(StageTimer::kCompact, st);
-    EmitParams P{};
-    P.T = T;
-    P.N = (uint32_t)N;
-    P.flags = flags;
-    const uint32_t R = 1u << (py.grid_levels - 1);
-    float w = 0.0f;
-    for (int l = 0; l <= T; ++l) {
-        P.lv[l].off = (uint32_t)off[l];
-        P.lv[l].n = (uint32_t)n_l[l];
-        P.lv[l].K1 = d_K + (l < T ? koff[l + 1] : koff[T]);
-        P.lv[l].bits = d_bits + py.woff[l];
-        P.lv[l].coff = py.coff[l];
-        P.lv[l].side = std::max<uint32_t>(1u, R >> l);
-    }
-    // widths: unitVoxelSize.x doubled per level (src/SVO.cu:351,483)
-    w = meta.gp.unit[0];
-    for (int l = 0; l <= T; ++l) {
-        P.lv[l].width = w;
-        w = w * 2.0f;
-    }
-    P.pre = d_pre;
-    P.gp = d_gp;
-    P.nodes = r->nodes;
-    P.verts = ve ? r->verts : nullptr;
-    P.edges = ve ? r->edges : nullptr;
-    P.dups = d_meta->dups;
-    check(launch_emit(P, ctx->num_sms, st), "emit");
-    tm.mark(StageTimer::kEmit, st);
-    check(cudaMemcpyAsync(&meta.top_code, d_K + koff[T], 8, cudaMemcpyDeviceToHost, st), "read top");
-    check(cudaMemcpyAsync(meta.dups, d_meta->dups, 16, cudaMemcpyDeviceToHost, st), "read dups");
-    check(cudaStreamSynchronize(st), "emit phase");
-    if (rc == SVO_OK && (T == 0 || (meta.top_code & 7) != 0))
-        rc = fail(SVO_ERR_DEGENERATE, "single top-level node with a non-zero octant: undefined in the reference");
-    if (rc == SVO_OK && ve && (meta.dups[0] || meta.dups[1])) {
-        // consecutive duplicates present (degenerate widths or absorbed
-        // coordinates): compact both arrays as thrust::unique does
-        const uint64_t nv = N * 8, ne = N * 12;
-        const uint64_t tiles = (std::max(nv, ne) + kUniqueTile - 1) / kUniqueTile;
-        uint32_t *tc = S.get<uint32_t>(tiles), *tp = S.get<uint32_t>(tiles + 1);
-        unsigned long long *ss = S.get<unsigned long long>(scan_scratch_words(tiles));
-        svo_vertex *v2 = meta.dups[0] ? pool_alloc<svo_vertex>(ctx->pool, st, nv, err) : nullptr;
-        svo_edge *e2 = meta.dups[1] ? pool_alloc<svo_edge>(ctx->pool, st, ne, err) : nullptr;
-        if (S.err != cudaSuccess || err != cudaSuccess) {
-            rc = cuda_fail(S.err != cudaSuccess ? S.err : err, "unique scratch");
-        } else {
-            uint32_t cv = 0, ce = 0;
-            if (v2) {
-                check(launch_unique_vertices(r->verts, nv, v2, tc, tp, ss, &d_meta->gp.status, st), "unique v");
-                check(cudaMemcpyAsync(&cv, tp + (nv + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost, st),
-                      "read");
-                check(cudaStreamSynchronize(st), "unique v");
+    Scratch S{ctx->pool, st};
+    StageTimer tm((flags & SVO_FLAG_TIMINGS) != 0);
+    if (n > 0) {
+        cudaError_t err = cudaSuccess;
+        // outputs, code lists, job tables
+        std::vector<CompactJob> jobs;
+        std::vector<uint64_t> word_off(1, 0);
+        std::vector<EmitParams> ep(n);
+        std::vector<uint64_t> node_off(n + 1, 0);
+        std::vector<const uint64_t *> top_ptr(n);
+        uint64_t ktot = 0;
+        std::vector<uint64_t> kbase(n);
+        for (int j = 0; j < n; ++j) {
+            const MeshHost &mh = b->m[wave[j]];
+            kbase[j] = ktot;
+            for (int l = 1; l <= mh.T; ++l) ktot += mh.totals[l];
+        }
+        uint64_t *K = S.get<uint64_t>(ktot + 1);
+        unsigned long long *dups = S.get<unsigned long long>(2 * (size_t)n);
+        uint64_t *top = S.get<uint64_t>(n);
+        if (!K || !dups || !top) return cuda_fail(S.err, "wave scratch");
+        check(cudaMemsetAsync(dups, 0, 16 * (size_t)n, st), "memset");
+        for (int j = 0; j < n; ++j) {
+            const MeshHost &mh = b->m[wave[j]];
+            const MeshDev &md = b->h_mesh[dev_k[j]];
+            svo_result *r = new svo_result();
+            res[j] = r;
+            r->device = ctx->device;
+            r->stream = st;
+            r->pool = ctx->pool;
+            r->depth = mh.T + 1;
+            for (int l = 0; l <= mh.T; ++l) r->level_counts.push_back((int64_t)mh.n_l[l]);
+            for (int a = 0; a < 3; ++a) {
+                r->bbox.min[a] = mh.gp.bbox[a];
+                r->bbox.max[a] = mh.gp.bbox[3 + a];
+                r->bbox.width[a] = mh.gp.bbox[6 + a];
+                r->unit[a] = mh.gp.unit[a];
             }
-            if (e2) {
-                check(launch_unique_edges(r->edges, ne, e2, tc, tp, ss, &d_meta->gp.status, st), "unique e");
-                check(cudaMemcpyAsync(&ce, tp + (ne + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost, st),
-                      "read");
-                check(cudaStreamSynchronize(st), "unique e");
+            r->n_nodes = mh.N;
+            r->nodes = pool_alloc<svo_node>(ctx->pool, st, mh.N, err);
+            if (ve) {
+                r->verts = pool_alloc<svo_vertex>(ctx->pool, st, mh.N * 8, err);
+                r->edges = pool_alloc<svo_edge>(ctx->pool, st, mh.N * 12, err);
+                r->n_verts = mh.N * 8;
+                r->n_edges = mh.N * 12;
             }
-            if (v2) {
-                cudaFreeAsync(r->verts, st);
-                r->verts = v2;
-                r->n_verts = cv;
+            if (want_keys) {
+                r->keys = pool_alloc<uint64_t>(ctx->pool, st, mh.totals[0], err);
+                r->n_keys = mh.totals[0];
             }
-            if (e2) {
-                cudaFreeAsync(r->edges, st);
-                r->edges = e2;
-                r->n_edges = ce;
+            if (err != cudaSuccess) break;
+            // compaction jobs: levels 1..T into K, level 0 into the keys
+            CompactJob job{};
+            job.bits = md.bits;
+            job.pre = md.pre;
+            job.py = mh.py;
+            job.l0 = 1;
+            job.l1 = mh.T + 1;
+            job.out = K + kbase[j];
+            uint64_t ko = 0;
+            for (int l = 1; l <= mh.T; ++l) {
+                job.koff[l] = ko;
+                ko += mh.totals[l];
+            }
+            jobs.push_back(job);
+            word_off.push_back(word_off.back() + mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1]);
+            if (want_keys) {
+                CompactJob k0 = job;
+                k0.l0 = 0;
+                k0.l1 = 1;
+                k0.out = r->keys;
+                std::memset(k0.koff, 0, sizeof(k0.koff));
+                jobs.push_back(k0);
+                word_off.push_back(word_off.back() + mh.py.words[0]);
+            }
+            // emission parameters
+            EmitParams &P = ep[j];
+            P.T = mh.T;
+            P.N = (uint32_t)mh.N;
+            P.flags = flags;
+            const uint32_t R = 1u << (mh.py.grid_levels - 1);
+            float w = mh.gp.unit[0];  // unitVoxelSize.x doubled per level (src/SVO.cu:351,483)
+            for (int l = 0; l <= mh.T; ++l) {
+                P.lv[l].off = (uint32_t)mh.off[l];
+                P.lv[l].n = (uint32_t)mh.n_l[l];
+                P.lv[l].K1 = job.out + (l < mh.T ? job.koff[l + 1] : job.koff[mh.T]);
+                P.lv[l].bits = md.bits + mh.py.woff[l];
+                P.lv[l].coff = mh.py.coff[l];
+                P.lv[l].side = std::max<uint32_t>(1u, R >> l);
+                P.lv[l].width = w;
+                w = w * 2.0f;
+            }
+            P.pre = md.pre;
+            P.gp = md.gp;
+            P.nodes = r->nodes;
+            P.verts = ve ? r->verts : nullptr;
+            P.edges = ve ? r->edges : nullptr;
+            P.dups = dups + 2 * j;
+            node_off[j + 1] = node_off[j] + (mh.N + 31) / 32 * 32;
+            top_ptr[j] = job.out + job.koff[mh.T];
+        }
+        if (err != cudaSuccess) {
+            for (svo_result *r : res) svo_result_free(r);
+            return cuda_fail(err, "output allocation");
+        }
+        CompactJob *d_jobs = S.get<CompactJob>(jobs.size());
+        uint64_t *d_word_off = S.get<uint64_t>(word_off.size());
+        EmitParams *d_ep = S.get<EmitParams>(n);
+        uint64_t *d_node_off = S.get<uint64_t>(n + 1);
+        const uint64_t **d_top_ptr = S.get<const uint64_t *>(n);
+        if (S.err != cudaSuccess) {
+            for (svo_result *r : res) svo_result_free(r);
+            return cuda_fail(S.err, "wave tables");
+        }
+        check(upload(d_jobs, jobs, st), "upload");
+        check(upload(d_word_off, word_off, st), "upload");
+        check(upload(d_ep, ep, st), "upload");
+        check(upload(d_node_off, node_off, st), "upload");
+        check(upload(d_top_ptr, top_ptr, st), "upload");
+        tm.mark(StageTimer::kCompact0, st);
+        check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
+        tm.mark(StageTimer::kCompact, st);
+        check(launch_emit(EmitBatch{d_ep, n, d_node_off}, node_off.back(), flags, ctx->num_sms, st), "emit");
+        tm.mark(StageTimer::kEmit, st);
+        k_gather_top<<<(n + 127) / 128, 128, 0, st>>>(d_top_ptr, n, top);
+        count_launches(1);
+        std::vector<uint64_t> h_top(n);
+        std::vector<unsigned long long> h_dups(2 * n);
+        check(cudaMemcpyAsync(h_top.data(), top, 8 * (size_t)n, cudaMemcpyDeviceToHost, st), "read top");
+        check(cudaMemcpyAsync(h_dups.data(), dups, 16 * (size_t)n, cudaMemcpyDeviceToHost, st), "read dups");
+        check(cudaStreamSynchronize(st), "emit phase");
+        for (int j = 0; j < n && rc == SVO_OK; ++j) {
+            MeshHost &mh = b->m[wave[j]];
+            svo_result *r = res[j];
+            if (mh.T == 0 || (h_top[j] & 7) != 0) {
+                mesh_error(mh, SVO_ERR_DEGENERATE,
+                           "single top-level node with a non-zero octant: undefined in the reference");
+                continue;
+            }
+            if (ve && (h_dups[2 * j] || h_dups[2 * j + 1])) {
+                // consecutive duplicates (degenerate widths or absorbed
+                // coordinates): compact both arrays as thrust::unique does
+                const uint64_t nv = mh.N * 8, ne = mh.N * 12;
+                const uint64_t tiles = (std::max(nv, ne) + kUniqueTile - 1) / kUniqueTile;
+                Scratch U{ctx->pool, st};
+                uint32_t *tc = U.get<uint32_t>(tiles), *tp = U.get<uint32_t>(tiles + 1);
+                unsigned long long *ss = U.get<unsigned long long>(scan_scratch_words(tiles));
+                uint32_t *ustat = U.get<uint32_t>(1);
+                svo_vertex *v2 = h_dups[2 * j] ? pool_alloc<svo_vertex>(ctx->pool, st, nv, err) : nullptr;
+                svo_edge *e2 = h_dups[2 * j + 1] ? pool_alloc<svo_edge>(ctx->pool, st, ne, err) : nullptr;
+                if (U.err != cudaSuccess || err != cudaSuccess) {
+                    rc = cuda_fail(U.err != cudaSuccess ? U.err : err, "unique scratch");
+                    break;
+                }
+                check(cudaMemsetAsync(ustat, 0, 4, st), "memset");
+                uint32_t cv = 0, ce = 0;
+                if (v2) {
+                    check(launch_unique_vertices(r->verts, nv, v2, tc, tp, ss, ustat, st), "unique v");
+                    check(cudaMemcpyAsync(&cv, tp + (nv + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost,
+                                          st), "read");
+                    check(cudaStreamSynchronize(st), "unique v");
+                }
+                if (e2) {
+                    check(launch_unique_edges(r->edges, ne, e2, tc, tp, ss, ustat, st), "unique e");
+                    check(cudaMemcpyAsync(&ce, tp + (ne + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost,
+                                          st), "read");
+                    check(cudaStreamSynchronize(st), "unique e");
+                }
+                if (v2) {
+                    cudaFreeAsync(r->verts, st);
+                    r->verts = v2;
+                    r->n_verts = cv;
+                }
+                if (e2) {
+                    cudaFreeAsync(r->edges, st);
+                    r->edges = e2;
+                    r->n_edges = ce;
+                }
             }
         }
+        tm.mark(StageTimer::kUnique, st);
+        for (int j = 0; j < n && rc == SVO_OK; ++j) {
+            MeshHost &mh = b->m[wave[j]];
+            if (mh.status != SVO_OK || !(flags & SVO_FLAG_DEDUP)) continue;
+            const int drc = build_dedup(ctx->pool, st, ep[j], d_ep + j, res[j]->n_dedup, res[j]->dedup, ctx->num_sms);
+            if (drc != SVO_OK) mesh_error(mh, drc, svo_last_error());
+        }
+        tm.mark(StageTimer::kDedup, st);
+        if (tm.on) cudaEventSynchronize(tm.ev[StageTimer::kDedup]);
     }
-    tm.mark(StageTimer::kUnique, st);
-    if (rc == SVO_OK && (flags & SVO_FLAG_DEDUP)) rc = build_dedup(ctx->pool, st, P, r->n_dedup, r->dedup, ctx->num_sms);
-    tm.mark(StageTimer::kDedup, st);
-    if (rc == SVO_OK) tm.store(r);
-    S.release();
+    int first_err = rc;
+    for (int j = 0; j < n; ++j) {
+        MeshHost &mh = b->m[wave[j]];
+        if (rc != SVO_OK && mh.status == SVO_OK) mesh_error(mh, rc, svo_last_error());
+        if (mh.status == SVO_OK) {
+            mh.emitted = true;
+            svo_result *r = res[j];
+            if (tm.on && b->timed) {
+                r->n_timings = 9;
+                r->timings[1] = b->timings_a[1];
+                r->timings[2] = b->timings_a[2];
+                r->timings[3] = b->timings_a[3];
+                r->timings[4] = b->timings_a[4];
+                r->timings[5] = tm.span(StageTimer::kCompact0, StageTimer::kCompact);
+                r->timings[6] = tm.span(StageTimer::kCompact, StageTimer::kEmit);
+                r->timings[7] = tm.span(StageTimer::kEmit, StageTimer::kUnique);
+                r->timings[8] = tm.span(StageTimer::kUnique, StageTimer::kDedup);
+                r->timings[0] = b->timings_a[0] + tm.span(StageTimer::kCompact0, StageTimer::kDedup);
+            }
+            out[wave[j] - first] = r;
+        } else {
+            svo_result_free(res[j]);
+        }
+    }
+    for (int i = first; i < first + count; ++i) {
+        if (status_out) status_out[i - first] = b->m[i].status;
+        if (b->m[i].status != SVO_OK && first_err == SVO_OK) first_err = b->m[i].status;
+    }
+    if (first_err != SVO_OK) {
+        for (int i = first; i < first + count; ++i)
+            if (b->m[i].status != SVO_OK) {
+                g_err = b->m[i].error;
+                break;
+            }
+    }
+    return first_err;
+}
+
+int batch_create(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, cudaStream_t st,
+                 svo_batch **out) {
+    svo_batch *b = new svo_batch();
+    b->ctx = ctx;
+    b->st = st;
+    b->flags = flags;
+    b->m.resize(n);
+    for (int i = 0; i < n; ++i) {
+        MeshHost &mh = b->m[i];
+        mh.h_pts = descs[i].points;
+        mh.n_pts = descs[i].n_points;
+        mh.h_tris = descs[i].tris;
+        mh.n_tris = descs[i].tris ? descs[i].n_tris : 0;
+        for (int a = 0; a < 3; ++a) mh.res[a] = descs[i].res[a];
+    }
+    const int rc = batch_phase_a(b);
     if (rc != SVO_OK) {
-        svo_result_free(r);
+        batch_release(b);
+        cudaStreamSynchronize(st);
+        delete b;
         return rc;
     }
-    *out = r;
+    *out = b;
     return SVO_OK;
+}
+
+void batch_destroy(svo_batch *b) {
+    if (!b) return;
+    cudaSetDevice(b->ctx->device);
+    batch_release(b);
+    cudaStreamSynchronize(b->st);
+    delete b;
 }
 
 }  // namespace
@@ -450,23 +821,90 @@ int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t) {
 int svo_build(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t *tris, int64_t n_tris,
               int res_x, int res_y, int res_z, uint32_t flags, void *stream, svo_result **out) {
     if (!ctx || !out) return fail(SVO_ERR_INVALID_ARGUMENT, "null context or output");
-    return build_one(ctx, points, n_points, tris, n_tris, res_x, res_y, res_z, flags,
-                     static_cast<cudaStream_t>(stream), out);
+    *out = nullptr;
+    svo_mesh_desc d{points, n_points, tris, n_tris, {res_x, res_y, res_z}, flags};
+    svo_batch *b = nullptr;
+    int rc = batch_create(ctx, &d, 1, flags, static_cast<cudaStream_t>(stream), &b);
+    if (rc != SVO_OK) return rc;
+    int st = SVO_OK;
+    rc = batch_phase_b(b, 0, 1, out, &st);
+    const std::string msg = g_err;
+    batch_destroy(b);
+    g_err = msg;
+    return rc != SVO_OK ? rc : st;
 }
 
 int svo_build_batch(svo_ctx *ctx, const svo_mesh_desc *descs, int n, void *stream, svo_result **out,
                     int *status_out) {
     if (!ctx || (!descs && n > 0) || !out) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    // one batch per distinct flags value (the kernels are specialised on them)
+    std::vector<uint32_t> kinds;
+    for (int i = 0; i < n; ++i)
+        if (std::find(kinds.begin(), kinds.end(), descs[i].flags) == kinds.end()) kinds.push_back(descs[i].flags);
     int first = SVO_OK;
-    for (int i = 0; i < n; ++i) {
-        const svo_mesh_desc &d = descs[i];
-        int rc = build_one(ctx, d.points, d.n_points, d.tris, d.n_tris, d.res[0], d.res[1], d.res[2], d.flags,
-                           static_cast<cudaStream_t>(stream), &out[i]);
-        if (status_out) status_out[i] = rc;
-        if (rc != SVO_OK && first == SVO_OK) first = rc;
+    std::string first_msg;
+    for (uint32_t f : kinds) {
+        std::vector<int> idx;
+        std::vector<svo_mesh_desc> sub;
+        for (int i = 0; i < n; ++i)
+            if (descs[i].flags == f) {
+                idx.push_back(i);
+                sub.push_back(descs[i]);
+            }
+        svo_batch *b = nullptr;
+        int rc = batch_create(ctx, sub.data(), (int)sub.size(), f, static_cast<cudaStream_t>(stream), &b);
+        std::vector<svo_result *> r(sub.size(), nullptr);
+        std::vector<int> st(sub.size(), rc);
+        if (rc == SVO_OK) {
+            rc = batch_phase_b(b, 0, (int)sub.size(), r.data(), st.data());
+            const std::string msg = g_err;
+            batch_destroy(b);
+            g_err = msg;
+        }
+        for (size_t k = 0; k < sub.size(); ++k) {
+            out[idx[k]] = r[k];
+            if (status_out) status_out[idx[k]] = st[k];
+        }
+        if (rc != SVO_OK && first == SVO_OK) {
+            first = rc;
+            first_msg = g_err;
+        }
     }
+    if (first != SVO_OK) g_err = first_msg;
     return first;
 }
+
+int svo_batch_create(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, void *stream,
+                     svo_batch **out) {
+    if (!ctx || (!descs && n > 0) || !out) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    return batch_create(ctx, descs, n, flags, static_cast<cudaStream_t>(stream), out);
+}
+
+int svo_batch_size(const svo_batch *b) { return b ? (int)b->m.size() : 0; }
+
+int svo_batch_mesh_status(const svo_batch *b, int i) {
+    if (!b || i < 0 || i >= (int)b->m.size()) return SVO_ERR_INVALID_ARGUMENT;
+    return b->m[i].status;
+}
+
+int64_t svo_batch_mesh_nodes(const svo_batch *b, int i) {
+    if (!b || i < 0 || i >= (int)b->m.size() || b->m[i].status != SVO_OK) return -1;
+    return (int64_t)b->m[i].N;
+}
+
+int64_t svo_batch_mesh_output_bytes(const svo_batch *b, int i) {
+    if (!b || i < 0 || i >= (int)b->m.size() || b->m[i].status != SVO_OK) return -1;
+    return (int64_t)output_bytes(b->m[i], b->flags);
+}
+
+int svo_batch_emit(svo_batch *b, int first, int count, svo_result **out, int *status_out) {
+    if (!b || !out || first < 0 || count < 0 || first + count > (int)b->m.size())
+        return fail(SVO_ERR_INVALID_ARGUMENT, "bad batch range");
+    return batch_phase_b(b, first, count, out, status_out);
+}
+
+void svo_batch_free(svo_batch *b) { batch_destroy(b); }
 
 void svo_result_free(svo_result *r) {
     if (!r) return;

@@ -3,7 +3,8 @@
 
 namespace svo {
 
-int build_dedup(cudaMemPool_t, cudaStream_t, const EmitParams &, uint64_t n_out[3], uint64_t *out[3], int) {
+int build_dedup(cudaMemPool_t, cudaStream_t, const EmitParams &, const EmitParams *, uint64_t n_out[3], uint64_t *out[3],
+                int) {
     for (int k = 0; k < 3; ++k) {
         n_out[k] = 0;
         out[k] = nullptr;

@@ -39,6 +39,34 @@ struct Pyramid {
 
 Pyramid make_pyramid(int rx, int ry, int rz);
 
+// One mesh of a batch, as the kernels see it (an array in device memory).
+// A single build is a batch of one.
+struct MeshDev {
+    const float *pts;        // device
+    const int32_t *tris;     // device; null = soup (3 points per triangle)
+    int64_t n_pts;
+    int64_t n_tris;
+    int res[3];
+    int pad_;
+    GridParams *gp;
+    uint32_t *mm;            // bbox scratch (6 u32)
+    uint64_t *bits;          // this mesh's pyramid (level l at bits + py.woff[l])
+    uint32_t *cnt;           // this mesh's block counts (level l at cnt + py.coff[l])
+    uint32_t *pre;           // exclusive prefix at this mesh's first block
+    uint32_t *totals;        // set bits per level (kMaxLevels)
+    uint32_t *done;          // pyramid CTAs finished
+    Pyramid py;
+};
+
+// Prefix tables over the meshes of a batch (device memory, n + 1 entries).
+struct BatchDev {
+    const MeshDev *mesh;
+    int n;
+    const uint64_t *tri_off;   // global index of each mesh's first triangle
+    const uint32_t *cta_off;   // first pyramid CTA of each mesh
+    const uint32_t *bbox_off;  // first bbox-reduction block of each mesh
+};
+
 // Per-level inputs of the node emission kernel.
 struct EmitLevel {
     uint32_t off;          // first node index of the level
@@ -50,12 +78,13 @@ struct EmitLevel {
     float width;           // node width
 };
 
+// One mesh of an emission pass (an array in device memory).
 struct EmitParams {
     int T;                  // top level index (depth - 1)
     uint32_t N;             // total nodes
     uint32_t flags;
     EmitLevel lv[kMaxLevels];
-    const uint32_t *pre;    // exclusive prefix of the block counts
+    const uint32_t *pre;    // exclusive prefix of the block counts (this mesh's base)
     const GridParams *gp;
     svo_node *nodes;
     svo_vertex *verts;      // may be null (SVO_FLAG_NO_VERT_EDGE)
@@ -63,29 +92,59 @@ struct EmitParams {
     unsigned long long *dups;  // [0] vertex, [1] edge consecutive duplicates
 };
 
-cudaError_t launch_bbox(const float *pts, int64_t n, int rx, int ry, int rz, uint32_t *mm_scratch,
-                        GridParams *gp, cudaStream_t st);
+// The meshes of one emission pass: mesh i owns global node slots
+// [node_off[i], node_off[i] + N_i), node_off[i] a multiple of 32 (a warp never
+// straddles two meshes).
+struct EmitBatch {
+    const EmitParams *p;
+    int n;
+    const uint64_t *node_off;  // n + 1 entries
+};
+
+// One compaction job: the set bits of levels [l0, l1) of one mesh, level l
+// written to out + koff[l]; jobs own consecutive ranges of a global word
+// index (word_off, n + 1 entries).
+struct CompactJob {
+    const uint64_t *bits;
+    const uint32_t *pre;
+    Pyramid py;
+    int l0, l1;
+    uint64_t *out;
+    uint64_t koff[kMaxLevels];
+};
+struct CompactBatch {
+    const CompactJob *job;
+    int n;
+    const uint64_t *word_off;
+};
+
+// Binary search: the i with off[i] <= x < off[i + 1] (off has n + 1 entries).
+template <class T>
+__host__ __device__ __forceinline__ int find_segment(const T *off, int n, T x) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (off[mid] <= x) lo = mid; else hi = mid - 1;
+    }
+    return lo;
+}
+
+cudaError_t launch_bbox(const BatchDev &b, uint32_t total_blocks, cudaStream_t st);
 // mm[0] = min, mm[1] = max of n int32 indices.
 cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaStream_t st);
-cudaError_t launch_voxelize(const float *pts, const int32_t *tris, int64_t nt, const GridParams *gp,
-                            int rx, int ry, int rz, bool strict, uint32_t *bm, const VoxTuning &tune,
-                            uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms,
-                            cudaStream_t st);
-// Builds levels 1.. of the pyramid and the per-block counts.
-cudaError_t launch_pyramid(const Pyramid &py, uint64_t *bits, uint32_t *cnt, uint32_t *done,
-                           cudaStream_t st);
+cudaError_t launch_voxelize(const BatchDev &b, int64_t total_tris, bool strict, const VoxTuning &tune,
+                            uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st);
+// Builds levels 1.. of every mesh's pyramid and the per-block counts.
+cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, cudaStream_t st);
 // Exclusive scan of n u32 values; out has n + 1 entries (out[n] = total).
 // scratch: >= scan_scratch_words(n) u64 words, zeroed by the call.
 size_t scan_scratch_words(uint64_t n);
 cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned long long *scratch,
                         uint32_t *status, cudaStream_t st);
-// Level totals C_l = pre[coff[l+1]] - pre[coff[l]] into totals[l].
-cudaError_t launch_level_totals(const Pyramid &py, const uint32_t *pre, uint32_t *totals,
-                                cudaStream_t st);
-// Sorted codes of levels [l0, l1): out + koff[l] receives level l's codes.
-cudaError_t launch_compact(const Pyramid &py, const uint64_t *bits, const uint32_t *pre, int l0,
-                           int l1, uint64_t *out, const uint64_t *koff, cudaStream_t st);
-cudaError_t launch_emit(const EmitParams &p, int num_sms, cudaStream_t st);
+// totals of every (mesh, level).
+cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st);
+cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st);
+cudaError_t launch_emit(const EmitBatch &b, uint64_t total_nodes, uint32_t flags, int num_sms, cudaStream_t st);
 // Stable removal of consecutive duplicates (thrust::unique semantics).
 cudaError_t launch_unique_vertices(const svo_vertex *in, uint64_t n, svo_vertex *out,
                                    uint32_t *tile_counts, uint32_t *tile_pre,
@@ -97,7 +156,12 @@ cudaError_t launch_unique_edges(const svo_edge *in, uint64_t n, svo_edge *out, u
 constexpr uint32_t kUniqueTile = 4096;
 
 // Morton-keyed unique vertex/edge/face keys of all nodes (SVO_FLAG_DEDUP).
-int build_dedup(cudaMemPool_t pool, cudaStream_t st, const EmitParams &p, uint64_t n_out[3], uint64_t *out[3],
-                int num_sms);
+int build_dedup(cudaMemPool_t pool, cudaStream_t st, const EmitParams &p, const EmitParams *p_dev,
+                uint64_t n_out[3], uint64_t *out[3], int num_sms);
+
+// Blocks of the bbox reduction for a mesh of n points.
+inline uint32_t bbox_blocks(int64_t n) {
+    return (uint32_t)std::max<int64_t>(1, std::min<int64_t>((n / 4 + 255) / 256, 148 * 4));
+}
 
 }  // namespace svo

@@ -117,8 +117,14 @@ extern "C" int svo_voxelize_keys_noalloc(const float *points, int64_t n_points, 
     uint32_t *mm = c.take<uint32_t>(8);
     int32_t *imm = c.take<int32_t>(2);
     uint32_t *totals = c.take<uint32_t>(kMaxLevels);
-    uint32_t *counters = c.take<uint32_t>(2);
+    uint32_t *counters = c.take<uint32_t>(4);
     uint32_t *done = c.take<uint32_t>(1);
+    MeshDev *d_mesh = c.take<MeshDev>(1);
+    uint64_t *d_tri_off = c.take<uint64_t>(2);
+    uint32_t *d_cta_off = c.take<uint32_t>(2);
+    uint32_t *d_bbox_off = c.take<uint32_t>(2);
+    CompactJob *d_job = c.take<CompactJob>(1);
+    uint64_t *d_word_off = c.take<uint64_t>(2);
     uint64_t *bits = c.take<uint64_t>(py.total_words);
     uint32_t *cnt = c.take<uint32_t>(py.total_blocks);
     uint32_t *pre = c.take<uint32_t>(py.total_blocks + 1);
@@ -135,18 +141,44 @@ extern "C" int svo_voxelize_keys_noalloc(const float *points, int64_t n_points, 
         if ((rc = cuda(cudaStreamSynchronize(st)))) return rc;
         if (h[0] < 0 || h[1] >= n_points) return noalloc_fail(SVO_ERR_INVALID_ARGUMENT, "triangle index out of range");
     }
+    // the one-mesh tables, copied from the host stack (no device allocation)
+    MeshDev md{};
+    md.pts = points;
+    md.tris = tris;
+    md.n_pts = n_points;
+    md.n_tris = nt;
+    md.res[0] = res_x;
+    md.res[1] = res_y;
+    md.res[2] = res_z;
+    md.gp = gp;
+    md.mm = mm;
+    md.bits = bits;
+    md.cnt = cnt;
+    md.pre = pre;
+    md.totals = totals;
+    md.done = done;
+    md.py = py;
+    const uint64_t h_tri_off[2] = {0, (uint64_t)nt};
+    const uint32_t h_cta_off[2] = {0, py.ctas};
+    const uint32_t h_bbox_off[2] = {0, bbox_blocks(n_points)};
     // everything that must start at zero (the array keeps the last call's data)
     if ((rc = cuda(cudaMemsetAsync(base, 0, c.used, st)))) return rc;
-    if ((rc = cuda(launch_bbox(points, n_points, res_x, res_y, res_z, mm, gp, st)))) return rc;
+    const uint32_t mm_init[6] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu, 0u, 0u, 0u};
+    if ((rc = cuda(cudaMemcpyAsync(mm, mm_init, sizeof(mm_init), cudaMemcpyHostToDevice, st)))) return rc;
+    if ((rc = cuda(cudaMemcpyAsync(d_mesh, &md, sizeof(md), cudaMemcpyHostToDevice, st)))) return rc;
+    if ((rc = cuda(cudaMemcpyAsync(d_tri_off, h_tri_off, sizeof(h_tri_off), cudaMemcpyHostToDevice, st)))) return rc;
+    if ((rc = cuda(cudaMemcpyAsync(d_cta_off, h_cta_off, sizeof(h_cta_off), cudaMemcpyHostToDevice, st)))) return rc;
+    if ((rc = cuda(cudaMemcpyAsync(d_bbox_off, h_bbox_off, sizeof(h_bbox_off), cudaMemcpyHostToDevice, st)))) return rc;
+    const BatchDev bd{d_mesh, 1, d_tri_off, d_cta_off, d_bbox_off};
+    if ((rc = cuda(launch_bbox(bd, h_bbox_off[1], st)))) return rc;
     VoxTuning tune;
     tune.warp_max = 0xFFFFFFFFu;  // no big-triangle queue: warps take every large triangle
-    if ((rc = cuda(launch_voxelize(points, tris, nt, gp, res_x, res_y, res_z, (flags & SVO_FLAG_STRICT_FP) != 0,
-                                   reinterpret_cast<uint32_t *>(bits), tune, nullptr, 0, counters,
+    if ((rc = cuda(launch_voxelize(bd, nt, (flags & SVO_FLAG_STRICT_FP) != 0, tune, nullptr, 0, counters,
                                    prop.multiProcessorCount, st))))
         return rc;
-    if ((rc = cuda(launch_pyramid(py, bits, cnt, done, st)))) return rc;
+    if ((rc = cuda(launch_pyramid(bd, py.ctas, st)))) return rc;
     if ((rc = cuda(launch_scan(cnt, pre, py.total_blocks, scan, &gp->status, st)))) return rc;
-    if ((rc = cuda(launch_level_totals(py, pre, totals, st)))) return rc;
+    if ((rc = cuda(launch_level_totals(bd, st)))) return rc;
     uint32_t h_tot = 0, h_status = 0;
     if ((rc = cuda(cudaMemcpyAsync(&h_tot, totals, 4, cudaMemcpyDeviceToHost, st)))) return rc;
     if ((rc = cuda(cudaMemcpyAsync(&h_status, &gp->status, 4, cudaMemcpyDeviceToHost, st)))) return rc;
@@ -155,7 +187,16 @@ extern "C" int svo_voxelize_keys_noalloc(const float *points, int64_t n_points, 
     if (h_status & kStatusScanTimeout) return noalloc_fail(SVO_ERR_DEVICE_TIMEOUT, "scan look-back timed out");
     *n_keys = h_tot;
     if ((int64_t)h_tot > keys_cap) return noalloc_fail(SVO_ERR_INVALID_ARGUMENT, "keys buffer too small (see *n_keys)");
-    uint64_t koff[kMaxLevels] = {};
-    if ((rc = cuda(launch_compact(py, bits, pre, 0, 1, keys, koff, st)))) return rc;
+    CompactJob job{};
+    job.bits = bits;
+    job.pre = pre;
+    job.py = py;
+    job.l0 = 0;
+    job.l1 = 1;
+    job.out = keys;
+    const uint64_t h_word_off[2] = {0, py.words[0]};
+    if ((rc = cuda(cudaMemcpyAsync(d_job, &job, sizeof(job), cudaMemcpyHostToDevice, st)))) return rc;
+    if ((rc = cuda(cudaMemcpyAsync(d_word_off, h_word_off, sizeof(h_word_off), cudaMemcpyHostToDevice, st)))) return rc;
+    if ((rc = cuda(launch_compact(CompactBatch{d_job, 1, d_word_off}, py.words[0], st)))) return rc;
     return cuda(cudaStreamSynchronize(st));
 }

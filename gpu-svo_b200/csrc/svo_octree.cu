@@ -67,13 +67,19 @@ __device__ __forceinline__ uint32_t nz_bytes(uint64_t v) {
 
 // Levels 1..4 per CTA (a CTA owns 2048 words of level 0), then the last CTA
 // to finish builds the remaining levels.
-__global__ void __launch_bounds__(256) k_pyramid(Pyramid py, uint64_t *__restrict__ bits,
-                                                 uint32_t *__restrict__ cnt, uint32_t *__restrict__ done) {
+__global__ void __launch_bounds__(256) k_pyramid(BatchDev bd) {
     __shared__ uint64_t s1[256];
     __shared__ uint64_t s2[32];
     __shared__ uint64_t s3[4];
     __shared__ bool s_last;
-    const uint32_t b = blockIdx.x, t = threadIdx.x;
+    const int m = find_segment(bd.cta_off, bd.n, (uint32_t)blockIdx.x);
+    const MeshDev &md = bd.mesh[m];
+    const Pyramid &py = md.py;
+    uint64_t *__restrict__ bits = md.bits;
+    uint32_t *__restrict__ cnt = md.cnt;
+    uint32_t *__restrict__ done = md.done;
+    const uint32_t nctas = bd.cta_off[m + 1] - bd.cta_off[m];
+    const uint32_t b = blockIdx.x - bd.cta_off[m], t = threadIdx.x;
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(bits + py.woff[0] + (uint64_t)b * 2048 + t * 8);
         uint64_t w1 = 0;
@@ -131,7 +137,7 @@ __global__ void __launch_bounds__(256) k_pyramid(Pyramid py, uint64_t *__restric
     }
     __threadfence();
     __syncthreads();
-    if (t == 0) s_last = atomicAdd(done, 1u) == gridDim.x - 1;
+    if (t == 0) s_last = atomicAdd(done, 1u) == nctas - 1;
     __syncthreads();
     if (!s_last) return;
     __threadfence();
@@ -258,32 +264,33 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restric
     if (tile == last_tile && t == kScanThreads - 1) out[n] = s_prefix + aggregate;
 }
 
-__global__ void k_level_totals(Pyramid py, const uint32_t *__restrict__ pre, uint32_t *__restrict__ totals) {
-    const int l = threadIdx.x;
-    if (l < py.levels) totals[l] = pre[py.coff[l + 1]] - pre[py.coff[l]];
+__global__ void k_level_totals(BatchDev bd) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int m = i / kMaxLevels, l = i % kMaxLevels;
+    if (m >= bd.n) return;
+    const MeshDev &md = bd.mesh[m];
+    if (l < md.py.levels) md.totals[l] = md.pre[md.py.coff[l + 1]] - md.pre[md.py.coff[l]];
 }
 
-struct KOff {
-    uint64_t v[kMaxLevels];
-};
-
-// One thread per 64-bit word of levels [l0, l1): its first rank is the
+// One thread per 64-bit word of every job's levels: its first rank is the
 // block prefix plus the popcounts of the preceding words of its block.
-__global__ void __launch_bounds__(256) k_compact(Pyramid py, const uint64_t *__restrict__ bits,
-                                                 const uint32_t *__restrict__ pre, int l0, int l1,
-                                                 uint64_t *__restrict__ out, KOff koff) {
-    const uint64_t gw = py.woff[l0] + blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (gw >= py.woff[l1 - 1] + py.words[l1 - 1]) return;
-    int l = l0;
-    while (l + 1 < l1 && gw >= py.woff[l + 1]) ++l;
-    uint64_t v = bits[gw];
+__global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total) {
+    const uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (gi >= total) return;
+    const int j = find_segment(cb.word_off, cb.n, gi);
+    const CompactJob &job = cb.job[j];
+    const Pyramid &py = job.py;
+    const uint64_t gw = py.woff[job.l0] + (gi - cb.word_off[j]);
+    int l = job.l0;
+    while (l + 1 < job.l1 && gw >= py.woff[l + 1]) ++l;
+    uint64_t v = job.bits[gw];
     if (!v) return;
     const uint64_t w = gw - py.woff[l];
     const uint64_t blk = w >> 3;
-    uint64_t r = pre[py.coff[l] + blk] - pre[py.coff[l]];
-    const uint64_t *bw = bits + py.woff[l] + blk * 8;
+    uint64_t r = job.pre[py.coff[l] + blk] - job.pre[py.coff[l]];
+    const uint64_t *bw = job.bits + py.woff[l] + blk * 8;
     for (int k = 0; k < (int)(w & 7); ++k) r += __popcll(bw[k]);
-    uint64_t *o = out + koff.v[l] + r;
+    uint64_t *o = job.out + job.koff[l] + r;
     const uint64_t base = w * 64;
     while (v) {
         *o++ = base + __ffsll((long long)v) - 1;
@@ -391,14 +398,18 @@ constexpr int kEmitWarps = 4;
 constexpr int kEmitBufBytes = 32 * 336;  // per warp
 
 template <bool S, bool FULL, bool VE>
-__global__ void __launch_bounds__(kEmitWarps * 32) k_emit(EmitParams P) {
+__global__ void __launch_bounds__(kEmitWarps * 32) k_emit(EmitBatch eb, uint64_t total) {
     extern __shared__ uint4 smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint4 *wbuf = smem + warp * (kEmitBufBytes / 16);
-    const float go[3] = {P.gp->origin[0], P.gp->origin[1], P.gp->origin[2]};
     const uint64_t nwarps = (uint64_t)gridDim.x * kEmitWarps;
-    unsigned long long vdup = 0, edup = 0;
-    for (uint64_t base = ((uint64_t)blockIdx.x * kEmitWarps + warp) * 32; base < P.N; base += nwarps * 32) {
+    for (uint64_t gbase = ((uint64_t)blockIdx.x * kEmitWarps + warp) * 32; gbase < total; gbase += nwarps * 32) {
+        const int mj = find_segment(eb.node_off, eb.n, gbase);
+        const EmitParams &P = eb.p[mj];
+        const uint64_t base = gbase - eb.node_off[mj];
+        if (base >= P.N) continue;  // padding between meshes
+        const float go[3] = {P.gp->origin[0], P.gp->origin[1], P.gp->origin[2]};
+        unsigned long long vdup = 0, edup = 0;
         const uint32_t t = (uint32_t)(base + lane);
         const bool valid = base + lane < P.N;
         const uint32_t cnt = (uint32_t)(P.N - base < 32 ? P.N - base : 32);
@@ -570,8 +581,6 @@ __global__ void __launch_bounds__(kEmitWarps * 32) k_emit(EmitParams P) {
         __syncwarp();
         warp_copy_out(wbuf, reinterpret_cast<char *>(P.edges) + base * 336, cnt * 336, lane);
         __syncwarp();
-    }
-    if (VE) {
 #pragma unroll
         for (int d = 16; d > 0; d >>= 1) {
             vdup += __shfl_xor_sync(0xFFFFFFFFu, vdup, d);
@@ -651,8 +660,8 @@ cudaError_t unique_impl(const T *in, uint64_t n, T *out, uint32_t *tile_counts, 
 
 }  // namespace
 
-cudaError_t launch_pyramid(const Pyramid &py, uint64_t *bits, uint32_t *cnt, uint32_t *done, cudaStream_t st) {
-    k_pyramid<<<py.ctas, 256, 0, st>>>(py, bits, cnt, done);
+cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, cudaStream_t st) {
+    k_pyramid<<<total_ctas, 256, 0, st>>>(b);
     count_launches(1);
     return cudaGetLastError();
 }
@@ -670,32 +679,29 @@ cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned 
     return cudaGetLastError();
 }
 
-cudaError_t launch_level_totals(const Pyramid &py, const uint32_t *pre, uint32_t *totals, cudaStream_t st) {
-    k_level_totals<<<1, 32, 0, st>>>(py, pre, totals);
+cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st) {
+    const int n = b.n * kMaxLevels;
+    k_level_totals<<<(n + 127) / 128, 128, 0, st>>>(b);
     count_launches(1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_compact(const Pyramid &py, const uint64_t *bits, const uint32_t *pre, int l0, int l1,
-                           uint64_t *out, const uint64_t *koff, cudaStream_t st) {
-    const uint64_t nw = py.woff[l1 - 1] + py.words[l1 - 1] - py.woff[l0];
-    if (nw == 0) return cudaSuccess;
-    KOff k;
-    for (int l = 0; l < kMaxLevels; ++l) k.v[l] = koff[l];
-    k_compact<<<(unsigned)((nw + 255) / 256), 256, 0, st>>>(py, bits, pre, l0, l1, out, k);
+cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st) {
+    if (total_words == 0) return cudaSuccess;
+    k_compact<<<(unsigned)((total_words + 255) / 256), 256, 0, st>>>(c, total_words);
     count_launches(1);
     return cudaGetLastError();
 }
 
-cudaError_t launch_emit(const EmitParams &p, int num_sms, cudaStream_t st) {
-    if (p.N == 0) return cudaSuccess;
-    const uint64_t warps = (p.N + 31) / 32;
+cudaError_t launch_emit(const EmitBatch &b, uint64_t total, uint32_t flags, int num_sms, cudaStream_t st) {
+    if (total == 0) return cudaSuccess;
+    const uint64_t warps = (total + 31) / 32;
     const unsigned blocks = (unsigned)std::max<uint64_t>(
         1, std::min<uint64_t>((warps + kEmitWarps - 1) / kEmitWarps, (uint64_t)num_sms * 12));
     const size_t shmem = (size_t)kEmitWarps * kEmitBufBytes;
-    const bool s = (p.flags & SVO_FLAG_STRICT_FP) != 0, f = (p.flags & SVO_FLAG_FULL_NEIGHBORS) != 0,
-               ve = p.verts != nullptr;
-#define SVO_EMIT(S_, F_, V_) k_emit<S_, F_, V_><<<blocks, kEmitWarps * 32, shmem, st>>>(p)
+    const bool s = (flags & SVO_FLAG_STRICT_FP) != 0, f = (flags & SVO_FLAG_FULL_NEIGHBORS) != 0,
+               ve = (flags & SVO_FLAG_NO_VERT_EDGE) == 0;
+#define SVO_EMIT(S_, F_, V_) k_emit<S_, F_, V_><<<blocks, kEmitWarps * 32, shmem, st>>>(b, total)
     if (s) {
         if (f) { if (ve) SVO_EMIT(true, true, true); else SVO_EMIT(true, true, false); }
         else { if (ve) SVO_EMIT(true, false, true); else SVO_EMIT(true, false, false); }

@@ -49,14 +49,19 @@ __device__ __forceinline__ void bbox_take(float v, int a, uint32_t lo[3], uint32
     hi[a] = max(hi[a], o);
 }
 
-// When pts is 16-byte aligned, 4 points (12 floats, 3 float4) per step; the
-// component of float k is k % 3, the same in every 12-float group.
-__global__ void k_bbox_reduce(const float *__restrict__ pts, int64_t n, uint32_t *__restrict__ mm,
-                              GridParams *__restrict__ gp) {
+// Block b belongs to mesh m = the segment of bbox_off holding b.  When the
+// mesh's points are 16-byte aligned, 4 points (12 floats, 3 float4) per step;
+// the component of float k is k % 3, the same in every 12-float group.
+__global__ void k_bbox_reduce(BatchDev bd) {
+    const int m = find_segment(bd.bbox_off, bd.n, (uint32_t)blockIdx.x);
+    const MeshDev &md = bd.mesh[m];
+    const float *__restrict__ pts = md.pts;
+    const int64_t n = md.n_pts;
     uint32_t lo[3] = {0xFFFFFFFFu, 0xFFFFFFFFu, 0xFFFFFFFFu}, hi[3] = {0u, 0u, 0u};
     bool bad = false;
-    const int64_t tid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x;
-    const int64_t nth = (int64_t)gridDim.x * blockDim.x;
+    const uint32_t nb = bd.bbox_off[m + 1] - bd.bbox_off[m];
+    const int64_t tid = (blockIdx.x - bd.bbox_off[m]) * (int64_t)blockDim.x + threadIdx.x;
+    const int64_t nth = (int64_t)nb * blockDim.x;
     int64_t done = 0;
     if ((reinterpret_cast<uintptr_t>(pts) & 15) == 0) {
         const float4 *p4 = reinterpret_cast<const float4 *>(pts);
@@ -78,12 +83,12 @@ __global__ void k_bbox_reduce(const float *__restrict__ pts, int64_t n, uint32_t
         lo[a] = __reduce_min_sync(0xFFFFFFFFu, lo[a]);
         hi[a] = __reduce_max_sync(0xFFFFFFFFu, hi[a]);
     }
-    if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) atomicOr(&gp->status, kStatusNonFinite);
+    if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) atomicOr(&md.gp->status, kStatusNonFinite);
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            atomicMin(mm + a, lo[a]);
-            atomicMax(mm + 3 + a, hi[a]);
+            atomicMin(md.mm + a, lo[a]);
+            atomicMax(md.mm + 3 + a, hi[a]);
         }
     }
 }
@@ -91,9 +96,13 @@ __global__ void k_bbox_reduce(const float *__restrict__ pts, int64_t n, uint32_t
 // createMeshBBCube (src/BaseModel.h:24-49) and unitVoxelSize
 // (src/SVO.cu:348-350).  Host code in the reference: no contraction there, so
 // every operation is an explicitly rounded intrinsic.
-__global__ void k_grid_setup(const uint32_t *__restrict__ mm, int rx, int ry, int rz,
-                             GridParams *__restrict__ gp) {
-    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+__global__ void k_grid_setup(BatchDev bd) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= bd.n) return;
+    const MeshDev &md = bd.mesh[m];
+    const uint32_t *mm = md.mm;
+    GridParams *gp = md.gp;
+    const int rx = md.res[0], ry = md.res[1], rz = md.res[2];
     float mn[3], mx[3], len[3], amin[3], amax[3];
     for (int a = 0; a < 3; ++a) {
         mn[a] = ord2f(mm[a]);
@@ -470,47 +479,46 @@ __device__ __forceinline__ void shfl_tri(Tri &dst, const Tri &src, int lane) {
     for (int i = 0; i < (int)(sizeof(Tri) / 4); ++i) d[i] = __shfl_sync(0xFFFFFFFFu, s[i], lane);
 }
 
-// One thread per triangle: setup, then either its own serial test
-// (grid bbox <= serial_max voxels) or queue entries of <= warp_max bricks.  INPLACE (no queue given): the triangle's warp walks its bricks
-// right here instead.
+// One thread per triangle of the batch (global index -> mesh by tri_off):
+// setup, then either its own serial test (grid bbox <= serial_max voxels) or
+// queue entries of <= warp_max bricks.  INPLACE (no queue given): the
+// triangle's warp walks its bricks right here instead.
 template <bool S, bool INPLACE>
-__global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(const float *__restrict__ pts,
-                                                     const int32_t *__restrict__ tris, int64_t nt,
-                                                     const GridParams *__restrict__ gpp, int rx, int ry,
-                                                     int rz, uint32_t *__restrict__ bm, VoxTuning tune,
-                                                     uint4 *__restrict__ big, uint32_t big_cap,
-                                                     uint32_t *__restrict__ big_count) {
-    const GridParams g = *gpp;
-    const int res[3] = {rx, ry, rz};
+__global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(BatchDev bd, int64_t total, VoxTuning tune,
+                                                                    uint4 *__restrict__ big, uint32_t big_cap,
+                                                                    uint32_t *__restrict__ big_count) {
     const int lane = threadIdx.x & 31;
     const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
-    HitSink sink{bm};
-    for (int64_t base = warp0; base < nt; base += stride) {
-        const int64_t tid = base + lane;
+    for (int64_t base = warp0; base < total; base += stride) {
+        const int64_t gid = base + lane;
         Tri t;
         uint32_t nb = 0;
-        int tier = -1;
-        if (tid < nt) {
+        int tier = -1, m = 0;
+        if (gid < total) {
+            m = find_segment(bd.tri_off, bd.n, (uint64_t)gid);
+            const MeshDev &md = bd.mesh[m];
+            const GridParams g = *md.gp;
             float p[3][3];
-            load_tri(pts, tris, tid, p);
-            tri_setup<S>(g, res, p[0], p[1], p[2], t);
+            load_tri(md.pts, md.tris, gid - (int64_t)bd.tri_off[m], p);
+            tri_setup<S>(g, md.res, p[0], p[1], p[2], t);
             const uint64_t vol = (uint64_t)(t.hi[0] - t.lo[0] + 1) * (uint64_t)(t.hi[1] - t.lo[1] + 1) *
                                  (uint64_t)(t.hi[2] - t.lo[2] + 1);
             nb = brick_count(t);
             tier = vol <= (uint64_t)tune.serial_max ? 0 : 1;
-        }
-        if (tier == 0) {
-            for (int z = t.lo[2]; z <= t.hi[2]; ++z)
-                for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
-            sink.flush();
-        } else if (!INPLACE && tier == 1) {
-            const uint32_t eb = tune.warp_max;
-            const uint32_t ne = (nb + eb - 1) / eb;
-            const uint32_t at = atomicAdd(big_count, ne);
-            if (at + ne <= big_cap) {
-                for (uint32_t e = 0; e < ne; ++e)
-                    big[at + e] = make_uint4((uint32_t)tid, e * eb, min(nb, (e + 1) * eb), 0);
+            if (tier == 0) {
+                HitSink sink{reinterpret_cast<uint32_t *>(md.bits)};
+                for (int z = t.lo[2]; z <= t.hi[2]; ++z)
+                    for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
+                sink.flush();
+            } else if (!INPLACE) {
+                const uint32_t eb = tune.warp_max;
+                const uint32_t ne = (nb + eb - 1) / eb;
+                const uint32_t at = atomicAdd(big_count, ne);
+                if (at + ne <= big_cap) {
+                    for (uint32_t e = 0; e < ne; ++e)
+                        big[at + e] = make_uint4((uint32_t)gid, e * eb, min(nb, (e + 1) * eb), (uint32_t)(gid >> 32));
+                }
             }
         }
         if (INPLACE) {
@@ -521,7 +529,10 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(const float *
                 Tri w;
                 shfl_tri(w, t, src);
                 const uint32_t wnb = __shfl_sync(0xFFFFFFFFu, nb, src);
-                warp_bricks<S>(w, g, bm, 0, wnb, 0, 32, tune.split != 0);
+                const int wm = __shfl_sync(0xFFFFFFFFu, m, src);
+                const MeshDev &md = bd.mesh[wm];
+                const GridParams g = *md.gp;
+                warp_bricks<S>(w, g, reinterpret_cast<uint32_t *>(md.bits), 0, wnb, 0, 32, tune.split != 0);
             }
         }
     }
@@ -530,16 +541,10 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(const float *
 // Queued triangles: each warp takes an entry (triangle, brick range) and
 // walks its bricks.
 template <bool S>
-__global__ void __launch_bounds__(256, 4) k_voxelize_bricks(const float *__restrict__ pts,
-                                                            const int32_t *__restrict__ tris,
-                                                            const GridParams *__restrict__ gpp, int rx,
-                                                            int ry, int rz, uint32_t *__restrict__ bm,
-                                                            const uint4 *__restrict__ big,
+__global__ void __launch_bounds__(256, 4) k_voxelize_bricks(BatchDev bd, const uint4 *__restrict__ big,
                                                             const uint32_t *__restrict__ big_count,
                                                             uint32_t big_cap, uint32_t *__restrict__ cursor,
                                                             bool split) {
-    const GridParams g = *gpp;
-    const int res[3] = {rx, ry, rz};
     const int lane = threadIdx.x & 31;
     const uint32_t n = *big_count;
     if (n > big_cap) return;  // reported by the host; the build is retried
@@ -549,11 +554,15 @@ __global__ void __launch_bounds__(256, 4) k_voxelize_bricks(const float *__restr
         e = __shfl_sync(0xFFFFFFFFu, e, 0);
         if (e >= n) return;
         const uint4 ent = big[e];
+        const int64_t gid = (int64_t)ent.x | ((int64_t)ent.w << 32);
+        const int m = find_segment(bd.tri_off, bd.n, (uint64_t)gid);
+        const MeshDev &md = bd.mesh[m];
+        const GridParams g = *md.gp;
         float p[3][3];
-        load_tri(pts, tris, ent.x, p);
+        load_tri(md.pts, md.tris, gid - (int64_t)bd.tri_off[m], p);
         Tri t;
-        tri_setup<S>(g, res, p[0], p[1], p[2], t);
-        warp_bricks<S>(t, g, bm, ent.y, ent.z, 0, 32, split);
+        tri_setup<S>(g, md.res, p[0], p[1], p[2], t);
+        warp_bricks<S>(t, g, reinterpret_cast<uint32_t *>(md.bits), ent.y, ent.z, 0, 32, split);
     }
 }
 
@@ -588,34 +597,23 @@ cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaS
     return cudaGetLastError();
 }
 
-cudaError_t launch_bbox(const float *pts, int64_t n, int rx, int ry, int rz, uint32_t *mm_scratch,
-                        GridParams *gp, cudaStream_t st) {
-    cudaError_t e = cudaMemsetAsync(mm_scratch, 0xFF, 3 * sizeof(uint32_t), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(mm_scratch + 3, 0, 3 * sizeof(uint32_t), st);
-    if (e == cudaSuccess) e = cudaMemsetAsync(gp, 0, sizeof(GridParams), st);
-    if (e != cudaSuccess) return e;
-    int blocks = (int)std::min<int64_t>((n / 4 + 255) / 256, 148 * 4);
-    blocks = std::max(blocks, 1);
-    k_bbox_reduce<<<blocks, 256, 0, st>>>(pts, n, mm_scratch, gp);
-    count_launches(1);
-    k_grid_setup<<<1, 32, 0, st>>>(mm_scratch, rx, ry, rz, gp);
-    count_launches(1);
+cudaError_t launch_bbox(const BatchDev &b, uint32_t total_blocks, cudaStream_t st) {
+    k_bbox_reduce<<<total_blocks, 256, 0, st>>>(b);
+    k_grid_setup<<<(b.n + 127) / 128, 128, 0, st>>>(b);
+    count_launches(2);
     return cudaGetLastError();
 }
 
-cudaError_t launch_voxelize(const float *pts, const int32_t *tris, int64_t nt, const GridParams *gp,
-                            int rx, int ry, int rz, bool strict, uint32_t *bm, const VoxTuning &tune,
-                            uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms,
-                            cudaStream_t st) {
-    // counters[0] = big entries, counters[1] = big cursor
+cudaError_t launch_voxelize(const BatchDev &b, int64_t total, bool strict, const VoxTuning &tune, uint4 *big,
+                            uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st) {
+    // counters[0] = queue entries, counters[1] = queue cursor
     cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
-    if (nt > 0) {
-        const int64_t want = (nt + 255) / 256;
+    if (total > 0) {
+        const int64_t want = (total + 255) / 256;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * 16));
         const bool inplace = big == nullptr || big_cap == 0;
-#define SVO_VOX(S_, I_) \
-    k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(pts, tris, nt, gp, rx, ry, rz, bm, tune, big, big_cap, counters)
+#define SVO_VOX(S_, I_) k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(b, total, tune, big, big_cap, counters)
         if (strict) {
             if (inplace) SVO_VOX(true, true); else SVO_VOX(true, false);
         } else {
@@ -626,11 +624,11 @@ cudaError_t launch_voxelize(const float *pts, const int32_t *tris, int64_t nt, c
         if (!inplace) {
             const int bblocks = num_sms * 4;
             if (strict)
-                k_voxelize_bricks<true><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters, big_cap,
-                                                                counters + 1, tune.split != 0);
+                k_voxelize_bricks<true><<<bblocks, 256, 0, st>>>(b, big, counters, big_cap, counters + 1,
+                                                                tune.split != 0);
             else
-                k_voxelize_bricks<false><<<bblocks, 256, 0, st>>>(pts, tris, gp, rx, ry, rz, bm, big, counters,
-                                                                 big_cap, counters + 1, tune.split != 0);
+                k_voxelize_bricks<false><<<bblocks, 256, 0, st>>>(b, big, counters, big_cap, counters + 1,
+                                                                 tune.split != 0);
             count_launches(1);
         }
     }

@@ -115,6 +115,16 @@ def lib() -> C.CDLL:
             g = getattr(L, f"svo_result_copy_{name}")
             g.argtypes = [vp, vp, i64]
         L.svo_result_timings.argtypes = [vp, vp, C.c_int]
+        L.svo_batch_create.argtypes = [vp, C.POINTER(MeshDesc), C.c_int, C.c_uint32, vp, C.POINTER(vp)]
+        L.svo_batch_size.argtypes = [vp]
+        L.svo_batch_mesh_status.argtypes = [vp, C.c_int]
+        L.svo_batch_mesh_nodes.argtypes = [vp, C.c_int]
+        L.svo_batch_mesh_nodes.restype = i64
+        L.svo_batch_mesh_output_bytes.argtypes = [vp, C.c_int]
+        L.svo_batch_mesh_output_bytes.restype = i64
+        L.svo_batch_emit.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp), C.POINTER(C.c_int)]
+        L.svo_batch_free.argtypes = [vp]
+        L.svo_batch_free.restype = None
         L.svo_kernel_launches.restype = i64
         L.svo_result_num_dedup.argtypes = [vp, C.c_int]
         L.svo_result_num_dedup.restype = i64
@@ -227,28 +237,80 @@ class Context:
                                stream or None, C.byref(h)))
         return Result(h)
 
+    def batch(self, meshes, flags: int = 0, stream: int = 0) -> "Batch":
+        """svo_batch_create over [(points, tris, res), ...] (counting phase)."""
+        descs, keep = _descs(meshes, flags)
+        h = C.c_void_p()
+        _check(lib().svo_batch_create(self._h, descs, len(meshes), flags, stream or None, C.byref(h)))
+        return Batch(h, keep)
+
     def build_batch(self, meshes, flags: int = 0, stream: int = 0):
-        """svo_build_batch over [(points, tris, res), ...]; returns (results, statuses)."""
-        keep = []
-        descs = (MeshDesc * len(meshes))()
-        for i, (pts, tri, res) in enumerate(meshes):
-            if isinstance(pts, np.ndarray):
-                pts = np.ascontiguousarray(pts, dtype=np.float32)
-            if isinstance(tri, np.ndarray):
-                tri = np.ascontiguousarray(tri, dtype=np.int32)
-            keep.append((pts, tri))
-            d = descs[i]
-            d.points = _ptr(pts)
-            d.n_points = pts.shape[0]
-            d.tris = _ptr(tri) if tri is not None else None
-            d.n_tris = 0 if tri is None else tri.shape[0]
-            d.res[:] = _res3(res)
-            d.flags = flags
+        """svo_build_batch over [(points, tris, res), ...] or [(points, tris, res, flags), ...];
+        returns (results, statuses, rc)."""
+        descs, keep = _descs(meshes, flags)
         outs = (C.c_void_p * len(meshes))()
         st = (C.c_int * len(meshes))()
         rc = lib().svo_build_batch(self._h, descs, len(meshes), stream or None, outs, st)
         results = [Result(C.c_void_p(outs[i])) if st[i] == OK else None for i in range(len(meshes))]
         return results, list(st), rc
+
+
+def _descs(meshes, flags):
+    keep = []
+    descs = (MeshDesc * len(meshes))()
+    for i, item in enumerate(meshes):
+        pts, tri, res = item[:3]
+        f = item[3] if len(item) > 3 else flags
+        if isinstance(pts, np.ndarray):
+            pts = np.ascontiguousarray(pts, dtype=np.float32)
+        if isinstance(tri, np.ndarray):
+            tri = np.ascontiguousarray(tri, dtype=np.int32)
+        keep.append((pts, tri))
+        d = descs[i]
+        d.points = _ptr(pts)
+        d.n_points = pts.shape[0]
+        d.tris = _ptr(tri) if tri is not None else None
+        d.n_tris = 0 if tri is None else tri.shape[0]
+        d.res[:] = _res3(res)
+        d.flags = f
+    return descs, keep
+
+
+class Batch:
+    """svo_batch: counting phase done for every mesh; emit() writes octrees."""
+
+    def __init__(self, h, keep):
+        self._h = h
+        self._keep = keep
+
+    def __len__(self) -> int:
+        return lib().svo_batch_size(self._h)
+
+    def status(self, i: int) -> int:
+        return lib().svo_batch_mesh_status(self._h, i)
+
+    def nodes(self, i: int) -> int:
+        return lib().svo_batch_mesh_nodes(self._h, i)
+
+    def output_bytes(self, i: int) -> int:
+        return lib().svo_batch_mesh_output_bytes(self._h, i)
+
+    def emit(self, first: int, count: int):
+        outs = (C.c_void_p * count)()
+        st = (C.c_int * count)()
+        rc = lib().svo_batch_emit(self._h, first, count, outs, st)
+        return [Result(C.c_void_p(outs[i])) if st[i] == OK else None for i in range(count)], list(st), rc
+
+    def close(self) -> None:
+        if self._h:
+            lib().svo_batch_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 class Result:

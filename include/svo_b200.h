@@ -141,10 +141,12 @@ int svo_build(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t
               int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags, void *stream,
               svo_result **out);
 
-/* Many independent builds in one pass over the device (batched launches; each
- * mesh's result equals its own svo_build).  descs[i] describes mesh i;
- * out[i] receives its result.  Status of the first failing mesh is returned;
- * per-mesh status in status_out (may be NULL). */
+/* Many independent builds in one pass over the device: every kernel of the
+ * pipeline runs once for all meshes (meshes with equal flags share a pass);
+ * each mesh's result equals its own svo_build bit for bit.  descs[i]
+ * describes mesh i; out[i] receives its result (NULL on error).  Returns the
+ * status of the first failing mesh; per-mesh status in status_out (may be
+ * NULL).  No counterpart in the reference (one mesh per process there). */
 typedef struct svo_mesh_desc {
     const float *points;
     int64_t n_points;
@@ -155,6 +157,24 @@ typedef struct svo_mesh_desc {
 } svo_mesh_desc;
 int svo_build_batch(svo_ctx *ctx, const svo_mesh_desc *descs, int n, void *stream,
                     svo_result **out, int *status_out);
+
+/* The same in two steps, for callers that bound device memory:
+ * svo_batch_create runs the counting phase of every mesh (voxelization,
+ * octree level sizes; about res^3/7 bytes of scratch per mesh) and knows each
+ * mesh's exact node count and output size; svo_batch_emit then writes the
+ * octrees of meshes [first, first + count) in one pass -- call it for
+ * consecutive ranges that fit the memory at hand and free their results
+ * between calls.  All meshes of a batch use `flags` (descs[i].flags is
+ * ignored).  The batch holds its scratch until svo_batch_free. */
+typedef struct svo_batch svo_batch;
+int svo_batch_create(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, void *stream,
+                     svo_batch **out);
+int svo_batch_size(const svo_batch *b);
+int svo_batch_mesh_status(const svo_batch *b, int i);
+int64_t svo_batch_mesh_nodes(const svo_batch *b, int i);        /* -1 on error */
+int64_t svo_batch_mesh_output_bytes(const svo_batch *b, int i); /* device bytes of its result */
+int svo_batch_emit(svo_batch *b, int first, int count, svo_result **out, int *status_out);
+void svo_batch_free(svo_batch *b);
 
 /* Sorted surface-voxel Morton keys of a mesh (the first stage of svo_build:
  * same bounding cube, same voxel test, same key list as svo_result_copy_keys)
