@@ -49,7 +49,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5", "heightfield"], default="torus_slivers")
+    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5", "heightfield", "batch256"],
+                    default="torus_slivers")
+    ap.add_argument("--flags", type=int, default=-1, help="override the workload's build flags (SVO_FLAG_*)")
+    ap.add_argument("--wave-gb", type=float, default=48.0, help="batch256: device bytes of results per emit wave")
     ap.add_argument("--res", type=int, default=0, help="override the workload's resolution")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
@@ -57,16 +60,19 @@ def parse_args():
 
 
 def workload(name: str):
+    """(points, tris, res, name, build flags) of a single-mesh workload."""
+    import svo_b200 as S
     from svo_b200 import meshgen
 
     if name == "torus_slivers":
         pts, tris, res = meshgen.torus_slivers()
-        return pts, tris, res, "torus_slivers_1M_res512"
+        return pts, tris, res, "torus_slivers_1M_res512", 0
     if name == "heightfield":
+        # 5M triangles at resolution 2048 with full neighbour tables and vertex/edge/face dedup
         pts, tris, res = meshgen.heightfield()
-        return pts, tris, res, "heightfield_5M_res2048"
+        return pts, tris, res, "heightfield_5M_res2048_full_dedup", S.FLAG_FULL_NEIGHBORS | S.FLAG_DEDUP
     pts, tris, res = meshgen.icosphere_l5()
-    return pts, tris, res, "icosphere_l5_res128"
+    return pts, tris, res, "icosphere_l5_res128", 0
 
 
 def n_triangles(pts, tris) -> int:
@@ -185,33 +191,57 @@ def cpu_sample(pts, tris, stride: int):
     return pts, tris[::stride]
 
 
-def time_cpu_build(pts, tris, res, threads: int) -> float:
+def time_cpu_build(pts, tris, res, threads: int, flags: int = 0) -> float:
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import oracle
 
     oracle.build()
     t = time.perf_counter()
-    r = oracle.build_svo(pts, tris, res, flags=0, threads=threads)
+    r = oracle.build_svo(pts, tris, res, flags=flags & (oracle.FLAG_FULL_NEIGHBORS | oracle.FLAG_DEDUP),
+                         threads=threads)
     dt = time.perf_counter() - t
     r.close()
     return dt
 
 
+def batch_cpu_sample(meshes, stride: int = 32):
+    """Every stride-th mesh of the batch, resolutions capped at 256 (a bounded sample)."""
+    return [(p, t, min(r, 256)) for p, t, r in meshes[::stride]]
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
-    pts, tris, res, wname = workload(args.workload)
-    stride = 16 if args.workload == "torus_slivers" else 1
-    spts, stris = cpu_sample(pts, tris, stride)
-    nt = stris.shape[0]
     threads = os.cpu_count() or 1
+    if args.workload == "batch256":
+        from svo_b200 import meshgen
+
+        sample_meshes = batch_cpu_sample(meshgen.batch(256, seed=3))
+        nt = sum(t.shape[0] for _, t, _ in sample_meshes)
+        wname, res = "batch256_seed3", [r for _, _, r in sample_meshes]
+
+        def one():
+            return sum(time_cpu_build(p, t, r, threads) for p, t, r in sample_meshes)
+
+        sample = (f"every 32nd mesh of the 256-mesh batch ({len(sample_meshes)} meshes, {nt} triangles), "
+                  f"resolution capped at 256, full builds")
+    else:
+        pts, tris, res, wname, wflags = workload(args.workload)
+        flags = wflags if args.flags < 0 else args.flags
+        stride = {"torus_slivers": 16, "heightfield": 8}.get(args.workload, 1)
+        spts, stris = cpu_sample(pts, tris, stride)
+        nt = stris.shape[0]
+
+        def one():
+            return time_cpu_build(spts, stris, res, threads, flags)
+
+        sample = (f"every {stride}th triangle of {wname} ({nt} triangles), res {res}, full build "
+                  f"(voxels, levels, nodes, vertex/edge arrays)")
     for _ in range(args.warmup):
-        time_cpu_build(spts, stris, res, threads)
-    times = [time_cpu_build(spts, stris, res, threads) for _ in range(args.steps)]
+        one()
+    times = [one() for _ in range(args.steps)]
     total = sum(times)
     value = nt * len(times) / total
-    sample = (f"every {stride}th triangle of {wname} ({nt} triangles), res {res}, full build "
-              f"(voxels, levels, nodes, vertex/edge arrays)")
     line = {
         "impl": "reference", "metric": "tris/s", "value": value, "unit": "tris/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
@@ -237,7 +267,8 @@ def run_ours(args, rank: int, world: int):
     torch.cuda.set_device(dev)
     stream = torch.cuda.current_stream()
     sid = stream.cuda_stream
-    pts, tris, res, wname = workload(args.workload)
+    pts, tris, res, wname, wflags = workload(args.workload)
+    bflags = wflags if args.flags < 0 else args.flags
     if args.res:
         res, wname = args.res, f"{wname.rsplit('_res', 1)[0]}_res{args.res}"
     nt = n_triangles(pts, tris)
@@ -251,7 +282,7 @@ def run_ours(args, rank: int, world: int):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
-        r = ctx.build(d_pts, d_tris, res, flags, sid)
+        r = ctx.build(d_pts, d_tris, res, flags | bflags, sid)
         e1.record(stream)
         e1.synchronize()
         ms = e0.elapsed_time(e1)
@@ -270,7 +301,9 @@ def run_ours(args, rank: int, world: int):
             ms, r = step()
             step_ms.append(ms)
             info = {"nodes": r.num_nodes, "vertices": r.num_vertices, "edges": r.num_edges, "keys": r.num_keys,
-                    "depth": r.depth}
+                    "depth": r.depth, "flags": bflags}
+            if bflags & S.FLAG_DEDUP:
+                info["dedup_keys"] = [int(S.lib().svo_result_num_dedup(r.handle, k)) for k in range(3)]
             r.close()
     torch.cuda.synchronize()
     launches = S.kernel_launches() - launches0
@@ -312,6 +345,8 @@ def run_ours(args, rank: int, world: int):
         h_pts = torch.from_numpy(pts).pin_memory()
         h_tris = torch.from_numpy(tris).pin_memory() if tris is not None else None
         nb = [info["nodes"] * 168, info["vertices"] * 16, info["edges"] * 28, info["keys"] * 8]
+        nd = info.get("dedup_keys", [])
+        nb += [8 * n for n in nd]
         out = [torch.empty(max(b, 1), dtype=torch.uint8).pin_memory() for b in nb]
         lib = S.lib()
 
@@ -319,12 +354,14 @@ def run_ours(args, rank: int, world: int):
             flush.fill_(1)
             torch.cuda.synchronize()
             t = time.perf_counter()
-            r = ctx.build(h_pts.numpy(), None if h_tris is None else h_tris.numpy(), res, 0, sid)
+            r = ctx.build(h_pts.numpy(), None if h_tris is None else h_tris.numpy(), res, bflags, sid)
             for fn, buf, n in ((lib.svo_result_copy_nodes, out[0], info["nodes"]),
                                (lib.svo_result_copy_vertices, out[1], info["vertices"]),
                                (lib.svo_result_copy_edges, out[2], info["edges"]),
                                (lib.svo_result_copy_keys, out[3], info["keys"])):
                 S._check(fn(r.handle, buf.data_ptr(), n))
+            for k, n in enumerate(nd):
+                S._check(lib.svo_result_copy_dedup(r.handle, k, out[4 + k].data_ptr(), n))
             dt = time.perf_counter() - t
             r.close()
             return dt
@@ -363,12 +400,140 @@ def run_ours(args, rank: int, world: int):
     ctx.close()
 
 
+def run_batch(args, rank: int, world: int):
+    """256 meshes (seed 3, icosphere/torus, 320-80k triangles, resolutions
+    64-512) built as one batch -- counting phase for all meshes, then emission
+    in waves of at most --wave-gb of results -- next to the plain path (one
+    svo_build per mesh) on the same resident meshes.  Device time between two
+    events on the build stream, host work between launches included."""
+    import torch
+
+    import svo_b200 as S
+    from svo_b200 import meshgen
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.current_stream()
+    sid = stream.cuda_stream
+    meshes = meshgen.batch(256, seed=3)
+    flags = 0 if args.flags < 0 else args.flags
+    d_meshes = [(torch.from_numpy(p).cuda(), torch.from_numpy(t).cuda(), r) for p, t, r in meshes]
+    nt = sum(t.shape[0] for _, t, _ in meshes)
+    ctx = S.Context(dev)
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+    budget = int(args.wave_gb * 1e9)
+
+    def waves(b):
+        out, first, acc = [], 0, 0
+        for i in range(len(b)):
+            ob = max(0, b.output_bytes(i))
+            if i > first and acc + ob > budget:
+                out.append((first, i - first))
+                first, acc = i, 0
+            acc += ob
+        out.append((first, len(b) - first))
+        return out
+
+    def timed(fn):
+        flush.fill_(1)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        extra = fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1), extra
+
+    def batch_once(extra_flags=0):
+        b = ctx.batch(d_meshes, flags | extra_flags, sid)
+        nodes, emit_ms, w = 0, 0.0, waves(b)
+        for first, count in w:
+            rs, st, rc = b.emit(first, count)
+            if rc != 0:
+                raise RuntimeError(f"batch emit failed: {st}")
+            if extra_flags & S.FLAG_TIMINGS:
+                emit_ms += rs[0].timings().get("emit", 0.0)
+            for r in rs:
+                nodes += r.num_nodes
+                r.close()
+        b.close()
+        return nodes, emit_ms, len(w)
+
+    def plain_once():
+        nodes = 0
+        for p, t, r in d_meshes:
+            res = ctx.build(p, t, r, flags, sid)
+            nodes += res.num_nodes
+            res.close()
+        return nodes
+
+    for _ in range(args.warmup):
+        timed(batch_once)
+        timed(plain_once)
+    dist_barrier()
+    torch.cuda.synchronize()
+    launches0 = S.kernel_launches()
+    batch_ms, plain_ms = [], []
+    with ClockSampler(dev) as clocks:
+        for _ in range(args.steps):
+            ms, (nodes, _, nwaves) = timed(batch_once)
+            batch_ms.append(ms)
+    launches = S.kernel_launches() - launches0
+    for _ in range(args.steps):
+        ms, pnodes = timed(plain_once)
+        plain_ms.append(ms)
+    assert pnodes == nodes
+    dist_barrier()
+    t_batch = dist_max(sum(batch_ms))
+    t_plain = dist_max(sum(plain_ms))
+    value = world * nt * args.steps / (t_batch / 1e3)
+    plain_value = world * nt * args.steps / (t_plain / 1e3)
+    emit_ms = statistics.median([batch_once(S.FLAG_TIMINGS)[1] for _ in range(3)])
+    peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
+    peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
+    emit_bytes = EMIT_BYTES_PER_NODE * nodes
+    achieved = emit_bytes / (emit_ms / 1e3) / 1e9 if emit_ms > 0 else None
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        sample_meshes = batch_cpu_sample(meshes)
+        threads = os.cpu_count() or 1
+        dt = sum(time_cpu_build(p, t, r, threads) for p, t, r in sample_meshes)
+        st = sum(t.shape[0] for _, t, _ in sample_meshes)
+        cpu = {"value": st / dt, "unit": "tris/s", "cores": threads, "kind": "port",
+               "sample": f"every 32nd mesh ({len(sample_meshes)} meshes, {st} triangles), resolution capped at "
+                         f"256, full oracle builds"}
+    if rank == 0:
+        line = {
+            "metric": "tris/s", "value": value, "unit": "tris/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": t_batch / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "batch256_seed3", "meshes": len(meshes), "triangles": nt,
+                       "resolutions": "64/128/256/512", "nodes": nodes, "flags": flags,
+                       "emit_waves": nwaves, "wave_bytes": budget, "parallelism": f"replicas{world}",
+                       "l2_flush": "256 MiB device write before every step, outside the timed span"},
+            "nodes_per_s": world * nodes * args.steps / (t_batch / 1e3),
+            "plain": {"value": plain_value, "unit": "tris/s", "ms_per_step": t_plain / args.steps,
+                      "path": "one svo_build per mesh, same stream, same flags"},
+            "batch_over_plain": value / plain_value,
+            "e2e": None,
+            "roofline": {"kernel": "k_emit (all waves)", "bound": "hbm", "achieved": achieved, "peak": peak,
+                         "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,
+                         "peak_source": "measured" if peaks else "fallback", "algorithmic_bytes": emit_bytes,
+                         "launch_ms": emit_ms},
+            "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+
+
 def main():
     args = parse_args()
     rank, world = dist_setup(args.gpus)
     try:
         if args.impl == "reference":
             run_reference(args, rank)
+        elif args.workload == "batch256":
+            run_batch(args, rank, world)
         else:
             run_ours(args, rank, world)
     finally:

@@ -632,7 +632,9 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         tm.mark(StageTimer::kCompact0, st);
         check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
         tm.mark(StageTimer::kCompact, st);
-        check(launch_emit(EmitBatch{d_ep, n, d_node_off}, node_off.back(), flags, ctx->num_sms, st), "emit");
+        check(launch_emit(EmitBatch{d_ep, n, d_node_off}, n == 1 ? &ep[0] : nullptr, node_off.back(), flags,
+                          ctx->num_sms, st),
+              "emit");
         tm.mark(StageTimer::kEmit, st);
         k_gather_top<<<(n + 127) / 128, 128, 0, st>>>(d_top_ptr, n, top);
         count_launches(1);

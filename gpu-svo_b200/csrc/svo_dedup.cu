@@ -1,15 +1,424 @@
 // svo_dedup.cu -- Morton-keyed unique vertices, edges and faces of the octree.
+//
+// Keys live on the finest lattice (voxel corners, coordinates 0..R):
+//   vertex key = morton(P)
+//   edge key   = morton(P) << 6 | level << 2 | axis     (P = the edge's low end)
+//   face key   = morton(P) << 6 | level << 2 | normal   (P = the face's low corner)
+// over every node of every level (sibling-filled nodes included), each list
+// sorted and unique.  The reference has no such lists (its README promises
+// them); the semantics are this library's and the oracle restates them.
+//
+// No sort is needed.  Every key names a lattice point P that is a node
+// corner, and a key of P exists iff some node touching P exists at that
+// level: at level l (P a multiple of 2^l, u = P >> l) the cells u - d,
+// d in {0,1}^3, and a cell exists iff its parent is set in the level l+1
+// occupancy bitmap (at the top level: iff it is the root).  So:
+//   1. mark a candidate bitmap D over Q = P >> 1 (each bit stands for the 8
+//      lattice points 2Q + r) from the node groups of levels >= 1 -- every
+//      level-0 corner is also a corner of a level-1 node;
+//   2. walk D's set bits in order and derive, per Q, the 8 points' keys from
+//      8 parent-bitmap lookups (coarser levels only for r = 0);
+//   3. count per 2048-bit chunk of D, scan, and emit: the keys come out in
+//      Morton order because D is in Morton order and each point's keys are
+//      produced in (level, axis) order.
+// D has R^3 bits (1 GiB at R = 2048); a 1-bit-per-chunk summary lets the two
+// walks skip untouched chunks without reading them.
+#include <cstdio>
+
+#include "svo_host.h"
 #include "svo_internal.h"
 
 namespace svo {
+namespace {
 
-int build_dedup(cudaMemPool_t, cudaStream_t, const EmitParams &, const EmitParams *, uint64_t n_out[3], uint64_t *out[3],
-                int) {
+constexpr int kDedupWarps = 8;
+constexpr uint64_t kChunkWords = 32;  // u64 words of D per chunk (2048 bits)
+
+struct DedupLevel {
+    const uint64_t *bits;  // occupancy bitmap of this level
+    const uint64_t *K1;    // sorted codes of level l+1 (this level's sibling groups)
+    uint32_t groups;       // number of those codes
+    uint32_t side;         // grid side at this level
+};
+
+struct DedupParams {
+    int T;                      // top level
+    const uint64_t *root;       // device: the root's code
+    DedupLevel lv[kMaxLevels];
+    uint32_t gstart[kMaxLevels + 1];  // marking threads of levels 1..T-1 (prefix of groups)
+    uint32_t *D;                // candidate bitmap over Q (u32 view)
+    uint32_t *G;                // one bit per chunk of D
+    uint64_t chunks;
+    uint32_t *cnt;              // [3][chunks]
+    const uint32_t *pre;        // [3][chunks + 1]
+    uint64_t *out[3];
+};
+
+__device__ __forceinline__ void mark_chunk(const DedupParams &p, uint64_t bit) {
+    const uint64_t ch = bit >> 11;
+    uint32_t *g = p.G + (ch >> 5);
+    const uint32_t m = 1u << (ch & 31);
+    if (!(*(volatile uint32_t *)g & m)) atomicOr(g, m);
+}
+
+__device__ __forceinline__ void mark_bit(const DedupParams &p, uint64_t bit) {
+    atomicOr(p.D + (bit >> 5), 1u << (bit & 31));
+    mark_chunk(p, bit);
+}
+
+// Marks the Q of every corner of every node at levels >= 1.
+//   level 1, group g (a level-2 code): nodes 2g + {0,1}^3, corners
+//     Q = 2g + {0,1,2}^3, i.e. for each e in {0,1}^3 the byte morton(g + e)
+//     of D gets the sub-points k' with k'_i = 0 wherever e_i = 1;
+//   level l >= 2: Q = (2g + {0,1,2}^3) << (l - 1), one bit each;
+//   the root (level T): Q = (root + {0,1}^3) << (T - 1).
+__global__ void k_dedup_mark(const __grid_constant__ DedupParams p, uint32_t total) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+        if (t == total - 1) {
+            const uint64_t rc = *p.root;
+            const uint32_t r[3] = {compact3(rc), compact3(rc >> 1), compact3(rc >> 2)};
+            const int sh = p.T - 1;
+            for (int d = 0; d < 8; ++d)
+                mark_bit(p, morton3((r[0] + (d & 1)) << sh, (r[1] + ((d >> 1) & 1)) << sh,
+                                    (r[2] + ((d >> 2) & 1)) << sh));
+            continue;
+        }
+        int l = 1;
+        while (l + 1 < p.T && t >= p.gstart[l + 1]) ++l;
+        const uint64_t gc = p.lv[l].K1[t - p.gstart[l]];
+        const uint32_t g[3] = {compact3(gc), compact3(gc >> 1), compact3(gc >> 2)};
+        if (l == 1) {
+            for (int e = 0; e < 8; ++e) {
+                const uint64_t byte = morton3(g[0] + (e & 1), g[1] + ((e >> 1) & 1), g[2] + ((e >> 2) & 1));
+                uint32_t m = 0xFFu;
+                if (e & 1) m &= 0x55u;
+                if (e & 2) m &= 0x33u;
+                if (e & 4) m &= 0x0Fu;
+                atomicOr(p.D + (byte >> 2), m << (8 * (byte & 3)));
+                mark_chunk(p, byte << 3);
+            }
+        } else {
+            const int sh = l - 1;
+            for (int k = 0; k < 27; ++k) {
+                const uint32_t kx = k % 3, ky = (k / 3) % 3, kz = k / 9;
+                mark_bit(p, morton3((2 * g[0] + kx) << sh, (2 * g[1] + ky) << sh, (2 * g[2] + kz) << sh));
+            }
+        }
+    }
+}
+
+// Bit e of the result: cell v - e exists at the level whose occupancy bitmap
+// is `bits` and whose side, dilated, is sx (x position).  v is given by its
+// Morton code vc (dilated coordinates, stepped in place); its coordinates are
+// at most the level's side.
+__device__ __forceinline__ uint32_t cell_mask(const uint64_t *bits, uint64_t vc, uint64_t sx) {
+    const uint64_t xm = vc & kDilX, ym = vc & kDilY, zm = vc & kDilZ;
+    const uint64_t xd = dil_dec(xm, kDilX), yd = dil_dec(ym, kDilY), zd = dil_dec(zm, kDilZ);
+    const bool vx0 = xm < sx, vy0 = ym < (sx << 1), vz0 = zm < (sx << 2);
+    const bool vx1 = xm != 0, vy1 = ym != 0, vz1 = zm != 0;
+    uint32_t m = 0;
+#pragma unroll
+    for (int e = 0; e < 8; ++e) {
+        const bool ok = ((e & 1) ? vx1 : vx0) && ((e & 2) ? vy1 : vy0) && ((e & 4) ? vz1 : vz0);
+        if (!ok) continue;
+        const uint64_t c = ((e & 1) ? xd : xm) | ((e & 2) ? yd : ym) | ((e & 4) ? zd : zm);
+        m |= (uint32_t)((bits[c >> 6] >> (c & 63)) & 1ull) << e;
+    }
+    return m;
+}
+
+// Shared tables.
+//   around[E * 8 + s]: existence of the 8 cells u - d around a point of
+//     parity s (bit d), given the parent mask E: cell u - d has parent
+//     v - (d & ~s)
+//   kinds[ex]: bit 0 vertex, bits 1-3 edges along x/y/z, bits 4-6 faces
+//     with normal x/y/z, from the cell existence mask ex
+//   cnt0[E]: keys of the 8 points 2Q + r at level 0 given E, packed
+//     (vertices | edges << 8 | faces << 16)
+struct DedupTables {
+    uint8_t around[2048];
+    uint8_t kinds[256];
+    uint32_t cnt0[256];
+};
+
+__device__ void init_tables(DedupTables &t) {
+    for (int i = threadIdx.x; i < 2048; i += blockDim.x) {
+        const uint32_t E = i >> 3, s = i & 7;
+        uint32_t ex = 0;
+        for (int d = 0; d < 8; ++d) ex |= ((E >> (d & ~s & 7)) & 1u) << d;
+        t.around[i] = (uint8_t)ex;
+    }
+    for (int ex = threadIdx.x; ex < 256; ex += blockDim.x) {
+        uint32_t k = ex != 0;
+        k |= (uint32_t)((ex & 0x55) != 0) << 1 | (uint32_t)((ex & 0x33) != 0) << 2 | (uint32_t)((ex & 0x0F) != 0) << 3;
+        k |= (uint32_t)((ex & 0x03) != 0) << 4 | (uint32_t)((ex & 0x05) != 0) << 5 | (uint32_t)((ex & 0x11) != 0) << 6;
+        t.kinds[ex] = (uint8_t)k;
+    }
+    __syncthreads();
+    for (int E = threadIdx.x; E < 256; E += blockDim.x) {
+        uint32_t v = 0, e = 0, f = 0;
+        for (int r = 0; r < 8; ++r) {
+            const uint32_t k = t.kinds[t.around[E * 8 + r]];
+            v += k & 1;
+            e += __popc((k >> 1) & 7);
+            f += __popc((k >> 4) & 7);
+        }
+        t.cnt0[E] = v | e << 8 | f << 16;
+    }
+    __syncthreads();
+}
+
+// Keys of the 8 lattice points 2Q + r: counts (c) and, when EMIT, writes them
+// at the cursors o[].
+template <bool EMIT>
+__device__ __forceinline__ void q_keys(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                       uint64_t root, uint64_t qc, uint32_t c[3], uint64_t *o[3]) {
+    const uint32_t E0 = cell_mask(p.lv[1].bits, qc, sx[1]);
+    if (!EMIT) {
+        const uint32_t k0 = tb.cnt0[E0];
+        c[0] += k0 & 0xFF;
+        c[1] += (k0 >> 8) & 0xFF;
+        c[2] += k0 >> 16;
+    }
+    // r = 0 (P = 2Q): level 0, then every level l with P a multiple of 2^l
+    bool vert = false;
+    {
+        const uint64_t pc = qc << 3;
+        const uint32_t k = tb.kinds[tb.around[E0 * 8]];
+        vert = k & 1;
+        if (EMIT) {
+            for (uint32_t a = 0; a < 3; ++a)
+                if (k >> (1 + a) & 1) *o[1]++ = (pc << 6) | a;
+            for (uint32_t a = 0; a < 3; ++a)
+                if (k >> (4 + a) & 1) *o[2]++ = (pc << 6) | a;
+        }
+        uint64_t uc = qc;  // u = P >> l at l = 1
+        for (int l = 1; l <= p.T; ++l) {
+            if (l > 1) {
+                if (uc & 7) break;
+                uc >>= 3;
+            }
+            uint32_t ex;
+            if (l < p.T) {
+                ex = tb.around[cell_mask(p.lv[l + 1].bits, uc >> 3, sx[l + 1]) * 8 + (uint32_t)(uc & 7)];
+            } else {
+                // the top level holds the root alone: cell u - d is the root iff d = u - root
+                const int dx = (int)compact3(uc) - (int)compact3(root);
+                const int dy = (int)compact3(uc >> 1) - (int)compact3(root >> 1);
+                const int dz = (int)compact3(uc >> 2) - (int)compact3(root >> 2);
+                ex = (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) ? 1u << (dx | dy << 1 | dz << 2)
+                                                                                      : 0u;
+            }
+            const uint32_t k = tb.kinds[ex];
+            vert |= k & 1;
+            if (EMIT) {
+                for (uint32_t a = 0; a < 3; ++a)
+                    if (k >> (1 + a) & 1) *o[1]++ = (pc << 6) | ((uint64_t)l << 2) | a;
+                for (uint32_t a = 0; a < 3; ++a)
+                    if (k >> (4 + a) & 1) *o[2]++ = (pc << 6) | ((uint64_t)l << 2) | a;
+            } else {
+                c[1] += __popc((k >> 1) & 7);
+                c[2] += __popc((k >> 4) & 7);
+            }
+        }
+        if (EMIT) {
+            if (vert) *o[0]++ = pc;
+        } else if (vert && !(tb.kinds[tb.around[E0 * 8]] & 1)) {
+            ++c[0];  // a vertex of coarser nodes only
+        }
+    }
+    if (EMIT) {
+        for (uint32_t r = 1; r < 8; ++r) {
+            const uint64_t pc = (qc << 3) | r;
+            const uint32_t k = tb.kinds[tb.around[E0 * 8 + r]];
+            if (k & 1) *o[0]++ = pc;
+            for (uint32_t a = 0; a < 3; ++a)
+                if (k >> (1 + a) & 1) *o[1]++ = (pc << 6) | a;
+            for (uint32_t a = 0; a < 3; ++a)
+                if (k >> (4 + a) & 1) *o[2]++ = (pc << 6) | a;
+        }
+    }
+}
+
+// One warp per chunk of D.  The chunk's set bits are listed in order in
+// shared memory, then taken 32 at a time (lane i the i-th): counts per kind
+// (EMIT false, one total per chunk) or keys written at the chunk's scanned
+// offset plus the warp prefix of the batch (EMIT true).
+template <bool EMIT>
+__global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_keys(const __grid_constant__ DedupParams p) {
+    __shared__ DedupTables tb;
+    __shared__ uint16_t list[kDedupWarps][2048];
+    __shared__ uint64_t sx[kMaxLevels];  // dilated side of each level
+    if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
+    init_tables(tb);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
+    const uint64_t root = *p.root;
+    const uint64_t *D64 = reinterpret_cast<const uint64_t *>(p.D);
+    uint16_t *lst = list[warp];
+    for (uint64_t ch = (uint64_t)blockIdx.x * kDedupWarps + warp; ch < p.chunks; ch += nwarps) {
+        const bool touched = (p.G[ch >> 5] >> (ch & 31)) & 1u;
+        if (!touched) {
+            if (!EMIT && lane < 3) p.cnt[lane * p.chunks + ch] = 0;
+            continue;
+        }
+        // list the chunk's set bits in order
+        uint64_t word = D64[ch * kChunkWords + lane];
+        const uint32_t n = __popcll(word);
+        uint32_t incl = n;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += y;
+        }
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        for (uint32_t k = incl - n; word; word &= word - 1, ++k)
+            lst[k] = (uint16_t)(lane * 64 + __ffsll((long long)word) - 1);
+        __syncwarp();
+        uint32_t c[3] = {0, 0, 0};
+        uint64_t base[3] = {0, 0, 0};
+        if (EMIT)
+            for (int k = 0; k < 3; ++k) base[k] = p.pre[k * (p.chunks + 1) + ch];
+        for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            const bool act = j < total;
+            const uint64_t qc = ch * 2048 + (act ? lst[j] : 0);
+            if (!EMIT) {
+                if (act) q_keys<false>(p, tb, sx, root, qc, c, nullptr);
+            } else {
+                uint32_t q[3] = {0, 0, 0};
+                if (act) q_keys<false>(p, tb, sx, root, qc, q, nullptr);
+                uint64_t *o[3];
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    uint32_t x = q[k];
+#pragma unroll
+                    for (int d = 1; d < 32; d <<= 1) {
+                        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+                        if (lane >= d) x += y;
+                    }
+                    o[k] = p.out[k] + base[k] + (x - q[k]);
+                    base[k] += __shfl_sync(0xFFFFFFFFu, x, 31);
+                }
+                if (act) q_keys<true>(p, tb, sx, root, qc, q, o);
+            }
+        }
+        __syncwarp();
+        if (!EMIT) {
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+#pragma unroll
+                for (int d = 16; d > 0; d >>= 1) c[k] += __shfl_xor_sync(0xFFFFFFFFu, c[k], d);
+            }
+            if (lane < 3) p.cnt[lane * p.chunks + ch] = lane == 0 ? c[0] : lane == 1 ? c[1] : c[2];
+        }
+    }
+}
+
+int dedup_fail(int code, const char *msg) {
+    svo::host::set_error(msg);
+    return code;
+}
+
+}  // namespace
+
+int build_dedup(cudaMemPool_t pool, cudaStream_t st, const EmitParams &ep, const EmitParams *, uint64_t n_out[3],
+                uint64_t *out[3], int num_sms) {
     for (int k = 0; k < 3; ++k) {
         n_out[k] = 0;
         out[k] = nullptr;
     }
-    return SVO_ERR_UNSUPPORTED;
+    const int T = ep.T;
+    if (T < 1) return dedup_fail(SVO_ERR_DEGENERATE, "dedup needs at least two levels");
+    if ((uint64_t)ep.N * 12 > 0xFFFFFFFFull) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup of more than 357M nodes");
+    DedupParams p{};
+    p.T = T;
+    p.root = ep.lv[T].K1;
+    for (int l = 0; l <= T; ++l) p.lv[l] = DedupLevel{ep.lv[l].bits, ep.lv[l].K1, ep.lv[l].n / 8, ep.lv[l].side};
+    uint32_t g = 0;
+    for (int l = 1; l < T; ++l) {
+        p.gstart[l] = g;
+        g += p.lv[l].groups;
+    }
+    p.gstart[T] = g;
+    const uint32_t mark_total = g + 1;
+    const uint64_t side = ep.lv[0].side;
+    const uint64_t d_bits = side * side * side;
+    const uint64_t d_words = std::max<uint64_t>((d_bits + 63) / 64 + kChunkWords - 1, kChunkWords) / kChunkWords * kChunkWords;
+    p.chunks = d_words / kChunkWords;
+    const uint64_t g_words = (p.chunks + 31) / 32;
+
+    void *blk[6] = {};
+    const size_t sz[6] = {d_words * 8, g_words * 4, 3 * p.chunks * 4, 3 * (p.chunks + 1) * 4,
+                          scan_scratch_words(p.chunks) * 8, 256};
+    cudaError_t e = cudaSuccess;
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaMallocFromPoolAsync(&blk[i], sz[i], pool, st);
+    auto release = [&]() {
+        for (void *b : blk)
+            if (b) cudaFreeAsync(b, st);
+    };
+    auto fail = [&](cudaError_t err, const char *what) {
+        release();
+        char msg[256];
+        snprintf(msg, sizeof msg, "dedup %s: %s", what, cudaGetErrorString(err));
+        return dedup_fail(err == cudaErrorMemoryAllocation ? SVO_ERR_OUT_OF_MEMORY : SVO_ERR_CUDA, msg);
+    };
+    if (e != cudaSuccess) return fail(e, "scratch");
+    p.D = static_cast<uint32_t *>(blk[0]);
+    p.G = static_cast<uint32_t *>(blk[1]);
+    p.cnt = static_cast<uint32_t *>(blk[2]);
+    uint32_t *pre = static_cast<uint32_t *>(blk[3]);
+    p.pre = pre;
+    auto *scan = static_cast<unsigned long long *>(blk[4]);
+    uint32_t *status = static_cast<uint32_t *>(blk[5]);
+    if ((e = cudaMemsetAsync(p.D, 0, sz[0], st)) != cudaSuccess || (e = cudaMemsetAsync(p.G, 0, sz[1], st)) ||
+        (e = cudaMemsetAsync(status, 0, 4, st)))
+        return fail(e, "memset");
+    k_dedup_mark<<<(mark_total + 255) / 256, 256, 0, st>>>(p, mark_total);
+    const unsigned blocks =
+        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((p.chunks + kDedupWarps - 1) / kDedupWarps,
+                                                          (uint64_t)num_sms * 16));
+    k_dedup_keys<false><<<blocks, kDedupWarps * 32, 0, st>>>(p);
+    count_launches(2);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "count");
+    for (int k = 0; k < 3; ++k)
+        if ((e = launch_scan(p.cnt + k * p.chunks, pre + k * (p.chunks + 1), p.chunks, scan, status, st)) !=
+            cudaSuccess)
+            return fail(e, "scan");
+    uint32_t h[4] = {0, 0, 0, 0};
+    for (int k = 0; k < 3; ++k)
+        if ((e = cudaMemcpyAsync(h + k, pre + k * (p.chunks + 1) + p.chunks, 4, cudaMemcpyDeviceToHost, st)))
+            return fail(e, "read totals");
+    if ((e = cudaMemcpyAsync(h + 3, status, 4, cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
+        return fail(e, "read totals");
+    if (h[3] & kStatusScanTimeout) {
+        release();
+        return dedup_fail(SVO_ERR_DEVICE_TIMEOUT, "dedup scan look-back timed out");
+    }
+    for (int k = 0; k < 3; ++k) {
+        if (h[k] == 0) continue;
+        void *o = nullptr;
+        if ((e = cudaMallocFromPoolAsync(&o, (size_t)h[k] * 8, pool, st)) != cudaSuccess) {
+            for (int j = 0; j < k; ++j)
+                if (out[j]) cudaFreeAsync(out[j], st);
+            for (int j = 0; j < 3; ++j) out[j] = nullptr;
+            return fail(e, "output");
+        }
+        out[k] = p.out[k] = static_cast<uint64_t *>(o);
+        n_out[k] = h[k];
+    }
+    k_dedup_keys<true><<<blocks, kDedupWarps * 32, 0, st>>>(p);
+    count_launches(1);
+    if ((e = cudaGetLastError()) != cudaSuccess) {
+        for (int j = 0; j < 3; ++j) {
+            if (out[j]) cudaFreeAsync(out[j], st);
+            out[j] = nullptr;
+            n_out[j] = 0;
+        }
+        return fail(e, "emit");
+    }
+    release();
+    return SVO_OK;
 }
 
 }  // namespace svo

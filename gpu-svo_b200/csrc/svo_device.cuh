@@ -34,6 +34,19 @@ __host__ __device__ __forceinline__ uint64_t morton3(uint32_t x, uint32_t y, uin
     return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
 }
 
+// Dilated (Morton-interleaved) coordinates: x at bits 0,3,6,..., y at
+// 1,4,7,..., z at 2,5,8,....  A coordinate can be stepped without decoding:
+// for xm = code & kDilX, (xm - 1) & kDilX is x - 1 (x >= 1) and
+// ((xm | ~kDilX) + 1) & kDilX is x + 1; comparisons of dilated values follow
+// the coordinates.
+constexpr uint64_t kDilX = 0x1249249249249249ull, kDilY = kDilX << 1, kDilZ = kDilX << 2;
+__host__ __device__ __forceinline__ uint64_t dil_dec(uint64_t m, uint64_t mask) {
+    return (m - (mask & (~mask + 1))) & mask;  // mask & -mask: the axis's lowest bit
+}
+__host__ __device__ __forceinline__ uint64_t dil_inc(uint64_t m, uint64_t mask) {
+    return ((m | ~mask) + (mask & (~mask + 1))) & mask;
+}
+
 #if defined(__CUDACC__)
 // ---------------------------------------------------------------------------
 // Floating-point model.  The reference's voxel test and node origins are

@@ -144,7 +144,10 @@ cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned 
 // totals of every (mesh, level).
 cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st);
 cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st);
-cudaError_t launch_emit(const EmitBatch &b, uint64_t total_nodes, uint32_t flags, int num_sms, cudaStream_t st);
+// one: the EmitParams of a one-mesh batch (host copy, passed by value to the
+// kernel), or null for a batch of several meshes.
+cudaError_t launch_emit(const EmitBatch &b, const EmitParams *one, uint64_t total_nodes, uint32_t flags,
+                        int num_sms, cudaStream_t st);
 // Stable removal of consecutive duplicates (thrust::unique semantics).
 cudaError_t launch_unique_vertices(const svo_vertex *in, uint64_t n, svo_vertex *out,
                                    uint32_t *tile_counts, uint32_t *tile_pre,

@@ -355,21 +355,59 @@ __device__ __forceinline__ void node_info(const EmitParams &P, const float go[3]
     ni.o[2] = Fp<S>::origin(go[2], ni.w, (float)z);
 }
 
-// Full 27-neighbourhood: the same-level node at offset (dx,dy,dz) exists iff
-// its parent group is a set bit of the next level.
-__device__ __forceinline__ uint32_t neighbor_of(const EmitParams &P, const NodeInfo &ni, uint32_t self, int j) {
-    if (j == 13) return self;
-    if (ni.l >= P.T) return kNone;
-    const int dx = j % 3 - 1, dy = (j / 3) % 3 - 1, dz = j / 9 - 1;
-    const int side = (int)P.lv[ni.l].side;
-    const int x = (int)compact3(ni.code) + dx, y = (int)compact3(ni.code >> 1) + dy,
-              z = (int)compact3(ni.code >> 2) + dz;
-    if (x < 0 || y < 0 || z < 0 || x >= side || y >= side || z >= side) return kNone;
-    const uint64_t c = morton3((uint32_t)x, (uint32_t)y, (uint32_t)z);
+// Full 27-neighbourhood.  The same-level node at offset d exists iff its
+// parent group is a set bit of the next level.  A node with coordinate parity
+// s has its neighbours' parents among 8 groups: its own and, per axis, the
+// one on the side it borders (-1 where s_i = 0, +1 where s_i = 1).  Those 7
+// other groups are ranked once; neighbour d then lies in group b (b_i = 1
+// where d crosses into the bordering group) at child (s ^ [d != 0]).
+__device__ __forceinline__ void full_neighbors(const EmitParams &P, const NodeInfo &ni, uint32_t self,
+                                               uint32_t nb[27]) {
+    nb[13] = self;
+    if (ni.l >= P.T) return;
     const int l1 = ni.l + 1;
-    if (!bit_of(P.lv[l1].bits, c >> 3)) return kNone;
-    const uint32_t g = (l1 < P.T) ? rank_of(P, l1, c >> 3) : 0u;
-    return P.lv[ni.l].off + 8u * g + (uint32_t)(c & 7);
+    const uint64_t pc = ni.code >> 3;
+    const uint32_t s = (uint32_t)(ni.code & 7);
+    const uint64_t sx = spread3(P.lv[l1].side);
+    const uint64_t m[3] = {pc & kDilX, pc & kDilY, pc & kDilZ};
+    const uint64_t lim[3] = {sx, sx << 1, sx << 2};
+    const uint64_t msk[3] = {kDilX, kDilY, kDilZ};
+    uint64_t step[3];
+    bool ok[3];
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if ((s >> a) & 1) {
+            step[a] = dil_inc(m[a], msk[a]);
+            ok[a] = step[a] < lim[a] && step[a] != 0;
+        } else {
+            ok[a] = m[a] != 0;
+            step[a] = dil_dec(m[a], msk[a]);
+        }
+    }
+    const uint32_t own = self - (uint32_t)(ni.code & 7);  // child 0 of the node's own group
+    uint32_t base[8];
+    base[0] = own;
+#pragma unroll
+    for (int b = 1; b < 8; ++b) {
+        base[b] = kNone;
+        if (((b & 1) && !ok[0]) || ((b & 2) && !ok[1]) || ((b & 4) && !ok[2])) continue;
+        const uint64_t q = ((b & 1) ? step[0] : m[0]) | ((b & 2) ? step[1] : m[1]) | ((b & 4) ? step[2] : m[2]);
+        if (!bit_of(P.lv[l1].bits, q)) continue;
+        base[b] = P.lv[ni.l].off + 8u * ((l1 < P.T) ? rank_of(P, l1, q) : 0u);
+    }
+#pragma unroll
+    for (int j = 0; j < 27; ++j) {
+        if (j == 13) continue;
+        const int d[3] = {j % 3 - 1, (j / 3) % 3 - 1, j / 9 - 1};
+        int b = 0, k = 0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const int sa = (int)((s >> a) & 1);
+            if (d[a] != 0 && (d[a] > 0) == (sa == 1)) b |= 1 << a;
+            k |= (sa ^ (d[a] != 0 ? 1 : 0)) << a;
+        }
+        nb[j] = base[b] == kNone ? kNone : base[b] + (uint32_t)k;
+    }
 }
 
 // Corners (Morton-numbered) joined by edge e, in the reference's edge order
@@ -397,16 +435,20 @@ __device__ __forceinline__ bool veq(const float *a, const float *b) {
 constexpr int kEmitWarps = 4;
 constexpr int kEmitBufBytes = 32 * 336;  // per warp
 
-template <bool S, bool FULL, bool VE>
-__global__ void __launch_bounds__(kEmitWarps * 32) k_emit(EmitBatch eb, uint64_t total) {
+// ONE: a single mesh whose parameters travel in the kernel's parameter space
+// (`one`, read through the constant cache); otherwise each warp looks up its
+// mesh in the batch table (global memory, L1-cached).
+template <bool S, bool FULL, bool VE, bool ONE>
+__global__ void __launch_bounds__(kEmitWarps * 32)
+    k_emit(EmitBatch eb, const __grid_constant__ EmitParams one, uint64_t total) {
     extern __shared__ uint4 smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     uint4 *wbuf = smem + warp * (kEmitBufBytes / 16);
     const uint64_t nwarps = (uint64_t)gridDim.x * kEmitWarps;
     for (uint64_t gbase = ((uint64_t)blockIdx.x * kEmitWarps + warp) * 32; gbase < total; gbase += nwarps * 32) {
-        const int mj = find_segment(eb.node_off, eb.n, gbase);
-        const EmitParams &P = eb.p[mj];
-        const uint64_t base = gbase - eb.node_off[mj];
+        const int mj = ONE ? 0 : find_segment(eb.node_off, eb.n, gbase);
+        const EmitParams &P = ONE ? one : eb.p[mj];
+        const uint64_t base = ONE ? gbase : gbase - eb.node_off[mj];
         if (base >= P.N) continue;  // padding between meshes
         const float go[3] = {P.gp->origin[0], P.gp->origin[1], P.gp->origin[2]};
         unsigned long long vdup = 0, edup = 0;
@@ -420,8 +462,7 @@ __global__ void __launch_bounds__(kEmitWarps * 32) k_emit(EmitBatch eb, uint64_t
         for (int j = 0; j < 27; ++j) nb[j] = kNone;
         if (valid) {
             if (FULL) {
-#pragma unroll 1
-                for (int j = 0; j < 27; ++j) nb[j] = neighbor_of(P, ni, t, j);
+                full_neighbors(P, ni, t, nb);
             } else if (ni.l == P.T && P.T >= 1) {
                 nb[13] = t;  // root self entry, src/SVO.cu:522-529,556-557
             }
@@ -693,7 +734,8 @@ cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStre
     return cudaGetLastError();
 }
 
-cudaError_t launch_emit(const EmitBatch &b, uint64_t total, uint32_t flags, int num_sms, cudaStream_t st) {
+cudaError_t launch_emit(const EmitBatch &b, const EmitParams *one, uint64_t total, uint32_t flags, int num_sms,
+                        cudaStream_t st) {
     if (total == 0) return cudaSuccess;
     const uint64_t warps = (total + 31) / 32;
     const unsigned blocks = (unsigned)std::max<uint64_t>(
@@ -701,7 +743,13 @@ cudaError_t launch_emit(const EmitBatch &b, uint64_t total, uint32_t flags, int 
     const size_t shmem = (size_t)kEmitWarps * kEmitBufBytes;
     const bool s = (flags & SVO_FLAG_STRICT_FP) != 0, f = (flags & SVO_FLAG_FULL_NEIGHBORS) != 0,
                ve = (flags & SVO_FLAG_NO_VERT_EDGE) == 0;
-#define SVO_EMIT(S_, F_, V_) k_emit<S_, F_, V_><<<blocks, kEmitWarps * 32, shmem, st>>>(b, total)
+    const EmitParams p1 = one ? *one : EmitParams{};
+#define SVO_EMIT1(S_, F_, V_)                                                                       \
+    do {                                                                                             \
+        if (one) k_emit<S_, F_, V_, true><<<blocks, kEmitWarps * 32, shmem, st>>>(b, p1, total);      \
+        else k_emit<S_, F_, V_, false><<<blocks, kEmitWarps * 32, shmem, st>>>(b, p1, total);        \
+    } while (0)
+#define SVO_EMIT(S_, F_, V_) SVO_EMIT1(S_, F_, V_)
     if (s) {
         if (f) { if (ve) SVO_EMIT(true, true, true); else SVO_EMIT(true, true, false); }
         else { if (ve) SVO_EMIT(true, false, true); else SVO_EMIT(true, false, false); }
@@ -709,6 +757,7 @@ cudaError_t launch_emit(const EmitBatch &b, uint64_t total, uint32_t flags, int 
         if (f) { if (ve) SVO_EMIT(false, true, true); else SVO_EMIT(false, true, false); }
         else { if (ve) SVO_EMIT(false, false, true); else SVO_EMIT(false, false, false); }
     }
+#undef SVO_EMIT1
 #undef SVO_EMIT
     count_launches(1);
     return cudaGetLastError();
