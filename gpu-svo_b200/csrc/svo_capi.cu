@@ -22,8 +22,16 @@ using namespace svo;
 struct svo_ctx {
     int device = 0;
     int num_sms = 148;
-    cudaMemPool_t pool = nullptr;
+    cudaMemPool_t pool = nullptr;      // per-build scratch (the device's default pool)
+    cudaMemPool_t out_pool = nullptr;  // result arrays, kept apart so scratch never splits their blocks
     VoxTuning tune;
+};
+
+// One device block that holds the output arrays of several results (a wave of
+// a batch); freed with the last of them.
+struct svo_arena {
+    void *base = nullptr;
+    std::atomic<int> refs{0};
 };
 
 struct svo_result {
@@ -43,6 +51,8 @@ struct svo_result {
     uint64_t *dedup[3] = {nullptr, nullptr, nullptr};
     int n_timings = 0;
     float timings[9] = {};
+    svo_arena *arena = nullptr;  // holds nodes/verts/edges/keys when set
+    uint32_t own = 0x7F;         // bit i: array i of {nodes, verts, edges, keys, dedup x3} is freed on its own
 };
 
 namespace {
@@ -316,10 +326,20 @@ int batch_phase_a(svo_batch *b) {
     if (!b->meta) return cuda_fail(err, "alloc meta");
     if (!idx_check.empty()) {  // device-side index ranges, one read for all meshes
         int32_t *imm = reinterpret_cast<int32_t *>(b->meta + ml.imm);
-        for (size_t k = 0; k < idx_check.size(); ++k) {
+        const int nj = (int)idx_check.size();
+        std::vector<IndexJob> jobs(nj);
+        std::vector<uint32_t> boff(nj + 1, 0);
+        for (int k = 0; k < nj; ++k) {
             const MeshHost &mh = b->m[idx_check[k]];
-            SVO_TRY(launch_index_range(mh.d_tris, mh.n_tris * 3, imm + 2 * k, st), "index range");
+            jobs[k] = IndexJob{mh.d_tris, mh.n_tris * 3};
+            boff[k + 1] = boff[k] + index_blocks(jobs[k].n);
         }
+        IndexJob *d_jobs = batch_alloc<IndexJob>(b, nj, err);
+        uint32_t *d_boff = d_jobs ? batch_alloc<uint32_t>(b, nj + 1, err) : nullptr;
+        if (!d_boff) return cuda_fail(err, "alloc index jobs");
+        SVO_TRY(upload(d_jobs, jobs, st), "upload");
+        SVO_TRY(upload(d_boff, boff, st), "upload");
+        SVO_TRY(launch_index_ranges(d_jobs, nj, d_boff, boff[nj], imm, st), "index range");
         std::vector<int32_t> h(2 * idx_check.size());
         SVO_TRY(cudaMemcpyAsync(h.data(), imm, h.size() * 4, cudaMemcpyDeviceToHost, st), "read");
         SVO_TRY(cudaStreamSynchronize(st), "index check");
@@ -486,6 +506,18 @@ uint64_t output_bytes(const MeshHost &mh, uint32_t flags) {
     return b;
 }
 
+size_t arena_round(size_t b) { return (b + 255) / 256 * 256; }
+
+template <class T>
+T *arena_take(unsigned char *&at, uint64_t count) {
+    T *p = reinterpret_cast<T *>(at);
+    at += arena_round(count * sizeof(T));
+    return p;
+}
+
+// Meshes of at least this many nodes are emitted by a launch of their own.
+constexpr uint64_t kOwnEmitNodes = 1u << 20;
+
 // Phase B for meshes [first, first + count).
 int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *status_out) {
     svo_ctx *ctx = b->ctx;
@@ -518,7 +550,6 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         std::vector<CompactJob> jobs;
         std::vector<uint64_t> word_off(1, 0);
         std::vector<EmitParams> ep(n);
-        std::vector<uint64_t> node_off(n + 1, 0);
         std::vector<const uint64_t *> top_ptr(n);
         uint64_t ktot = 0;
         std::vector<uint64_t> kbase(n);
@@ -532,6 +563,29 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         uint64_t *top = S.get<uint64_t>(n);
         if (!K || !dups || !top) return cuda_fail(S.err, "wave scratch");
         check(cudaMemsetAsync(dups, 0, 16 * (size_t)n, st), "memset");
+        // one block for the output arrays of the whole wave
+        size_t arena_bytes = 0;
+        for (int j = 0; j < n; ++j) {
+            const MeshHost &mh = b->m[wave[j]];
+            arena_bytes += arena_round(mh.N * sizeof(svo_node));
+            if (ve) arena_bytes += arena_round(mh.N * 8 * sizeof(svo_vertex)) + arena_round(mh.N * 12 * sizeof(svo_edge));
+            if (want_keys) arena_bytes += arena_round((size_t)mh.totals[0] * 8);
+        }
+        svo_arena *arena = new svo_arena();
+        arena->refs = 1;  // the wave's own reference, dropped below
+        if (cudaMallocFromPoolAsync(&arena->base, std::max<size_t>(arena_bytes, 256), ctx->out_pool, st) != cudaSuccess) {
+            delete arena;
+            cudaGetLastError();
+            return fail(SVO_ERR_OUT_OF_MEMORY, "wave outputs: %zu bytes", arena_bytes);
+        }
+        unsigned char *arena_at = static_cast<unsigned char *>(arena->base);
+        auto drop_arena = [&]() {
+            if (arena && arena->refs.fetch_sub(1) == 1) {
+                cudaFreeAsync(arena->base, st);
+                delete arena;
+            }
+            arena = nullptr;
+        };
         for (int j = 0; j < n; ++j) {
             const MeshHost &mh = b->m[wave[j]];
             const MeshDev &md = b->h_mesh[dev_k[j]];
@@ -549,18 +603,20 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 r->unit[a] = mh.gp.unit[a];
             }
             r->n_nodes = mh.N;
-            r->nodes = pool_alloc<svo_node>(ctx->pool, st, mh.N, err);
+            r->nodes = arena_take<svo_node>(arena_at, mh.N);
             if (ve) {
-                r->verts = pool_alloc<svo_vertex>(ctx->pool, st, mh.N * 8, err);
-                r->edges = pool_alloc<svo_edge>(ctx->pool, st, mh.N * 12, err);
+                r->verts = arena_take<svo_vertex>(arena_at, mh.N * 8);
+                r->edges = arena_take<svo_edge>(arena_at, mh.N * 12);
                 r->n_verts = mh.N * 8;
                 r->n_edges = mh.N * 12;
             }
             if (want_keys) {
-                r->keys = pool_alloc<uint64_t>(ctx->pool, st, mh.totals[0], err);
+                r->keys = arena_take<uint64_t>(arena_at, mh.totals[0]);
                 r->n_keys = mh.totals[0];
             }
-            if (err != cudaSuccess) break;
+            r->arena = arena;
+            r->own = 0x70;
+            arena->refs.fetch_add(1);
             // compaction jobs: levels 1..T into K, level 0 into the keys
             CompactJob job{};
             job.bits = md.bits;
@@ -608,33 +664,53 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             P.verts = ve ? r->verts : nullptr;
             P.edges = ve ? r->edges : nullptr;
             P.dups = dups + 2 * j;
-            node_off[j + 1] = node_off[j] + (mh.N + 31) / 32 * 32;
             top_ptr[j] = job.out + job.koff[mh.T];
         }
         if (err != cudaSuccess) {
             for (svo_result *r : res) svo_result_free(r);
+            drop_arena();
             return cuda_fail(err, "output allocation");
         }
         CompactJob *d_jobs = S.get<CompactJob>(jobs.size());
         uint64_t *d_word_off = S.get<uint64_t>(word_off.size());
-        EmitParams *d_ep = S.get<EmitParams>(n);
-        uint64_t *d_node_off = S.get<uint64_t>(n + 1);
         const uint64_t **d_top_ptr = S.get<const uint64_t *>(n);
         if (S.err != cudaSuccess) {
             for (svo_result *r : res) svo_result_free(r);
+            drop_arena();
             return cuda_fail(S.err, "wave tables");
         }
         check(upload(d_jobs, jobs, st), "upload");
         check(upload(d_word_off, word_off, st), "upload");
-        check(upload(d_ep, ep, st), "upload");
-        check(upload(d_node_off, node_off, st), "upload");
         check(upload(d_top_ptr, top_ptr, st), "upload");
         tm.mark(StageTimer::kCompact0, st);
         check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
         tm.mark(StageTimer::kCompact, st);
-        check(launch_emit(EmitBatch{d_ep, n, d_node_off}, n == 1 ? &ep[0] : nullptr, node_off.back(), flags,
-                          ctx->num_sms, st),
-              "emit");
+        // Large meshes get launches of their own (parameters in the kernel's
+        // constant space); the rest share one launch over the mesh table.
+        std::vector<EmitParams> ep_small;
+        std::vector<uint64_t> off_small(1, 0);
+        for (int j = 0; j < n; ++j) {
+            if (n == 1 || ep[j].N >= kOwnEmitNodes) {
+                check(launch_emit(EmitBatch{nullptr, 1, nullptr}, &ep[j], ep[j].N, flags, ctx->num_sms, st), "emit");
+            } else {
+                ep_small.push_back(ep[j]);
+                off_small.push_back(off_small.back() + (ep[j].N + 31) / 32 * 32);
+            }
+        }
+        if (!ep_small.empty()) {
+            EmitParams *d_eps = S.get<EmitParams>(ep_small.size());
+            uint64_t *d_offs = S.get<uint64_t>(off_small.size());
+            if (S.err != cudaSuccess) {
+                for (svo_result *r : res) svo_result_free(r);
+                drop_arena();
+                return cuda_fail(S.err, "wave tables");
+            }
+            check(upload(d_eps, ep_small, st), "upload");
+            check(upload(d_offs, off_small, st), "upload");
+            check(launch_emit(EmitBatch{d_eps, (int)ep_small.size(), d_offs}, nullptr, off_small.back(), flags,
+                              ctx->num_sms, st),
+                  "emit");
+        }
         tm.mark(StageTimer::kEmit, st);
         k_gather_top<<<(n + 127) / 128, 128, 0, st>>>(d_top_ptr, n, top);
         count_launches(1);
@@ -660,8 +736,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 uint32_t *tc = U.get<uint32_t>(tiles), *tp = U.get<uint32_t>(tiles + 1);
                 unsigned long long *ss = U.get<unsigned long long>(scan_scratch_words(tiles));
                 uint32_t *ustat = U.get<uint32_t>(1);
-                svo_vertex *v2 = h_dups[2 * j] ? pool_alloc<svo_vertex>(ctx->pool, st, nv, err) : nullptr;
-                svo_edge *e2 = h_dups[2 * j + 1] ? pool_alloc<svo_edge>(ctx->pool, st, ne, err) : nullptr;
+                svo_vertex *v2 = h_dups[2 * j] ? pool_alloc<svo_vertex>(ctx->out_pool, st, nv, err) : nullptr;
+                svo_edge *e2 = h_dups[2 * j + 1] ? pool_alloc<svo_edge>(ctx->out_pool, st, ne, err) : nullptr;
                 if (U.err != cudaSuccess || err != cudaSuccess) {
                     rc = cuda_fail(U.err != cudaSuccess ? U.err : err, "unique scratch");
                     break;
@@ -681,13 +757,15 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                     check(cudaStreamSynchronize(st), "unique e");
                 }
                 if (v2) {
-                    cudaFreeAsync(r->verts, st);
+                    if (r->own & 2) cudaFreeAsync(r->verts, st);
                     r->verts = v2;
+                    r->own |= 2;
                     r->n_verts = cv;
                 }
                 if (e2) {
-                    cudaFreeAsync(r->edges, st);
+                    if (r->own & 4) cudaFreeAsync(r->edges, st);
                     r->edges = e2;
+                    r->own |= 4;
                     r->n_edges = ce;
                 }
             }
@@ -696,11 +774,13 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         for (int j = 0; j < n && rc == SVO_OK; ++j) {
             MeshHost &mh = b->m[wave[j]];
             if (mh.status != SVO_OK || !(flags & SVO_FLAG_DEDUP)) continue;
-            const int drc = build_dedup(ctx->pool, st, ep[j], d_ep + j, res[j]->n_dedup, res[j]->dedup, ctx->num_sms);
+            const int drc = build_dedup(ctx->pool, ctx->out_pool, st, ep[j], res[j]->n_dedup, res[j]->dedup,
+                                        ctx->num_sms);
             if (drc != SVO_OK) mesh_error(mh, drc, svo_last_error());
         }
         tm.mark(StageTimer::kDedup, st);
         if (tm.on) cudaEventSynchronize(tm.ev[StageTimer::kDedup]);
+        drop_arena();
     }
     int first_err = rc;
     for (int j = 0; j < n; ++j) {
@@ -797,11 +877,30 @@ int svo_ctx_create(int device, svo_ctx **out) {
     SVO_TRY(cudaDeviceGetDefaultMemPool(&c->pool, device), "mem pool");
     uint64_t keep = UINT64_MAX;  // keep freed blocks cached for the next build
     SVO_TRY(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&c->out_pool, &props) != cudaSuccess) {
+        delete c;
+        return fail(SVO_ERR_CUDA, "result memory pool");
+    }
+    SVO_TRY(cudaMemPoolSetAttribute(c->out_pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
     *out = c;
     return SVO_OK;
 }
 
-void svo_ctx_destroy(svo_ctx *ctx) { delete ctx; }
+// Results may outlive the context: a pool destroyed with allocations
+// outstanding is released once they are freed.
+void svo_ctx_destroy(svo_ctx *ctx) {
+    if (!ctx) return;
+    if (ctx->out_pool) {
+        cudaSetDevice(ctx->device);
+        cudaMemPoolDestroy(ctx->out_pool);
+    }
+    delete ctx;
+}
 
 int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t) {
     if (!ctx || !t) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
@@ -809,6 +908,7 @@ int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t) {
     ctx->tune.serial_max = t->serial_max;
     ctx->tune.warp_max = t->warp_max;
     ctx->tune.split = t->split;
+    ctx->tune.inplace_max = t->inplace_max;
     return SVO_OK;
 }
 
@@ -817,6 +917,7 @@ int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t) {
     t->serial_max = ctx->tune.serial_max;
     t->warp_max = ctx->tune.warp_max;
     t->split = ctx->tune.split;
+    t->inplace_max = ctx->tune.inplace_max;
     return SVO_OK;
 }
 
@@ -912,9 +1013,12 @@ void svo_result_free(svo_result *r) {
     if (!r) return;
     cudaSetDevice(r->device);
     void *ptrs[] = {r->nodes, r->verts, r->edges, r->keys, r->dedup[0], r->dedup[1], r->dedup[2]};
-    for (void *p : ptrs)
-        if (p) cudaFreeAsync(p, r->stream);
-    cudaStreamSynchronize(r->stream);
+    for (int i = 0; i < 7; ++i)
+        if (ptrs[i] && ((r->own >> i) & 1)) cudaFreeAsync(ptrs[i], r->stream);
+    if (r->arena && r->arena->refs.fetch_sub(1) == 1) {
+        cudaFreeAsync(r->arena->base, r->stream);
+        delete r->arena;
+    }
     delete r;
 }
 

@@ -322,8 +322,8 @@ int dedup_fail(int code, const char *msg) {
 
 }  // namespace
 
-int build_dedup(cudaMemPool_t pool, cudaStream_t st, const EmitParams &ep, const EmitParams *, uint64_t n_out[3],
-                uint64_t *out[3], int num_sms) {
+int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, const EmitParams &ep,
+                uint64_t n_out[3], uint64_t *out[3], int num_sms) {
     for (int k = 0; k < 3; ++k) {
         n_out[k] = 0;
         out[k] = nullptr;
@@ -398,7 +398,7 @@ int build_dedup(cudaMemPool_t pool, cudaStream_t st, const EmitParams &ep, const
     for (int k = 0; k < 3; ++k) {
         if (h[k] == 0) continue;
         void *o = nullptr;
-        if ((e = cudaMallocFromPoolAsync(&o, (size_t)h[k] * 8, pool, st)) != cudaSuccess) {
+        if ((e = cudaMallocFromPoolAsync(&o, (size_t)h[k] * 8, out_pool, st)) != cudaSuccess) {
             for (int j = 0; j < k; ++j)
                 if (out[j]) cudaFreeAsync(out[j], st);
             for (int j = 0; j < 3; ++j) out[j] = nullptr;

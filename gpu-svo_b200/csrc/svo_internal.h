@@ -20,6 +20,7 @@ struct VoxTuning {
     uint32_t serial_max = 64;    // grid-bbox voxels tested by one thread, row by row
     uint32_t warp_max = 256;     // 4x4x4 bricks per queue entry (one warp walks one entry)
     uint32_t split = 0;          // cull 2x2x2 sub-bricks of surviving bricks too
+    uint32_t inplace_max = 32;   // bricks of a triangle walked by the warp that set it up
 };
 
 // Occupancy bitmap pyramid: level 0 is the voxel grid (one bit per Morton
@@ -132,6 +133,16 @@ __host__ __device__ __forceinline__ int find_segment(const T *off, int n, T x) {
 cudaError_t launch_bbox(const BatchDev &b, uint32_t total_blocks, cudaStream_t st);
 // mm[0] = min, mm[1] = max of n int32 indices.
 cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaStream_t st);
+// The same for a table of n index arrays in one launch: job k gets
+// index_blocks(jobs[k].n) blocks, block_off their prefix (n + 1 entries);
+// mm[2k], mm[2k+1] = min, max of job k.
+struct IndexJob {
+    const int32_t *idx;
+    int64_t n;
+};
+uint32_t index_blocks(int64_t n);
+cudaError_t launch_index_ranges(const IndexJob *jobs, int n, const uint32_t *block_off, uint32_t total_blocks,
+                                int32_t *mm, cudaStream_t st);
 cudaError_t launch_voxelize(const BatchDev &b, int64_t total_tris, bool strict, const VoxTuning &tune,
                             uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st);
 // Builds levels 1.. of every mesh's pyramid and the per-block counts.
@@ -159,7 +170,7 @@ cudaError_t launch_unique_edges(const svo_edge *in, uint64_t n, svo_edge *out, u
 constexpr uint32_t kUniqueTile = 4096;
 
 // Morton-keyed unique vertex/edge/face keys of all nodes (SVO_FLAG_DEDUP).
-int build_dedup(cudaMemPool_t pool, cudaStream_t st, const EmitParams &p, const EmitParams *p_dev,
+int build_dedup(cudaMemPool_t scratch_pool, cudaMemPool_t out_pool, cudaStream_t st, const EmitParams &p,
                 uint64_t n_out[3], uint64_t *out[3], int num_sms);
 
 // Blocks of the bbox reduction for a mesh of n points.

@@ -360,6 +360,38 @@ __device__ __forceinline__ bool brick_reject(const Tri &t, const GridParams &g, 
     return false;
 }
 
+// The 64 voxels of brick (sx, sy, sz) of triangle t (the same in every
+// lane): 2 voxels per lane, one ballot and one atomicOr per bitmap word.
+template <bool S>
+__device__ __forceinline__ void brick_voxels(const Tri &t, const GridParams &g, uint32_t *__restrict__ bm, int sx,
+                                             int sy, int sz, int lane) {
+#pragma unroll
+    for (int h = 0; h < 2; ++h) {
+        const int lm = lane + 32 * h;  // local Morton index in the brick
+        const int x = 4 * sx + ((lm & 1) | ((lm >> 2) & 2));
+        const int y = 4 * sy + (((lm >> 1) & 1) | ((lm >> 3) & 2));
+        const int z = 4 * sz + (((lm >> 2) & 1) | ((lm >> 4) & 2));
+        const bool in = x >= t.lo[0] && x <= t.hi[0] && y >= t.lo[1] && y <= t.hi[1] && z >= t.lo[2] && z <= t.hi[2];
+        const uint32_t w = __ballot_sync(0xFFFFFFFFu, in && voxel_pass<S>(t, g, x, y, z));
+        if (lane == h && w) atomicOr(bm + ((morton3((uint32_t)sx, (uint32_t)sy, (uint32_t)sz) << 1) | h), w);
+    }
+}
+
+// Brick j (row-major over the triangle's brick box) of triangle t: its brick
+// coordinates, and whether it survives the culling test.
+template <bool S>
+__device__ __forceinline__ bool brick_live(const Tri &t, const GridParams &g, uint32_t j, int &bx, int &by, int &bz) {
+    const int bx0 = t.lo[0] >> 2, by0 = t.lo[1] >> 2, bz0 = t.lo[2] >> 2;
+    const uint32_t nbx = (uint32_t)((t.hi[0] >> 2) - bx0 + 1), nby = (uint32_t)((t.hi[1] >> 2) - by0 + 1);
+    const uint32_t jy = j / nbx, jz = jy / nby;
+    bx = bx0 + (int)(j - jy * nbx);
+    by = by0 + (int)(jy - jz * nby);
+    bz = bz0 + (int)jz;
+    const int lo[3] = {max(4 * bx, t.lo[0]), max(4 * by, t.lo[1]), max(4 * bz, t.lo[2])};
+    const int hi[3] = {min(4 * bx + 3, t.hi[0]), min(4 * by + 3, t.hi[1]), min(4 * bz + 3, t.hi[2])};
+    return !t.cull || !brick_reject<S>(t, g, lo, hi);
+}
+
 // Bricks [b0, b1) of triangle t (the same t in every lane), chunks of 32
 // bricks taken with stride `step` starting at b0 + first.  Three rounds, each
 // with one item per lane: 32 bricks (4^3); the 8 sub-bricks (2^3) of 4
@@ -370,39 +402,17 @@ __device__ __forceinline__ void warp_bricks(const Tri &t, const GridParams &g, u
                                             uint32_t b0, uint32_t b1, uint32_t first, uint32_t step,
                                             bool split) {
     const int lane = threadIdx.x & 31, grp = lane >> 3, sub = lane & 7;
-    const int bx0 = t.lo[0] >> 2, by0 = t.lo[1] >> 2, bz0 = t.lo[2] >> 2;
-    const uint32_t nbx = (uint32_t)((t.hi[0] >> 2) - bx0 + 1), nby = (uint32_t)((t.hi[1] >> 2) - by0 + 1);
     for (uint32_t c = b0 + first; c < b1; c += step) {
         const uint32_t j = c + lane;
-        bool live = false;
         int bx = 0, by = 0, bz = 0;
-        if (j < b1) {
-            const uint32_t jy = j / nbx, jz = jy / nby;
-            bx = bx0 + (int)(j - jy * nbx);
-            by = by0 + (int)(jy - jz * nby);
-            bz = bz0 + (int)jz;
-            int lo[3] = {max(4 * bx, t.lo[0]), max(4 * by, t.lo[1]), max(4 * bz, t.lo[2])};
-            int hi[3] = {min(4 * bx + 3, t.hi[0]), min(4 * by + 3, t.hi[1]), min(4 * bz + 3, t.hi[2])};
-            live = !t.cull || !brick_reject<S>(t, g, lo, hi);
-        }
+        const bool live = j < b1 && brick_live<S>(t, g, j, bx, by, bz);
         uint32_t m = __ballot_sync(0xFFFFFFFFu, live);
         while (m && !split) {
-            // one surviving brick at a time, 2 voxels per lane, one ballot per bitmap word
+            // one surviving brick at a time
             const int src = __ffs(m) - 1;
             m &= m - 1;
-            const int sx = __shfl_sync(0xFFFFFFFFu, bx, src), sy = __shfl_sync(0xFFFFFFFFu, by, src),
-                      sz = __shfl_sync(0xFFFFFFFFu, bz, src);
-#pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int lm = lane + 32 * h;  // local Morton index in the brick
-                const int x = 4 * sx + ((lm & 1) | ((lm >> 2) & 2));
-                const int y = 4 * sy + (((lm >> 1) & 1) | ((lm >> 3) & 2));
-                const int z = 4 * sz + (((lm >> 2) & 1) | ((lm >> 4) & 2));
-                const bool in = x >= t.lo[0] && x <= t.hi[0] && y >= t.lo[1] && y <= t.hi[1] && z >= t.lo[2] &&
-                                z <= t.hi[2];
-                const uint32_t w = __ballot_sync(0xFFFFFFFFu, in && voxel_pass<S>(t, g, x, y, z));
-                if (lane == h && w) atomicOr(bm + ((morton3((uint32_t)sx, (uint32_t)sy, (uint32_t)sz) << 1) | h), w);
-            }
+            brick_voxels<S>(t, g, bm, __shfl_sync(0xFFFFFFFFu, bx, src), __shfl_sync(0xFFFFFFFFu, by, src),
+                            __shfl_sync(0xFFFFFFFFu, bz, src), lane);
         }
         while (m) {
             // up to 4 surviving bricks: lane = (brick, sub-brick)
@@ -472,22 +482,78 @@ __device__ __forceinline__ void load_tri(const float *__restrict__ pts, const in
     }
 }
 
-__device__ __forceinline__ void shfl_tri(Tri &dst, const Tri &src, int lane) {
-    const float *s = reinterpret_cast<const float *>(&src);
-    float *d = reinterpret_cast<float *>(&dst);
+// The bricks of the warp's in-warp triangles (lane i's triangle st[i] when
+// it has cnt > 0 bricks), packed across triangles: rounds of 32 (triangle,
+// brick) items, each lane culling one brick of its item's triangle (read from
+// shared memory: the 39-word stride is odd, so distinct triangles fall in
+// distinct banks); the surviving bricks are then tested one at a time by the
+// whole warp, the current triangle held in registers.
+template <bool S>
+__device__ __forceinline__ void warp_packed(const BatchDev &bd, const Tri *st, int m, uint32_t cnt, int lane) {
+    uint32_t incl = cnt;
 #pragma unroll
-    for (int i = 0; i < (int)(sizeof(Tri) / 4); ++i) d[i] = __shfl_sync(0xFFFFFFFFu, s[i], lane);
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    const uint32_t excl = incl - cnt;
+    int cur = -1;  // lane whose triangle is held in ct
+    Tri ct;
+    GridParams cg;
+    uint32_t *cbm = nullptr;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t item = base + lane;
+        // owner lane: the number of lanes whose inclusive count is <= item
+        int pos = 0;
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, pos + step - 1);
+            if (v <= item) pos += step;
+        }
+        const bool valid = item < total;
+        const int src = valid ? pos : 0;
+        const int wm = __shfl_sync(0xFFFFFFFFu, m, src);
+        const uint32_t j = item - __shfl_sync(0xFFFFFFFFu, excl, src);
+        int bx = 0, by = 0, bz = 0;
+        bool live = false;
+        if (valid) {
+            const GridParams g = *bd.mesh[wm].gp;
+            live = brick_live<S>(st[src], g, j, bx, by, bz);
+        }
+        uint32_t lm = __ballot_sync(0xFFFFFFFFu, live);
+        while (lm) {
+            const int s = __ffs(lm) - 1;
+            lm &= lm - 1;
+            const int own = __shfl_sync(0xFFFFFFFFu, src, s);
+            if (own != cur) {
+                cur = own;
+                ct = st[own];
+                const int mm = __shfl_sync(0xFFFFFFFFu, m, own);
+                cg = *bd.mesh[mm].gp;
+                cbm = reinterpret_cast<uint32_t *>(bd.mesh[mm].bits);
+            }
+            brick_voxels<S>(ct, cg, cbm, __shfl_sync(0xFFFFFFFFu, bx, s), __shfl_sync(0xFFFFFFFFu, by, s),
+                            __shfl_sync(0xFFFFFFFFu, bz, s), lane);
+        }
+    }
 }
 
 // One thread per triangle of the batch (global index -> mesh by tri_off):
-// setup, then either its own serial test (grid bbox <= serial_max voxels) or
-// queue entries of <= warp_max bricks.  INPLACE (no queue given): the
-// triangle's warp walks its bricks right here instead.
+// setup, then
+//   tier 0 (grid bbox <= serial_max voxels): its own serial row-by-row test;
+//   tier 1 (<= inplace_max 4^3 bricks, or any size when INPLACE): its bricks
+//     are walked by this warp right after setup (warp_packed), shared with the
+//     warp's other tier-1 triangles;
+//   tier 2 (more bricks): queue entries of <= warp_max bricks for
+//     k_voxelize_bricks, which balances them across the GPU.
 template <bool S, bool INPLACE>
-__global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(BatchDev bd, int64_t total, VoxTuning tune,
+__global__ void __launch_bounds__(256, 2) k_voxelize(BatchDev bd, int64_t total, VoxTuning tune,
                                                                     uint4 *__restrict__ big, uint32_t big_cap,
                                                                     uint32_t *__restrict__ big_count) {
+    __shared__ Tri s_tri[8][32];  // the warp's tier-1 triangles
     const int lane = threadIdx.x & 31;
+    Tri *st = s_tri[threadIdx.x >> 5];
     const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = warp0; base < total; base += stride) {
@@ -505,13 +571,15 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(BatchDev bd, 
             const uint64_t vol = (uint64_t)(t.hi[0] - t.lo[0] + 1) * (uint64_t)(t.hi[1] - t.lo[1] + 1) *
                                  (uint64_t)(t.hi[2] - t.lo[2] + 1);
             nb = brick_count(t);
-            tier = vol <= (uint64_t)tune.serial_max ? 0 : 1;
+            tier = vol <= (uint64_t)tune.serial_max ? 0 : (INPLACE || nb <= tune.inplace_max) ? 1 : 2;
             if (tier == 0) {
                 HitSink sink{reinterpret_cast<uint32_t *>(md.bits)};
                 for (int z = t.lo[2]; z <= t.hi[2]; ++z)
                     for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
                 sink.flush();
-            } else if (!INPLACE) {
+            } else if (tier == 1) {
+                st[lane] = t;
+            } else {
                 const uint32_t eb = tune.warp_max;
                 const uint32_t ne = (nb + eb - 1) / eb;
                 const uint32_t at = atomicAdd(big_count, ne);
@@ -521,19 +589,10 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3) k_voxelize(BatchDev bd, 
                 }
             }
         }
-        if (INPLACE) {
-            uint32_t coop = __ballot_sync(0xFFFFFFFFu, tier == 1);
-            while (coop) {
-                const int src = __ffs(coop) - 1;
-                coop &= coop - 1;
-                Tri w;
-                shfl_tri(w, t, src);
-                const uint32_t wnb = __shfl_sync(0xFFFFFFFFu, nb, src);
-                const int wm = __shfl_sync(0xFFFFFFFFu, m, src);
-                const MeshDev &md = bd.mesh[wm];
-                const GridParams g = *md.gp;
-                warp_bricks<S>(w, g, reinterpret_cast<uint32_t *>(md.bits), 0, wnb, 0, 32, tune.split != 0);
-            }
+        if (__any_sync(0xFFFFFFFFu, tier == 1)) {
+            __syncwarp();
+            warp_packed<S>(bd, st, m, tier == 1 ? nb : 0u, lane);
+            __syncwarp();  // st is rewritten by the next round
         }
     }
 }
@@ -586,6 +645,35 @@ __global__ void k_index_range(const int32_t *__restrict__ idx, int64_t n, int32_
     }
 }
 
+// Min/max index of each job of a table (jobs whose blocks follow block_off).
+__global__ void k_index_ranges_init(int32_t *mm, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        mm[2 * i] = 0x7FFFFFFF;
+        mm[2 * i + 1] = (int32_t)0x80000000;
+    }
+}
+
+__global__ void k_index_ranges(const IndexJob *__restrict__ jobs, int n, const uint32_t *__restrict__ block_off,
+                               int32_t *__restrict__ mm) {
+    const int k = find_segment(block_off, n, (uint32_t)blockIdx.x);
+    const IndexJob jb = jobs[k];
+    const int64_t nb = block_off[k + 1] - block_off[k];
+    int32_t lo = 0x7FFFFFFF, hi = (int32_t)0x80000000;
+    for (int64_t i = (blockIdx.x - block_off[k]) * (int64_t)blockDim.x + threadIdx.x; i < jb.n;
+         i += nb * blockDim.x) {
+        const int32_t v = __ldg(jb.idx + i);
+        lo = min(lo, v);
+        hi = max(hi, v);
+    }
+    lo = __reduce_min_sync(0xFFFFFFFFu, lo);
+    hi = __reduce_max_sync(0xFFFFFFFFu, hi);
+    if ((threadIdx.x & 31) == 0) {
+        atomicMin(mm + 2 * k, lo);
+        atomicMax(mm + 2 * k + 1, hi);
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaStream_t st) {
@@ -594,6 +682,17 @@ cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaS
     const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, 148 * 8));
     k_index_range<<<blocks, 256, 0, st>>>(idx, n, mm);
     count_launches(1);
+    return cudaGetLastError();
+}
+
+uint32_t index_blocks(int64_t n) { return (uint32_t)std::max<int64_t>(1, std::min<int64_t>((n + 2047) / 2048, 256)); }
+
+cudaError_t launch_index_ranges(const IndexJob *jobs, int n, const uint32_t *block_off, uint32_t total_blocks,
+                                int32_t *mm, cudaStream_t st) {
+    if (n == 0) return cudaSuccess;
+    k_index_ranges_init<<<(n + 127) / 128, 128, 0, st>>>(mm, n);
+    k_index_ranges<<<total_blocks, 256, 0, st>>>(jobs, n, block_off, mm);
+    count_launches(2);
     return cudaGetLastError();
 }
 
@@ -613,7 +712,10 @@ cudaError_t launch_voxelize(const BatchDev &b, int64_t total, bool strict, const
         const int64_t want = (total + 255) / 256;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * 16));
         const bool inplace = big == nullptr || big_cap == 0;
-#define SVO_VOX(S_, I_) k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(b, total, tune, big, big_cap, counters)
+        // Few triangles: the in-warp tier would leave most SMs idle, the queue spreads the bricks.
+        VoxTuning tn = tune;
+        if (!inplace && total < (int64_t)num_sms * 256) tn.inplace_max = 0;
+#define SVO_VOX(S_, I_) k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(b, total, tn, big, big_cap, counters)
         if (strict) {
             if (inplace) SVO_VOX(true, true); else SVO_VOX(true, false);
         } else {

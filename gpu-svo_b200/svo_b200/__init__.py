@@ -62,7 +62,8 @@ class _Aabb(C.Structure):
 
 
 class Tuning(C.Structure):
-    _fields_ = [("serial_max", C.c_uint32), ("warp_max", C.c_uint32), ("split", C.c_uint32)]
+    _fields_ = [("serial_max", C.c_uint32), ("warp_max", C.c_uint32), ("split", C.c_uint32),
+                ("inplace_max", C.c_uint32)]
 
 
 class MeshDesc(C.Structure):
@@ -213,14 +214,16 @@ class Context:
 
     @property
     def tuning(self) -> tuple:
+        """(serial_max, warp_max, split, inplace_max) of the voxelizer work split."""
         t = Tuning()
         _check(lib().svo_ctx_get_tuning(self._h, C.byref(t)))
-        return (t.serial_max, t.warp_max, t.split)
+        return (t.serial_max, t.warp_max, t.split, t.inplace_max)
 
     @tuning.setter
     def tuning(self, value) -> None:
-        t = Tuning(int(value[0]), int(value[1]), int(value[2]) if len(value) > 2 else 0)
-        _check(lib().svo_ctx_set_tuning(self._h, C.byref(t)))
+        cur = self.tuning
+        v = tuple(int(x) for x in value) + cur[len(value):]
+        _check(lib().svo_ctx_set_tuning(self._h, C.byref(Tuning(*v))))
 
     def build(self, points, tris, res, flags: int = 0, stream: int = 0) -> "Result":
         """svo_build.  points float32[n,3] and tris int32[m,3] (tris=None: soup),

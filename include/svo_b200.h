@@ -91,14 +91,17 @@ int svo_ctx_create(int device, svo_ctx **out);
 void svo_ctx_destroy(svo_ctx *ctx);
 
 /* Voxelizer work split: triangles whose grid bbox has at most serial_max
- * voxels are tested by one thread; larger ones are cut into queue entries of
- * at most warp_max 4x4x4 bricks, one warp per entry.  Results do not depend on
- * these values, only the speed.  No counterpart in the reference
- * (one thread per triangle there, src/SVO.cu:37-188). */
+ * voxels are tested by one thread; triangles of at most inplace_max 4x4x4
+ * bricks are walked by the warp that set them up, packed 32 bricks per round
+ * across the warp's triangles; larger ones are cut into queue entries of at
+ * most warp_max bricks, one warp per entry.  Results do not depend on these
+ * values, only the speed.  No counterpart in the reference (one thread per
+ * triangle there, src/SVO.cu:37-188). */
 typedef struct svo_tuning {
     uint32_t serial_max;
     uint32_t warp_max;
-    uint32_t split; /* also cull the 2x2x2 sub-bricks of surviving bricks */
+    uint32_t split; /* also cull the 2x2x2 sub-bricks of surviving bricks (queue tier) */
+    uint32_t inplace_max;
 } svo_tuning;
 int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t);
 int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t);
@@ -164,8 +167,10 @@ int svo_build_batch(svo_ctx *ctx, const svo_mesh_desc *descs, int n, void *strea
  * mesh's exact node count and output size; svo_batch_emit then writes the
  * octrees of meshes [first, first + count) in one pass -- call it for
  * consecutive ranges that fit the memory at hand and free their results
- * between calls.  All meshes of a batch use `flags` (descs[i].flags is
- * ignored).  The batch holds its scratch until svo_batch_free. */
+ * between calls.  The node/vertex/edge/key arrays of the results of one
+ * svo_batch_emit call share one device block, released when the last of
+ * those results is freed.  All meshes of a batch use `flags` (descs[i].flags
+ * is ignored).  The batch holds its scratch until svo_batch_free. */
 typedef struct svo_batch svo_batch;
 int svo_batch_create(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, void *stream,
                      svo_batch **out);
