@@ -49,8 +49,10 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5", "heightfield", "batch256"],
+    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5", "heightfield", "batch256", "serve"],
                     default="torus_slivers")
+    ap.add_argument("--rates", default="200,500,1000,2000,5000", help="serve: Poisson arrival rates (req/s)")
+    ap.add_argument("--window", type=float, default=1.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--flags", type=int, default=-1, help="override the workload's build flags (SVO_FLAG_*)")
     ap.add_argument("--wave-gb", type=float, default=48.0, help="batch256: device bytes of results per emit wave")
     ap.add_argument("--res", type=int, default=0, help="override the workload's resolution")
@@ -213,7 +215,7 @@ def run_reference(args, rank: int):
     if rank != 0:
         return
     threads = os.cpu_count() or 1
-    if args.workload == "batch256":
+    if args.workload in ("batch256", "serve"):
         from svo_b200 import meshgen
 
         sample_meshes = batch_cpu_sample(meshgen.batch(256, seed=3))
@@ -526,6 +528,93 @@ def run_batch(args, rank: int, world: int):
     ctx.close()
 
 
+def run_serve(args, rank: int, world: int):
+    """Poisson request stream: meshes of the batch distribution (64 resident
+    meshes, seed 4), resolutions drawn from {64, 128, 256, 512, 1024} (seed 5),
+    arrivals at each rate for --window seconds.  Served: svo_server with 3
+    workers, batches of up to 64, 40 GB admission budget.  Plain: the same
+    requests one svo_build at a time in arrival order (one worker, batches of
+    one).  Latency = build finished - submitted, from the server's clock."""
+    import torch
+
+    import svo_b200 as S
+    from svo_b200 import meshgen
+
+    dev = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(dev)
+    rng = np.random.default_rng(4)
+    pool = [meshgen.batch_mesh(rng) for _ in range(64)]
+    dpool = [(torch.from_numpy(p).cuda(), torch.from_numpy(t).cuda(), t.shape[0]) for p, t in pool]
+    ctx = S.Context(dev)
+    flags = 0 if args.flags < 0 else args.flags
+    budget = 40 * 10**9
+    rates = [float(x) for x in args.rates.split(",") if x]
+
+    def run(rate, workers, max_batch, reqs, arrivals):
+        srv = S.Server(ctx, budget, workers=workers, max_batch=max_batch, flags=flags)
+        tickets = [None] * len(reqs)
+        t0 = time.perf_counter()
+
+        def client():
+            for i, ((mi, res), at) in enumerate(zip(reqs, arrivals)):
+                d = at - (time.perf_counter() - t0)
+                if d > 0:
+                    time.sleep(d)
+                p, t, _ = dpool[mi]
+                tickets[i] = srv.submit(p, t, res)
+
+        th = threading.Thread(target=client)
+        th.start()
+        lat = []
+        for _ in range(len(reqs)):  # completion order: each result released as soon as it is built
+            t, r, st, l = srv.next()
+            if st != 0:
+                raise RuntimeError(f"request {t} failed: {st}")
+            lat.append(l)
+            srv.release(t)
+        th.join()
+        span = time.perf_counter() - t0
+        batches = srv.stats()["batches"]
+        srv.close()
+        lat = np.array(lat) * 1e3
+        tris = sum(dpool[mi][2] for mi, _ in reqs)
+        return {"p50_ms": float(np.percentile(lat, 50)), "p99_ms": float(np.percentile(lat, 99)),
+                "req_per_s": len(reqs) / span, "tris_per_s": tris / span, "batches": int(batches),
+                "span_s": span}
+
+    # warm-up: every resolution once, both paths
+    warm = [(i % 64, r) for i, r in enumerate((64, 128, 256, 512, 1024) * 2)]
+    run(1000.0, 3, 64, warm, [0.0] * len(warm))
+    run(1000.0, 1, 1, warm, [0.0] * len(warm))
+    launches0 = S.kernel_launches()
+    out = []
+    with ClockSampler(dev) as clocks:
+        for k, rate in enumerate(rates):
+            rr = np.random.default_rng(5 + k)
+            n = max(50, min(1500, int(rate * args.window)))
+            arrivals = np.cumsum(rr.exponential(1.0 / rate, size=n)).tolist()
+            reqs = [(int(rr.integers(0, 64)), int(rr.choice([64, 128, 256, 512, 1024]))) for _ in range(n)]
+            served = run(rate, 3, 64, reqs, arrivals)
+            plain = run(rate, 1, 1, reqs, arrivals)
+            out.append({"rate": rate, "requests": n, "served": served, "plain": plain})
+    launches = S.kernel_launches() - launches0
+    ctx.close()
+    if rank == 0:
+        top = out[-1]
+        line = {
+            "metric": "tris/s served (p50/p99 latency per rate)", "value": top["served"]["tris_per_s"],
+            "unit": "tris/s", "n_gpus": world, "steps": len(out), "warmup": 2, "ms_per_step": None,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": "serve_poisson", "mesh_pool": "64 meshes of the batch distribution (seed 4)",
+                       "resolutions": "64/128/256/512/1024", "budget_bytes": budget, "served_workers": 3,
+                       "served_max_batch": 64, "flags": flags, "window_s": args.window,
+                       "parallelism": f"replicas{world}"},
+            "rates": out, "e2e": None, "roofline": None, "cpu_baseline": None, "clocks": clocks.summary(),
+            "gpu_launches": launches,
+        }
+        print(json.dumps(line), flush=True)
+
+
 def main():
     args = parse_args()
     rank, world = dist_setup(args.gpus)
@@ -534,6 +623,8 @@ def main():
             run_reference(args, rank)
         elif args.workload == "batch256":
             run_batch(args, rank, world)
+        elif args.workload == "serve":
+            run_serve(args, rank, world)
         else:
             run_ours(args, rank, world)
     finally:

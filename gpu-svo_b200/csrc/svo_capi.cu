@@ -22,7 +22,7 @@ using namespace svo;
 struct svo_ctx {
     int device = 0;
     int num_sms = 148;
-    cudaMemPool_t pool = nullptr;      // per-build scratch (the device's default pool)
+    cudaMemPool_t pool = nullptr;      // per-build scratch
     cudaMemPool_t out_pool = nullptr;  // result arrays, kept apart so scratch never splits their blocks
     VoxTuning tune;
 };
@@ -874,20 +874,47 @@ int svo_ctx_create(int device, svo_ctx **out) {
     svo_ctx *c = new svo_ctx();
     c->device = device;
     c->num_sms = prop.multiProcessorCount;
-    SVO_TRY(cudaDeviceGetDefaultMemPool(&c->pool, device), "mem pool");
-    uint64_t keep = UINT64_MAX;  // keep freed blocks cached for the next build
-    SVO_TRY(cudaMemPoolSetAttribute(c->pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
+    // Two pools of its own: per-build scratch, and result arrays (kept apart
+    // so scratch never splits their blocks).  Freed blocks stay cached.
     cudaMemPoolProps props{};
     props.allocType = cudaMemAllocationTypePinned;
     props.handleTypes = cudaMemHandleTypeNone;
     props.location.type = cudaMemLocationTypeDevice;
     props.location.id = device;
-    if (cudaMemPoolCreate(&c->out_pool, &props) != cudaSuccess) {
-        delete c;
-        return fail(SVO_ERR_CUDA, "result memory pool");
+    uint64_t keep = UINT64_MAX;
+    for (cudaMemPool_t *pp : {&c->pool, &c->out_pool}) {
+        if (cudaMemPoolCreate(pp, &props) != cudaSuccess ||
+            cudaMemPoolSetAttribute(*pp, cudaMemPoolAttrReleaseThreshold, &keep) != cudaSuccess) {
+            svo_ctx_destroy(c);
+            cudaGetLastError();
+            return fail(SVO_ERR_CUDA, "memory pool");
+        }
     }
-    SVO_TRY(cudaMemPoolSetAttribute(c->out_pool, cudaMemPoolAttrReleaseThreshold, &keep), "pool attr");
     *out = c;
+    return SVO_OK;
+}
+
+int svo_ctx_reserve(svo_ctx *ctx, uint64_t result_bytes, uint64_t scratch_bytes, void *stream) {
+    if (!ctx) return fail(SVO_ERR_INVALID_ARGUMENT, "null context");
+    SVO_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const std::pair<cudaMemPool_t, uint64_t> want[2] = {{ctx->out_pool, result_bytes}, {ctx->pool, scratch_bytes}};
+    for (const auto &w : want) {
+        if (w.second == 0) continue;
+        void *p = nullptr;
+        if (cudaMallocFromPoolAsync(&p, w.second, w.first, st) != cudaSuccess) {
+            cudaGetLastError();
+            return fail(SVO_ERR_OUT_OF_MEMORY, "cannot reserve %llu bytes", (unsigned long long)w.second);
+        }
+        SVO_TRY(cudaFreeAsync(p, st), "free");
+    }
+    SVO_TRY(cudaStreamSynchronize(st), "reserve");
+    return SVO_OK;
+}
+
+int svo_ctx_device(const svo_ctx *ctx, int *device) {
+    if (!ctx || !device) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    *device = ctx->device;
     return SVO_OK;
 }
 
@@ -895,10 +922,9 @@ int svo_ctx_create(int device, svo_ctx **out) {
 // outstanding is released once they are freed.
 void svo_ctx_destroy(svo_ctx *ctx) {
     if (!ctx) return;
-    if (ctx->out_pool) {
-        cudaSetDevice(ctx->device);
-        cudaMemPoolDestroy(ctx->out_pool);
-    }
+    cudaSetDevice(ctx->device);
+    if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
+    if (ctx->out_pool) cudaMemPoolDestroy(ctx->out_pool);
     delete ctx;
 }
 

@@ -1,0 +1,303 @@
+// svo_server.cpp -- a request loop around the batched build (continuous
+// batching under a device-memory budget).  No counterpart in the reference,
+// which builds one mesh per process (main.cpp:8-14).
+//
+// Requests wait in a FIFO queue.  Each worker thread owns a CUDA stream and
+// repeatedly takes the longest queue prefix that fits the budget (at most
+// max_batch requests), builds it as one batch (svo_batch_create, then one
+// svo_batch_emit for all of it) and publishes the results.  While one
+// worker's batch is on the GPU the others admit what arrived meanwhile and
+// launch on their own streams, so batches of different sizes overlap on the
+// device.  Admission reserves svo_estimate_bytes() per request; once a batch
+// is built the reservation becomes the exact bytes of the result, held until
+// the client releases it.
+#include <chrono>
+#include <condition_variable>
+#include <deque>
+#include <mutex>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "svo_b200.h"
+#include "svo_host.h"
+
+struct svo_server {
+    struct Req {
+        uint64_t ticket = 0;
+        svo_mesh_desc desc{};
+        uint64_t est = 0;   // bytes reserved at admission
+        uint64_t held = 0;  // bytes reserved now
+        std::chrono::steady_clock::time_point t_submit, t_start, t_done;
+        bool done = false;
+        int status = SVO_OK;
+        svo_result *result = nullptr;
+    };
+    svo_ctx *ctx = nullptr;
+    svo_server_config cfg{};
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<Req *> queue;
+    std::deque<uint64_t> finished;  // tickets in completion order, not yet taken by svo_server_next
+    std::unordered_map<uint64_t, Req *> reqs;
+    uint64_t next_ticket = 1;
+    uint64_t reserved = 0;
+    int busy = 0;  // workers with a batch on the device
+    bool stop = false;
+    std::vector<std::thread> workers;
+    std::vector<cudaStream_t> streams;
+    uint64_t batches = 0, built = 0;
+    double build_s = 0.0, queue_s = 0.0;  // summed over batches / requests
+};
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+int server_fail(int code, const char *msg) {
+    svo::host::set_error(msg);
+    return code;
+}
+
+int max_res(const int r[3]) { return std::max(r[0], std::max(r[1], r[2])); }
+
+// The longest FIFO prefix that fits the budget; a request larger than the
+// whole budget runs alone when nothing else is reserved.
+bool admissible(const svo_server *s) {
+    if (s->queue.empty()) return false;
+    const uint64_t e = s->queue.front()->est;
+    return s->reserved + e <= s->cfg.mem_budget || s->reserved == 0;
+}
+
+void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &take) {
+    const int n = (int)take.size();
+    const auto t0 = Clock::now();
+    std::vector<svo_mesh_desc> d(n);
+    for (int i = 0; i < n; ++i) d[i] = take[i]->desc;
+    std::vector<svo_result *> out(n, nullptr);
+    std::vector<int> status(n, SVO_OK);
+    std::vector<uint64_t> bytes(n, 0);
+    svo_batch *b = nullptr;
+    int rc = svo_batch_create(s->ctx, d.data(), n, s->cfg.flags, st, &b);
+    if (rc == SVO_OK) {
+        rc = svo_batch_emit(b, 0, n, out.data(), status.data());
+        for (int i = 0; i < n; ++i)
+            if (status[i] == SVO_OK) bytes[i] = (uint64_t)svo_batch_mesh_output_bytes(b, i);
+        svo_batch_free(b);
+    } else {
+        for (int i = 0; i < n; ++i) status[i] = rc;
+    }
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        const auto now = Clock::now();
+        for (int i = 0; i < n; ++i) {
+            svo_server::Req *r = take[i];
+            s->reserved -= r->held;
+            r->held = bytes[i];
+            s->reserved += r->held;
+            r->result = out[i];
+            r->status = status[i];
+            r->t_done = now;
+            r->done = true;
+            s->finished.push_back(r->ticket);
+        }
+        s->batches += 1;
+        s->built += (uint64_t)n;
+        s->build_s += std::chrono::duration<double>(now - t0).count();
+        for (int i = 0; i < n; ++i) s->queue_s += std::chrono::duration<double>(take[i]->t_start - take[i]->t_submit).count();
+        --s->busy;
+    }
+    s->cv_done.notify_all();
+    s->cv_work.notify_all();
+}
+
+void worker(svo_server *s, int w) {
+    int dev = 0;
+    svo_ctx_device(s->ctx, &dev);
+    cudaSetDevice(dev);
+    cudaStream_t st = s->streams[w];
+    for (;;) {
+        std::vector<svo_server::Req *> take;
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_work.wait(lk, [&] { return admissible(s) || (s->stop && s->queue.empty()); });
+            if (s->queue.empty()) return;  // stopping and drained
+            const auto now = Clock::now();
+            while (!s->queue.empty() && (int)take.size() < s->cfg.max_batch) {
+                svo_server::Req *r = s->queue.front();
+                if (s->reserved + r->est > s->cfg.mem_budget && !(s->reserved == 0 && take.empty())) break;
+                s->reserved += r->est;
+                r->held = r->est;
+                r->t_start = now;
+                take.push_back(r);
+                s->queue.pop_front();
+            }
+            ++s->busy;
+        }
+        run_batch(s, st, take);
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+uint64_t svo_estimate_bytes(int64_t n_points, int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags) {
+    const int r[3] = {res_x, res_y, res_z};
+    uint64_t side = 1;
+    while (side < (uint64_t)max_res(r)) side *= 2;
+    const uint64_t nt = n_tris > 0 ? (uint64_t)n_tris : (uint64_t)std::max<int64_t>(n_points, 0) / 3;
+    const uint64_t inputs = 12 * (uint64_t)std::max<int64_t>(n_points, 0) + 12 * nt;
+    const uint64_t scratch = side * side * side / 7 + 32 * nt + (1u << 20);
+    const uint64_t nodes = 16 * side * side;  // a closed surface spanning the grid
+    uint64_t per_node = sizeof(svo_node);
+    if (!(flags & SVO_FLAG_NO_VERT_EDGE)) per_node += 8 * sizeof(svo_vertex) + 12 * sizeof(svo_edge);
+    if (flags & SVO_FLAG_DEDUP) per_node += 8 * 4;
+    return inputs + scratch + nodes * per_node;
+}
+
+int svo_server_create(svo_ctx *ctx, const svo_server_config *cfg, svo_server **out) {
+    if (!ctx || !cfg || !out) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    if (cfg->workers < 1 || cfg->workers > 64 || cfg->max_batch < 1 || cfg->mem_budget == 0)
+        return server_fail(SVO_ERR_INVALID_ARGUMENT, "workers in [1, 64], max_batch >= 1, mem_budget > 0");
+    int dev = 0;
+    svo_ctx_device(ctx, &dev);
+    if (cudaSetDevice(dev) != cudaSuccess) return server_fail(SVO_ERR_CUDA, "cudaSetDevice");
+    svo_server *s = new svo_server();
+    s->ctx = ctx;
+    s->cfg = *cfg;
+    for (int w = 0; w < cfg->workers; ++w) {
+        cudaStream_t st = nullptr;
+        if (cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking) != cudaSuccess) {
+            for (cudaStream_t x : s->streams) cudaStreamDestroy(x);
+            delete s;
+            return server_fail(SVO_ERR_CUDA, "worker stream");
+        }
+        s->streams.push_back(st);
+    }
+    // Map the budget's memory into the context's pools now, so that batches
+    // carve cached memory instead of growing the pools while serving.
+    svo_ctx_reserve(ctx, cfg->mem_budget, cfg->mem_budget / 4, s->streams[0]);
+    for (int w = 0; w < cfg->workers; ++w) s->workers.emplace_back(worker, s, w);
+    *out = s;
+    return SVO_OK;
+}
+
+int svo_server_submit(svo_server *s, const svo_mesh_desc *desc, uint64_t *ticket) {
+    if (!s || !desc || !ticket) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    auto *r = new svo_server::Req();
+    r->desc = *desc;
+    r->est = svo_estimate_bytes(desc->n_points, desc->n_tris, desc->res[0], desc->res[1], desc->res[2],
+                                s->cfg.flags);
+    r->t_submit = Clock::now();
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->stop) {
+            delete r;
+            return server_fail(SVO_ERR_INVALID_ARGUMENT, "server is shutting down");
+        }
+        r->ticket = s->next_ticket++;
+        s->reqs[r->ticket] = r;
+        s->queue.push_back(r);
+        *ticket = r->ticket;
+    }
+    s->cv_work.notify_one();
+    return SVO_OK;
+}
+
+int svo_server_wait(svo_server *s, uint64_t ticket, int64_t timeout_us, svo_result **result, int *status,
+                    double *latency_s) {
+    if (!s) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null server");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto it = s->reqs.find(ticket);
+    if (it == s->reqs.end()) return server_fail(SVO_ERR_INVALID_ARGUMENT, "unknown ticket");
+    svo_server::Req *r = it->second;
+    auto ready = [&] { return r->done; };
+    if (timeout_us < 0) {
+        s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), ready)) {
+        return server_fail(SVO_ERR_TIMEOUT, "request not finished");
+    }
+    if (result) *result = r->result;
+    if (status) *status = r->status;
+    if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+    return SVO_OK;
+}
+
+int svo_server_next(svo_server *s, int64_t timeout_us, uint64_t *ticket, svo_result **result, int *status,
+                    double *latency_s) {
+    if (!s || !ticket) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    std::unique_lock<std::mutex> lk(s->mu);
+    auto ready = [&] { return !s->finished.empty(); };
+    if (timeout_us < 0) {
+        s->cv_done.wait(lk, ready);
+    } else if (!s->cv_done.wait_for(lk, std::chrono::microseconds(timeout_us), ready)) {
+        return server_fail(SVO_ERR_TIMEOUT, "no finished request");
+    }
+    *ticket = s->finished.front();
+    s->finished.pop_front();
+    svo_server::Req *r = s->reqs.at(*ticket);
+    if (result) *result = r->result;
+    if (status) *status = r->status;
+    if (latency_s) *latency_s = std::chrono::duration<double>(r->t_done - r->t_submit).count();
+    return SVO_OK;
+}
+
+int svo_server_release(svo_server *s, uint64_t ticket) {
+    if (!s) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null server");
+    svo_result *res = nullptr;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return server_fail(SVO_ERR_INVALID_ARGUMENT, "unknown ticket");
+        svo_server::Req *r = it->second;
+        if (!r->done) return server_fail(SVO_ERR_INVALID_ARGUMENT, "request not finished");
+        for (auto f = s->finished.begin(); f != s->finished.end(); ++f)
+            if (*f == ticket) {
+                s->finished.erase(f);
+                break;
+            }
+        s->reserved -= r->held;
+        res = r->result;
+        s->reqs.erase(it);
+        delete r;
+    }
+    svo_result_free(res);
+    s->cv_work.notify_all();
+    return SVO_OK;
+}
+
+int svo_server_stats(const svo_server *s, svo_server_stats_t *out) {
+    if (!s || !out) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    auto *m = const_cast<svo_server *>(s);
+    std::lock_guard<std::mutex> lk(m->mu);
+    out->queued = (int64_t)s->queue.size();
+    out->busy_workers = s->busy;
+    out->reserved_bytes = s->reserved;
+    out->batches = s->batches;
+    out->built = s->built;
+    out->build_seconds = s->build_s;
+    out->queue_seconds = s->queue_s;
+    return SVO_OK;
+}
+
+void svo_server_destroy(svo_server *s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    for (auto &t : s->workers) t.join();
+    for (auto &kv : s->reqs) {
+        svo_result_free(kv.second->result);
+        delete kv.second;
+    }
+    for (cudaStream_t st : s->streams) cudaStreamDestroy(st);
+    delete s;
+}
+
+}  // extern "C"

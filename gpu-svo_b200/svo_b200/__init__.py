@@ -25,6 +25,7 @@ ERR_IO = 6
 ERR_PARSE = 7
 ERR_UNSUPPORTED = 8
 ERR_DEVICE_TIMEOUT = 9
+ERR_TIMEOUT = 10
 
 FLAG_FULL_NEIGHBORS = 0x1
 FLAG_DEDUP = 0x2
@@ -77,6 +78,16 @@ class MeshDesc(C.Structure):
     ]
 
 
+class ServerConfig(C.Structure):
+    _fields_ = [("mem_budget", C.c_uint64), ("workers", C.c_int), ("max_batch", C.c_int), ("flags", C.c_uint32)]
+
+
+class ServerStats(C.Structure):
+    _fields_ = [("queued", C.c_int64), ("busy_workers", C.c_int), ("reserved_bytes", C.c_uint64),
+                ("batches", C.c_uint64), ("built", C.c_uint64), ("build_seconds", C.c_double),
+                ("queue_seconds", C.c_double)]
+
+
 _lib = None
 
 
@@ -126,6 +137,19 @@ def lib() -> C.CDLL:
         L.svo_batch_emit.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp), C.POINTER(C.c_int)]
         L.svo_batch_free.argtypes = [vp]
         L.svo_batch_free.restype = None
+        L.svo_estimate_bytes.argtypes = [i64, i64, C.c_int, C.c_int, C.c_int, C.c_uint32]
+        L.svo_estimate_bytes.restype = C.c_uint64
+        L.svo_server_create.argtypes = [vp, C.POINTER(ServerConfig), C.POINTER(vp)]
+        L.svo_server_submit.argtypes = [vp, C.POINTER(MeshDesc), C.POINTER(C.c_uint64)]
+        L.svo_server_wait.argtypes = [vp, C.c_uint64, i64, C.POINTER(vp), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_double)]
+        L.svo_server_release.argtypes = [vp, C.c_uint64]
+        L.svo_server_next.argtypes = [vp, i64, C.POINTER(C.c_uint64), C.POINTER(vp), C.POINTER(C.c_int),
+                                      C.POINTER(C.c_double)]
+        L.svo_server_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        L.svo_server_destroy.argtypes = [vp]
+        L.svo_server_destroy.restype = None
+        L.svo_ctx_device.argtypes = [vp, C.POINTER(C.c_int)]
         L.svo_kernel_launches.restype = i64
         L.svo_result_num_dedup.argtypes = [vp, C.c_int]
         L.svo_result_num_dedup.restype = i64
@@ -258,6 +282,76 @@ class Context:
         return results, list(st), rc
 
 
+def estimate_bytes(n_points: int, n_tris: int, res, flags: int = 0) -> int:
+    """svo_estimate_bytes: the server's admission estimate for one mesh."""
+    return int(lib().svo_estimate_bytes(n_points, n_tris, *_res3(res), flags))
+
+
+class Server:
+    """svo_server: continuous batching of build requests under a device-memory
+    budget.  Mesh arrays must stay alive until their request is released."""
+
+    def __init__(self, ctx: "Context", mem_budget: int, workers: int = 2, max_batch: int = 64, flags: int = 0):
+        cfg = ServerConfig(int(mem_budget), int(workers), int(max_batch), int(flags))
+        h = C.c_void_p()
+        _check(lib().svo_server_create(ctx.handle, C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._flags = flags
+        self._keep = {}
+
+    def submit(self, points, tris, res) -> int:
+        descs, keep = _descs([(points, tris, res)], self._flags)
+        t = C.c_uint64()
+        _check(lib().svo_server_submit(self._h, descs, C.byref(t)))
+        self._keep[t.value] = (descs, keep)
+        return t.value
+
+    def wait(self, ticket: int, timeout_us: int = -1):
+        """(Result borrowed until release, status, latency seconds); None on timeout."""
+        r = C.c_void_p()
+        st = C.c_int()
+        lat = C.c_double()
+        rc = lib().svo_server_wait(self._h, ticket, timeout_us, C.byref(r), C.byref(st), C.byref(lat))
+        if rc == ERR_TIMEOUT:
+            return None
+        _check(rc)
+        return (Result(r, owned=False) if st.value == OK else None), st.value, lat.value
+
+    def next(self, timeout_us: int = -1):
+        """(ticket, Result borrowed until release, status, latency s) of the next
+        finished request in completion order; None on timeout."""
+        t = C.c_uint64()
+        r = C.c_void_p()
+        st = C.c_int()
+        lat = C.c_double()
+        rc = lib().svo_server_next(self._h, timeout_us, C.byref(t), C.byref(r), C.byref(st), C.byref(lat))
+        if rc == ERR_TIMEOUT:
+            return None
+        _check(rc)
+        return t.value, (Result(r, owned=False) if st.value == OK else None), st.value, lat.value
+
+    def release(self, ticket: int) -> None:
+        _check(lib().svo_server_release(self._h, ticket))
+        self._keep.pop(ticket, None)
+
+    def stats(self) -> dict:
+        s = ServerStats()
+        _check(lib().svo_server_stats(self._h, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
+
+    def close(self) -> None:
+        if self._h:
+            lib().svo_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 def _descs(meshes, flags):
     keep = []
     descs = (MeshDesc * len(meshes))()
@@ -317,15 +411,17 @@ class Batch:
 
 
 class Result:
-    """svo_result: device-resident octree of one build."""
+    """svo_result: device-resident octree of one build (owned: freed by
+    close(); borrowed: a server's result, valid until its ticket is released)."""
 
-    def __init__(self, h: C.c_void_p):
+    def __init__(self, h: C.c_void_p, owned: bool = True):
         self._h = h
+        self._owned = owned
 
     def close(self) -> None:
-        if self._h:
+        if self._h and self._owned:
             lib().svo_result_free(self._h)
-            self._h = None
+        self._h = None
 
     def __del__(self):
         try:

@@ -34,6 +34,7 @@ extern "C" {
 #define SVO_ERR_PARSE 7
 #define SVO_ERR_UNSUPPORTED 8
 #define SVO_ERR_DEVICE_TIMEOUT 9 /* a bounded device-side wait gave up */
+#define SVO_ERR_TIMEOUT 10       /* a host-side wait ran out (svo_server_wait) */
 
 /* ---- build flags ---------------------------------------------------------- */
 /* Default (0): the reference's effective behaviour bit for bit, including its
@@ -89,6 +90,11 @@ typedef struct svo_result svo_result;
  * per-call cudaMalloc/thrust allocations (src/SVO.cu:353-376). */
 int svo_ctx_create(int device, svo_ctx **out);
 void svo_ctx_destroy(svo_ctx *ctx);
+int svo_ctx_device(const svo_ctx *ctx, int *device);
+/* Maps device memory into the context's pools up front (result arrays,
+ * per-build scratch); builds then carve it without growing the pools.  The
+ * memory stays with the context until svo_ctx_destroy. */
+int svo_ctx_reserve(svo_ctx *ctx, uint64_t result_bytes, uint64_t scratch_bytes, void *stream);
 
 /* Voxelizer work split: triangles whose grid bbox has at most serial_max
  * voxels are tested by one thread; triangles of at most inplace_max 4x4x4
@@ -180,6 +186,49 @@ int64_t svo_batch_mesh_nodes(const svo_batch *b, int i);        /* -1 on error *
 int64_t svo_batch_mesh_output_bytes(const svo_batch *b, int i); /* device bytes of its result */
 int svo_batch_emit(svo_batch *b, int first, int count, svo_result **out, int *status_out);
 void svo_batch_free(svo_batch *b);
+
+/* ---- served builds (no counterpart in the reference) ------------------------
+ * A request loop with continuous batching: worker threads, one CUDA stream
+ * each, take the longest FIFO prefix of queued requests that fits mem_budget
+ * (at most max_batch) and build it as one batch, while the other workers
+ * admit later arrivals and overlap their batches on the device.  Admission
+ * reserves svo_estimate_bytes() per request; once built, the reservation is
+ * the exact size of the result until svo_server_release.  Mesh pointers
+ * (host or device) must stay valid until the request is finished. */
+typedef struct svo_server svo_server;
+typedef struct svo_server_config {
+    uint64_t mem_budget; /* device bytes for admitted requests and live results */
+    int workers;         /* batches on the device at once */
+    int max_batch;       /* requests per batch */
+    uint32_t flags;      /* build flags of every request */
+} svo_server_config;
+typedef struct svo_server_stats_t {
+    int64_t queued;
+    int busy_workers;
+    uint64_t reserved_bytes;
+    uint64_t batches; /* batches built so far */
+    uint64_t built;   /* requests built so far */
+    double build_seconds; /* wall time of all batches (summed over workers) */
+    double queue_seconds; /* time requests waited for admission (summed) */
+} svo_server_stats_t;
+/* Device bytes admission reserves for a mesh: inputs, scratch of a res^3
+ * grid and the outputs of 16*res^2 nodes (a closed surface spanning it). */
+uint64_t svo_estimate_bytes(int64_t n_points, int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags);
+int svo_server_create(svo_ctx *ctx, const svo_server_config *cfg, svo_server **out);
+int svo_server_submit(svo_server *s, const svo_mesh_desc *desc, uint64_t *ticket);
+/* Blocks until the request is built (timeout_us < 0: no limit; else
+ * SVO_ERR_TIMEOUT when it runs out).  *result stays owned by the server and
+ * valid until svo_server_release; latency = build finished - submitted. */
+int svo_server_wait(svo_server *s, uint64_t ticket, int64_t timeout_us, svo_result **result, int *status,
+                    double *latency_s);
+/* The next finished request in completion order (each reported once, unless
+ * released first); same outputs as svo_server_wait. */
+int svo_server_next(svo_server *s, int64_t timeout_us, uint64_t *ticket, svo_result **result, int *status,
+                    double *latency_s);
+int svo_server_release(svo_server *s, uint64_t ticket);
+int svo_server_stats(const svo_server *s, svo_server_stats_t *out);
+/* Finishes every queued request, then frees all results not yet released. */
+void svo_server_destroy(svo_server *s);
 
 /* Sorted surface-voxel Morton keys of a mesh (the first stage of svo_build:
  * same bounding cube, same voxel test, same key list as svo_result_copy_keys)

@@ -24,3 +24,14 @@ def test_exports(svo_mod):
 
 def test_cli_built(svo_mod):
     assert os.access(svo_mod.CLI_PATH, os.X_OK)
+
+
+def test_estimate_bytes_host_only(svo_mod):
+    """The admission estimate is host arithmetic: grows with resolution and triangles, drops without vertex/edge arrays."""
+    e64 = svo_mod.estimate_bytes(1000, 2000, 64)
+    e128 = svo_mod.estimate_bytes(1000, 2000, 128)
+    assert 0 < e64 < e128
+    assert svo_mod.estimate_bytes(1000, 4000, 64) > e64
+    assert svo_mod.estimate_bytes(1000, 2000, 1024, svo_mod.FLAG_NO_VERT_EDGE) < svo_mod.estimate_bytes(1000, 2000, 1024)
+    # 16 res^2 nodes of 632 bytes dominate at res 1024
+    assert 16 * 1024 ** 2 * 632 < svo_mod.estimate_bytes(0, 0, 1024) < 12e9

@@ -1,0 +1,111 @@
+"""Served builds (svo_server): every request's result is the same alone and
+in the mix -- bit for bit, whatever batch and stream it landed in."""
+import threading
+import time
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+def _same(a, b):
+    assert a.depth == b.depth
+    assert a.nodes().tobytes() == b.nodes().tobytes()
+    assert a.vertices().tobytes() == b.vertices().tobytes()
+    assert a.edges().tobytes() == b.edges().tobytes()
+    assert a.keys().tobytes() == b.keys().tobytes()
+
+
+def _requests(n, seed, res_choices=(64, 128, 256, 512)):
+    from svo_b200 import meshgen
+
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(n):
+        v, f = meshgen.batch_mesh(rng)
+        out.append((v, f, int(rng.choice(res_choices))))
+    return out
+
+
+@pytest.mark.parametrize("workers,max_batch,budget", [(2, 8, 8 << 30), (3, 64, 40 << 30), (1, 1, 1)])
+def test_mix_equals_alone(gpu_ctx, svo_mod, workers, max_batch, budget):
+    reqs = _requests(16, seed=7)
+    srv = svo_mod.Server(gpu_ctx, budget, workers=workers, max_batch=max_batch)
+    tickets = [srv.submit(*r) for r in reqs]
+    for t, (p, f, res) in zip(tickets, reqs):
+        r, st, lat = srv.wait(t)
+        assert st == 0 and lat > 0
+        _same(r, gpu_ctx.build(p, f, res))
+        srv.release(t)
+    s = srv.stats()
+    assert s["built"] == len(reqs) and s["queued"] == 0 and s["reserved_bytes"] == 0
+    srv.close()
+
+
+def test_arrivals_while_busy(gpu_ctx, svo_mod):
+    """Requests submitted from another thread while batches are on the GPU."""
+    import torch
+
+    reqs = _requests(24, seed=8, res_choices=(128, 256, 512))
+    dev = [(torch.from_numpy(p).cuda(), torch.from_numpy(f).cuda(), r) for p, f, r in reqs]
+    srv = svo_mod.Server(gpu_ctx, 16 << 30, workers=3, max_batch=4)
+    tickets = [None] * len(dev)
+
+    def client():
+        for i, m in enumerate(dev):
+            tickets[i] = srv.submit(*m)
+            time.sleep(0.0005)
+
+    th = threading.Thread(target=client)
+    th.start()
+    th.join()
+    for t, m in zip(tickets, dev):
+        r, st, _ = srv.wait(t)
+        assert st == 0
+        _same(r, gpu_ctx.build(*m))
+        srv.release(t)
+    assert srv.stats()["batches"] >= 2
+    srv.close()
+
+
+def test_failures_in_the_mix(gpu_ctx, svo_mod):
+    reqs = _requests(4, seed=9)
+    pts = np.array([[0, 0, 0], [1, 1, 1], [0.5, 0.2, 0.1]], dtype=np.float32)
+    bad = (pts, np.zeros((0, 3), np.int32), 8)
+    mix = [reqs[0], bad, reqs[1], reqs[2], bad, reqs[3]]
+    srv = svo_mod.Server(gpu_ctx, 40 << 30, workers=2, max_batch=8)
+    tickets = [srv.submit(*m) for m in mix]
+    for t, m in zip(tickets, mix):
+        r, st, _ = srv.wait(t)
+        if m is bad:
+            assert st == svo_mod.ERR_EMPTY and r is None
+        else:
+            assert st == 0
+            _same(r, gpu_ctx.build(*m))
+        srv.release(t)
+    srv.close()
+
+
+def test_wait_timeout_and_close_with_pending(gpu_ctx, svo_mod):
+    reqs = _requests(6, seed=10, res_choices=(512,))
+    srv = svo_mod.Server(gpu_ctx, 40 << 30, workers=1, max_batch=1)
+    tickets = [srv.submit(*m) for m in reqs]
+    first = srv.wait(tickets[-1], timeout_us=0)
+    assert first is None or first[1] == 0  # not finished yet, or already done
+    srv.close()  # finishes the queue and frees the unreleased results
+
+
+def test_completion_order(gpu_ctx, svo_mod):
+    reqs = _requests(10, seed=11)
+    srv = svo_mod.Server(gpu_ctx, 40 << 30, workers=2, max_batch=4)
+    tickets = {srv.submit(*m): m for m in reqs}
+    seen = set()
+    for _ in range(len(reqs)):
+        t, r, st, lat = srv.next()
+        assert st == 0 and t in tickets and t not in seen
+        seen.add(t)
+        _same(r, gpu_ctx.build(*tickets[t]))
+        srv.release(t)
+    assert srv.next(timeout_us=1000) is None
+    srv.close()
