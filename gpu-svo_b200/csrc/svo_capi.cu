@@ -549,6 +549,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         // outputs, code lists, job tables
         std::vector<CompactJob> jobs;
         std::vector<uint64_t> word_off(1, 0);
+        std::vector<KeyJob> kjobs;
+        std::vector<uint64_t> blk_off(1, 0);
         std::vector<EmitParams> ep(n);
         std::vector<const uint64_t *> top_ptr(n);
         uint64_t ktot = 0;
@@ -559,9 +561,18 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             for (int l = 1; l <= mh.T; ++l) ktot += mh.totals[l];
         }
         uint64_t *K = S.get<uint64_t>(ktot + 1);
+        // per-word ranks of levels >= 1 (k_compact writes them, rank lookups read them)
+        uint64_t wtot = 0;
+        std::vector<uint64_t> wbase(n);
+        for (int j = 0; j < n; ++j) {
+            const MeshHost &mh = b->m[wave[j]];
+            wbase[j] = wtot;
+            wtot += mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1];
+        }
+        uint32_t *WP = S.get<uint32_t>(wtot + 1);
         unsigned long long *dups = S.get<unsigned long long>(2 * (size_t)n);
         uint64_t *top = S.get<uint64_t>(n);
-        if (!K || !dups || !top) return cuda_fail(S.err, "wave scratch");
+        if (!K || !WP || !dups || !top) return cuda_fail(S.err, "wave scratch");
         check(cudaMemsetAsync(dups, 0, 16 * (size_t)n, st), "memset");
         // one block for the output arrays of the whole wave
         size_t arena_bytes = 0;
@@ -625,6 +636,7 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             job.l0 = 1;
             job.l1 = mh.T + 1;
             job.out = K + kbase[j];
+            job.wpre = WP + wbase[j];
             uint64_t ko = 0;
             for (int l = 1; l <= mh.T; ++l) {
                 job.koff[l] = ko;
@@ -632,11 +644,16 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             }
             jobs.push_back(job);
             word_off.push_back(word_off.back() + mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1]);
-            if (want_keys) {
+            if (want_keys && mh.T >= 3) {
+                // the level-3 code list is the list of non-empty level-0 blocks
+                kjobs.push_back(KeyJob{md.bits, md.pre, job.out + job.koff[3], r->keys});
+                blk_off.push_back(blk_off.back() + mh.totals[3]);
+            } else if (want_keys) {
                 CompactJob k0 = job;
                 k0.l0 = 0;
                 k0.l1 = 1;
                 k0.out = r->keys;
+                k0.wpre = nullptr;
                 std::memset(k0.koff, 0, sizeof(k0.koff));
                 jobs.push_back(k0);
                 word_off.push_back(word_off.back() + mh.py.words[0]);
@@ -653,6 +670,7 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 P.lv[l].n = (uint32_t)mh.n_l[l];
                 P.lv[l].K1 = job.out + (l < mh.T ? job.koff[l + 1] : job.koff[mh.T]);
                 P.lv[l].bits = md.bits + mh.py.woff[l];
+                P.lv[l].wpre = l >= 1 ? job.wpre + (mh.py.woff[l] - mh.py.woff[1]) : nullptr;
                 P.lv[l].coff = mh.py.coff[l];
                 P.lv[l].side = std::max<uint32_t>(1u, R >> l);
                 P.lv[l].width = w;
@@ -673,6 +691,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         }
         CompactJob *d_jobs = S.get<CompactJob>(jobs.size());
         uint64_t *d_word_off = S.get<uint64_t>(word_off.size());
+        KeyJob *d_kjobs = kjobs.empty() ? nullptr : S.get<KeyJob>(kjobs.size());
+        uint64_t *d_blk_off = kjobs.empty() ? nullptr : S.get<uint64_t>(blk_off.size());
         const uint64_t **d_top_ptr = S.get<const uint64_t *>(n);
         if (S.err != cudaSuccess) {
             for (svo_result *r : res) svo_result_free(r);
@@ -681,9 +701,15 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         }
         check(upload(d_jobs, jobs, st), "upload");
         check(upload(d_word_off, word_off, st), "upload");
+        if (!kjobs.empty()) {
+            check(upload(d_kjobs, kjobs, st), "upload");
+            check(upload(d_blk_off, blk_off, st), "upload");
+        }
         check(upload(d_top_ptr, top_ptr, st), "upload");
         tm.mark(StageTimer::kCompact0, st);
         check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
+        if (!kjobs.empty())
+            check(launch_compact_keys(KeyBatch{d_kjobs, (int)kjobs.size(), d_blk_off}, blk_off.back(), st), "keys");
         tm.mark(StageTimer::kCompact, st);
         // Large meshes get launches of their own (parameters in the kernel's
         // constant space); the rest share one launch over the mesh table.

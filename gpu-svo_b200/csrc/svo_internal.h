@@ -74,6 +74,7 @@ struct EmitLevel {
     uint32_t n;            // nodes in the level
     const uint64_t *K1;    // sorted codes of level l+1 (the level's groups); level T: its own code
     const uint64_t *bits;  // bitmap of level l
+    const uint32_t *wpre;  // rank at each non-empty word of level l (l >= 1)
     uint64_t coff;         // block-count offset of level l
     uint32_t side;         // grid side at this level (R >> l)
     float width;           // node width
@@ -111,12 +112,26 @@ struct CompactJob {
     Pyramid py;
     int l0, l1;
     uint64_t *out;
+    uint32_t *wpre;  // optional: rank at each non-empty word of levels >= 1 (indexed from woff[1])
     uint64_t koff[kMaxLevels];
 };
 struct CompactBatch {
     const CompactJob *job;
     int n;
     const uint64_t *word_off;
+};
+// The surface-voxel keys of one mesh, from its non-empty level-0 blocks
+// (= its level-3 code list).
+struct KeyJob {
+    const uint64_t *bits;    // level-0 bitmap
+    const uint32_t *pre;     // the mesh's scanned block counts (level 0 first)
+    const uint64_t *blocks;  // sorted non-empty block indices
+    uint64_t *out;
+};
+struct KeyBatch {
+    const KeyJob *job;
+    int n;
+    const uint64_t *blk_off;  // prefix of the jobs' block counts
 };
 
 // Binary search: the i with off[i] <= x < off[i + 1] (off has n + 1 entries).
@@ -155,6 +170,7 @@ cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned 
 // totals of every (mesh, level).
 cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st);
 cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st);
+cudaError_t launch_compact_keys(const KeyBatch &k, uint64_t total_blocks, cudaStream_t st);
 // one: the EmitParams of a one-mesh batch (host copy, passed by value to the
 // kernel), or null for a batch of several meshes.
 cudaError_t launch_emit(const EmitBatch &b, const EmitParams *one, uint64_t total_nodes, uint32_t flags,

@@ -65,20 +65,19 @@ __device__ __forceinline__ uint32_t nz_bytes(uint64_t v) {
     return (uint32_t)((m * 0x0102040810204080ull) >> 56);
 }
 
-// Levels 1..4 per CTA (a CTA owns 2048 words of level 0), then the last CTA
-// to finish builds the remaining levels.
+// Levels 1..4 of one 2048-word chunk of level 0 per CTA (one 512-bit block
+// of level 0 per thread, 16-byte streaming loads).  No fence or completion
+// counter, so a CTA retires as soon as its stores are issued; the levels
+// above 4 come from k_pyramid_top.
 __global__ void __launch_bounds__(256) k_pyramid(BatchDev bd) {
     __shared__ uint64_t s1[256];
     __shared__ uint64_t s2[32];
     __shared__ uint64_t s3[4];
-    __shared__ bool s_last;
     const int m = find_segment(bd.cta_off, bd.n, (uint32_t)blockIdx.x);
     const MeshDev &md = bd.mesh[m];
     const Pyramid &py = md.py;
     uint64_t *__restrict__ bits = md.bits;
     uint32_t *__restrict__ cnt = md.cnt;
-    uint32_t *__restrict__ done = md.done;
-    const uint32_t nctas = bd.cta_off[m + 1] - bd.cta_off[m];
     const uint32_t b = blockIdx.x - bd.cta_off[m], t = threadIdx.x;
     {
         const uint4 *src = reinterpret_cast<const uint4 *>(bits + py.woff[0] + (uint64_t)b * 2048 + t * 8);
@@ -135,12 +134,15 @@ __global__ void __launch_bounds__(256) k_pyramid(BatchDev bd) {
         atomicAdd(cnt + py.coff[3] + b / 2, c);
         reinterpret_cast<uint32_t *>(bits + py.woff[4])[b] = w;
     }
-    __threadfence();
-    __syncthreads();
-    if (t == 0) s_last = atomicAdd(done, 1u) == nctas - 1;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
+}
+
+// Levels 5.. and the counts of levels 4.. of every mesh: one CTA per mesh.
+__global__ void __launch_bounds__(256) k_pyramid_top(BatchDev bd) {
+    const MeshDev &md = bd.mesh[blockIdx.x];
+    const Pyramid &py = md.py;
+    uint64_t *__restrict__ bits = md.bits;
+    uint32_t *__restrict__ cnt = md.cnt;
+    const uint32_t t = threadIdx.x;
     for (int l = 4; l < py.levels; ++l) {
         const uint64_t *in = bits + py.woff[l];
         const uint64_t nblk = py.words[l] / 8;
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(256) k_pyramid(BatchDev bd) {
             uint32_t c = 0;
 #pragma unroll
             for (int k = 0; k < 8; ++k) {
-                const uint64_t v = __ldcg(in + 8 * j + k);
+                const uint64_t v = in[8 * j + k];
                 c += __popcll(v);
                 w |= (uint64_t)nz_bytes(v) << (8 * k);
             }
@@ -160,7 +162,6 @@ __global__ void __launch_bounds__(256) k_pyramid(BatchDev bd) {
         }
         __syncthreads();
     }
-    if (t == 0) *done = 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -274,26 +275,78 @@ __global__ void k_level_totals(BatchDev bd) {
 
 // One thread per 64-bit word of every job's levels: its first rank is the
 // block prefix plus the popcounts of the preceding words of its block.
+// One thread per bitmap word; the 8 lanes of a 512-bit block are 8 aligned
+// lanes of a warp (every level and job starts on a block boundary), so a
+// word's rank in its level is the block's scanned base plus an 8-lane prefix
+// of popcounts.  Writes the sorted set-bit positions and, for levels >= 1
+// when wpre is given, the rank at each non-empty word (rank_of's table).
 __global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total) {
     const uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
-    if (gi >= total) return;
-    const int j = find_segment(cb.word_off, cb.n, gi);
-    const CompactJob &job = cb.job[j];
-    const Pyramid &py = job.py;
-    const uint64_t gw = py.woff[job.l0] + (gi - cb.word_off[j]);
-    int l = job.l0;
-    while (l + 1 < job.l1 && gw >= py.woff[l + 1]) ++l;
-    uint64_t v = job.bits[gw];
+    if (gi >= ((total + 31) & ~31ull)) return;  // whole warps stay for the shuffles
+    const int sub = threadIdx.x & 7;
+    uint64_t v = 0, w = 0;
+    uint32_t r = 0;
+    int l = 0, j = 0;
+    if (gi < total) {
+        j = find_segment(cb.word_off, cb.n, gi);
+        const CompactJob &job = cb.job[j];
+        const Pyramid &py = job.py;
+        const uint64_t gw = py.woff[job.l0] + (gi - cb.word_off[j]);
+        l = job.l0;
+        while (l + 1 < job.l1 && gw >= py.woff[l + 1]) ++l;
+        w = gw - py.woff[l];
+        v = job.bits[gw];
+        if (v) r = job.pre[py.coff[l] + (w >> 3)] - job.pre[py.coff[l]];
+    }
+    const uint32_t pc = __popcll(v);
+    uint32_t x = pc;
+#pragma unroll
+    for (int d = 1; d < 8; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d, 8);
+        if (sub >= d) x += y;
+    }
     if (!v) return;
-    const uint64_t w = gw - py.woff[l];
-    const uint64_t blk = w >> 3;
-    uint64_t r = job.pre[py.coff[l] + blk] - job.pre[py.coff[l]];
-    const uint64_t *bw = job.bits + py.woff[l] + blk * 8;
-    for (int k = 0; k < (int)(w & 7); ++k) r += __popcll(bw[k]);
+    r += x - pc;
+    const CompactJob &job = cb.job[j];
+    if (job.wpre && l >= 1) job.wpre[job.py.woff[l] - job.py.woff[1] + w] = r;
     uint64_t *o = job.out + job.koff[l] + r;
-    const uint64_t base = w * 64;
+    const uint64_t b64 = w * 64;
     while (v) {
-        *o++ = base + __ffsll((long long)v) - 1;
+        *o++ = b64 + __ffsll((long long)v) - 1;
+        v &= v - 1;
+    }
+}
+
+// Level-0 set bits (the surface-voxel keys) from the non-empty 512-bit blocks
+// only: a mesh's level-3 code list is exactly its non-empty level-0 blocks,
+// in order.  8 lanes per block, one word each.
+__global__ void __launch_bounds__(256) k_compact_keys(KeyBatch kb, uint64_t total_blocks) {
+    const uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    const uint64_t item = gi >> 3;
+    if (((gi >> 5) << 2) >= total_blocks) return;  // whole warps stay for the shuffles
+    const int sub = threadIdx.x & 7;
+    uint64_t v = 0, blk = 0;
+    uint32_t r = 0;
+    int j = 0;
+    if (item < total_blocks) {
+        j = find_segment(kb.blk_off, kb.n, item);
+        const KeyJob &job = kb.job[j];
+        blk = job.blocks[item - kb.blk_off[j]];
+        v = job.bits[blk * 8 + sub];
+        r = job.pre[blk] - job.pre[0];
+    }
+    const uint32_t pc = __popcll(v);
+    uint32_t x = pc;
+#pragma unroll
+    for (int d = 1; d < 8; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d, 8);
+        if (sub >= d) x += y;
+    }
+    if (!v) return;
+    uint64_t *o = kb.job[j].out + r + x - pc;
+    const uint64_t b64 = (blk * 8 + sub) * 64;
+    while (v) {
+        *o++ = b64 + __ffsll((long long)v) - 1;
         v &= v - 1;
     }
 }
@@ -312,15 +365,11 @@ struct NodeInfo {
     float w;
 };
 
+// Rank of set bit c among level l's set bits (l >= 1): the word's rank from
+// k_compact plus the set bits below c in its word.
 __device__ __forceinline__ uint32_t rank_of(const EmitParams &P, int l, uint64_t c) {
-    const uint64_t blk = c >> 9;
-    const uint64_t co = P.lv[l].coff;
-    uint32_t r = P.pre[co + blk] - P.pre[co];
-    const uint64_t *w = P.lv[l].bits + blk * 8;
-    const int wi = (int)((c >> 6) & 7);
-    for (int k = 0; k < wi; ++k) r += __popcll(w[k]);
-    r += __popcll(w[wi] & ((1ull << (c & 63)) - 1ull));
-    return r;
+    const uint64_t w = c >> 6;
+    return P.lv[l].wpre[w] + (uint32_t)__popcll(P.lv[l].bits[w] & ((1ull << (c & 63)) - 1ull));
 }
 
 __device__ __forceinline__ bool bit_of(const uint64_t *bits, uint64_t c) {
@@ -702,8 +751,10 @@ cudaError_t unique_impl(const T *in, uint64_t n, T *out, uint32_t *tile_counts, 
 }  // namespace
 
 cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, cudaStream_t st) {
+    if (total_ctas == 0) return cudaSuccess;
     k_pyramid<<<total_ctas, 256, 0, st>>>(b);
-    count_launches(1);
+    k_pyramid_top<<<b.n, 256, 0, st>>>(b);
+    count_launches(2);
     return cudaGetLastError();
 }
 
@@ -730,6 +781,13 @@ cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st) {
 cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st) {
     if (total_words == 0) return cudaSuccess;
     k_compact<<<(unsigned)((total_words + 255) / 256), 256, 0, st>>>(c, total_words);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_keys(const KeyBatch &k, uint64_t total_blocks, cudaStream_t st) {
+    if (total_blocks == 0) return cudaSuccess;
+    k_compact_keys<<<(unsigned)((total_blocks * 8 + 255) / 256), 256, 0, st>>>(k, total_blocks);
     count_launches(1);
     return cudaGetLastError();
 }
