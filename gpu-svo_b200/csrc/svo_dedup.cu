@@ -49,8 +49,10 @@ struct DedupParams {
     uint32_t *D;                // candidate bitmap over Q (u32 view)
     uint32_t *G;                // one bit per chunk of D
     uint64_t chunks;
-    uint32_t *cnt;              // [3][chunks]
-    const uint32_t *pre;        // [3][chunks + 1]
+    const uint32_t *list;       // the touched chunks (a set bit in G), in order
+    uint64_t ntouched;
+    uint32_t *cnt;              // [3][ntouched]
+    const uint32_t *pre;        // [3][ntouched + 1]
     uint64_t *out[3];
 };
 
@@ -168,82 +170,96 @@ __device__ void init_tables(DedupTables &t) {
     __syncthreads();
 }
 
-// Keys of the 8 lattice points 2Q + r: counts (c) and, when EMIT, writes them
-// at the cursors o[].
-template <bool EMIT>
-__device__ __forceinline__ void q_keys(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                       uint64_t root, uint64_t qc, uint32_t c[3], uint64_t *o[3]) {
-    const uint32_t E0 = cell_mask(p.lv[1].bits, qc, sx[1]);
-    if (!EMIT) {
-        const uint32_t k0 = tb.cnt0[E0];
-        c[0] += k0 & 0xFF;
-        c[1] += (k0 >> 8) & 0xFF;
-        c[2] += k0 >> 16;
+// Cell existence around P = 2Q at level l >= 1 (u = P >> l has Morton code
+// uc): from the level l+1 bitmap, or at the top level, which holds the root
+// alone, cell u - d exists iff d = u - root.
+__device__ __forceinline__ uint32_t coarse_ex(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                              uint64_t root, int l, uint64_t uc) {
+    if (l < p.T) return tb.around[cell_mask(p.lv[l + 1].bits, uc >> 3, sx[l + 1]) * 8 + (uint32_t)(uc & 7)];
+    const int dx = (int)compact3(uc) - (int)compact3(root);
+    const int dy = (int)compact3(uc >> 1) - (int)compact3(root >> 1);
+    const int dz = (int)compact3(uc >> 2) - (int)compact3(root >> 2);
+    return (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) ? 1u << (dx | dy << 1 | dz << 2) : 0u;
+}
+
+// What one Q needs for all its keys: the level-0 parent mask E0 (the 8
+// points 2Q + r at level 0) and the cells around 2Q at level 1.  Levels >= 2
+// apply only to Q even in every coordinate and are computed where needed.
+struct QState {
+    uint32_t E0, ex1;
+};
+
+__device__ __forceinline__ QState q_eval(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                         uint64_t root, uint64_t qc) {
+    return QState{cell_mask(p.lv[1].bits, qc, sx[1]), coarse_ex(p, tb, sx, root, 1, qc)};
+}
+
+// Keys of the 8 points per kind (vertices, edges, faces).
+__device__ __forceinline__ void q_count(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                        uint64_t root, uint64_t qc, const QState &q, uint32_t c[3]) {
+    const uint32_t k0 = tb.cnt0[q.E0];
+    c[0] += k0 & 0xFF;
+    c[1] += (k0 >> 8) & 0xFF;
+    c[2] += k0 >> 16;
+    const bool v0 = tb.kinds[tb.around[q.E0 * 8]] & 1;
+    uint32_t k = tb.kinds[q.ex1];
+    bool v = v0 || (k & 1);
+    c[1] += __popc((k >> 1) & 7);
+    c[2] += __popc((k >> 4) & 7);
+    uint64_t uc = qc;
+    for (int l = 2; l <= p.T; ++l) {
+        if (uc & 7) break;
+        uc >>= 3;
+        k = tb.kinds[coarse_ex(p, tb, sx, root, l, uc)];
+        v |= k & 1;
+        c[1] += __popc((k >> 1) & 7);
+        c[2] += __popc((k >> 4) & 7);
     }
-    // r = 0 (P = 2Q): level 0, then every level l with P a multiple of 2^l
-    bool vert = false;
-    {
+    c[0] += (v && !v0) ? 1u : 0u;  // a vertex of coarser nodes only
+}
+
+// Writes the keys of the 8 points at the cursors o[] (vertices, edges,
+// faces), each kind in output order: point, then level, then axis.
+__device__ __forceinline__ void q_write(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                        uint64_t root, uint64_t qc, const QState &q, uint64_t *o[3]) {
+    {  // r = 0: level 0, level 1, then every level l with 2Q a multiple of 2^l
         const uint64_t pc = qc << 3;
-        const uint32_t k = tb.kinds[tb.around[E0 * 8]];
-        vert = k & 1;
-        if (EMIT) {
-            for (uint32_t a = 0; a < 3; ++a)
-                if (k >> (1 + a) & 1) *o[1]++ = (pc << 6) | a;
-            for (uint32_t a = 0; a < 3; ++a)
-                if (k >> (4 + a) & 1) *o[2]++ = (pc << 6) | a;
-        }
-        uint64_t uc = qc;  // u = P >> l at l = 1
+        uint32_t k = tb.kinds[tb.around[q.E0 * 8]];
+        bool v = k & 1;
+        for (uint32_t a = 0; a < 3; ++a)
+            if ((k >> (1 + a)) & 1) *o[1]++ = (pc << 6) | a;
+        for (uint32_t a = 0; a < 3; ++a)
+            if ((k >> (4 + a)) & 1) *o[2]++ = (pc << 6) | a;
+        uint64_t uc = qc;
         for (int l = 1; l <= p.T; ++l) {
-            if (l > 1) {
+            if (l >= 2) {
                 if (uc & 7) break;
                 uc >>= 3;
             }
-            uint32_t ex;
-            if (l < p.T) {
-                ex = tb.around[cell_mask(p.lv[l + 1].bits, uc >> 3, sx[l + 1]) * 8 + (uint32_t)(uc & 7)];
-            } else {
-                // the top level holds the root alone: cell u - d is the root iff d = u - root
-                const int dx = (int)compact3(uc) - (int)compact3(root);
-                const int dy = (int)compact3(uc >> 1) - (int)compact3(root >> 1);
-                const int dz = (int)compact3(uc >> 2) - (int)compact3(root >> 2);
-                ex = (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) ? 1u << (dx | dy << 1 | dz << 2)
-                                                                                      : 0u;
-            }
-            const uint32_t k = tb.kinds[ex];
-            vert |= k & 1;
-            if (EMIT) {
-                for (uint32_t a = 0; a < 3; ++a)
-                    if (k >> (1 + a) & 1) *o[1]++ = (pc << 6) | ((uint64_t)l << 2) | a;
-                for (uint32_t a = 0; a < 3; ++a)
-                    if (k >> (4 + a) & 1) *o[2]++ = (pc << 6) | ((uint64_t)l << 2) | a;
-            } else {
-                c[1] += __popc((k >> 1) & 7);
-                c[2] += __popc((k >> 4) & 7);
-            }
+            k = tb.kinds[l == 1 ? q.ex1 : coarse_ex(p, tb, sx, root, l, uc)];
+            v |= k & 1;
+            for (uint32_t a = 0; a < 3; ++a)
+                if ((k >> (1 + a)) & 1) *o[1]++ = (pc << 6) | ((uint64_t)l << 2) | a;
+            for (uint32_t a = 0; a < 3; ++a)
+                if ((k >> (4 + a)) & 1) *o[2]++ = (pc << 6) | ((uint64_t)l << 2) | a;
         }
-        if (EMIT) {
-            if (vert) *o[0]++ = pc;
-        } else if (vert && !(tb.kinds[tb.around[E0 * 8]] & 1)) {
-            ++c[0];  // a vertex of coarser nodes only
-        }
+        if (v) *o[0]++ = pc;
     }
-    if (EMIT) {
-        for (uint32_t r = 1; r < 8; ++r) {
-            const uint64_t pc = (qc << 3) | r;
-            const uint32_t k = tb.kinds[tb.around[E0 * 8 + r]];
-            if (k & 1) *o[0]++ = pc;
-            for (uint32_t a = 0; a < 3; ++a)
-                if (k >> (1 + a) & 1) *o[1]++ = (pc << 6) | a;
-            for (uint32_t a = 0; a < 3; ++a)
-                if (k >> (4 + a) & 1) *o[2]++ = (pc << 6) | a;
-        }
+    for (uint32_t r = 1; r < 8; ++r) {
+        const uint64_t pc = (qc << 3) | r;
+        const uint32_t k = tb.kinds[tb.around[q.E0 * 8 + r]];
+        if (k & 1) *o[0]++ = pc;
+        for (uint32_t a = 0; a < 3; ++a)
+            if ((k >> (1 + a)) & 1) *o[1]++ = (pc << 6) | a;
+        for (uint32_t a = 0; a < 3; ++a)
+            if ((k >> (4 + a)) & 1) *o[2]++ = (pc << 6) | a;
     }
 }
 
-// One warp per chunk of D.  The chunk's set bits are listed in order in
-// shared memory, then taken 32 at a time (lane i the i-th): counts per kind
-// (EMIT false, one total per chunk) or keys written at the chunk's scanned
-// offset plus the warp prefix of the batch (EMIT true).
+// One warp per touched chunk of D.  The chunk's set bits are listed in order
+// in shared memory, then taken 32 at a time (lane i the i-th): counts per
+// kind (EMIT false, one total per chunk) or keys written at the chunk's
+// scanned offset plus the warp prefix of the batch (EMIT true).
 template <bool EMIT>
 __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_keys(const __grid_constant__ DedupParams p) {
     __shared__ DedupTables tb;
@@ -256,12 +272,8 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_keys(const __grid_co
     const uint64_t root = *p.root;
     const uint64_t *D64 = reinterpret_cast<const uint64_t *>(p.D);
     uint16_t *lst = list[warp];
-    for (uint64_t ch = (uint64_t)blockIdx.x * kDedupWarps + warp; ch < p.chunks; ch += nwarps) {
-        const bool touched = (p.G[ch >> 5] >> (ch & 31)) & 1u;
-        if (!touched) {
-            if (!EMIT && lane < 3) p.cnt[lane * p.chunks + ch] = 0;
-            continue;
-        }
+    for (uint64_t i = (uint64_t)blockIdx.x * kDedupWarps + warp; i < p.ntouched; i += nwarps) {
+        const uint64_t ch = p.list[i];
         // list the chunk's set bits in order
         uint64_t word = D64[ch * kChunkWords + lane];
         const uint32_t n = __popcll(word);
@@ -278,30 +290,31 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_keys(const __grid_co
         uint32_t c[3] = {0, 0, 0};
         uint64_t base[3] = {0, 0, 0};
         if (EMIT)
-            for (int k = 0; k < 3; ++k) base[k] = p.pre[k * (p.chunks + 1) + ch];
+            for (int k = 0; k < 3; ++k) base[k] = p.pre[k * (p.ntouched + 1) + i];
         for (uint32_t j0 = 0; j0 < total; j0 += 32) {
             const uint32_t j = j0 + lane;
             const bool act = j < total;
             const uint64_t qc = ch * 2048 + (act ? lst[j] : 0);
+            const QState q = act ? q_eval(p, tb, sx, root, qc) : QState{0, 0};
             if (!EMIT) {
-                if (act) q_keys<false>(p, tb, sx, root, qc, c, nullptr);
-            } else {
-                uint32_t q[3] = {0, 0, 0};
-                if (act) q_keys<false>(p, tb, sx, root, qc, q, nullptr);
-                uint64_t *o[3];
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    uint32_t x = q[k];
-#pragma unroll
-                    for (int d = 1; d < 32; d <<= 1) {
-                        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
-                        if (lane >= d) x += y;
-                    }
-                    o[k] = p.out[k] + base[k] + (x - q[k]);
-                    base[k] += __shfl_sync(0xFFFFFFFFu, x, 31);
-                }
-                if (act) q_keys<true>(p, tb, sx, root, qc, q, o);
+                if (act) q_count(p, tb, sx, root, qc, q, c);
+                continue;
             }
+            uint32_t cq[3] = {0, 0, 0};
+            if (act) q_count(p, tb, sx, root, qc, q, cq);
+            uint64_t *o[3];
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                uint32_t x = cq[k];
+#pragma unroll
+                for (int d = 1; d < 32; d <<= 1) {
+                    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+                    if (lane >= d) x += y;
+                }
+                o[k] = p.out[k] + base[k] + (x - cq[k]);
+                base[k] += __shfl_sync(0xFFFFFFFFu, x, 31);
+            }
+            if (act) q_write(p, tb, sx, root, qc, q, o);
         }
         __syncwarp();
         if (!EMIT) {
@@ -310,8 +323,27 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_keys(const __grid_co
 #pragma unroll
                 for (int d = 16; d > 0; d >>= 1) c[k] += __shfl_xor_sync(0xFFFFFFFFu, c[k], d);
             }
-            if (lane < 3) p.cnt[lane * p.chunks + ch] = lane == 0 ? c[0] : lane == 1 ? c[1] : c[2];
+            if (lane < 3) p.cnt[lane * p.ntouched + i] = lane == 0 ? c[0] : lane == 1 ? c[1] : c[2];
         }
+    }
+}
+
+// The touched chunks in order: per-word popcounts of G, then (after a scan)
+// the chunk index of every set bit.
+__global__ void k_touched_count(const uint32_t *__restrict__ G, uint64_t n, uint32_t *__restrict__ cnt) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i < n) cnt[i] = __popc(G[i]);
+}
+
+__global__ void k_touched_list(const uint32_t *__restrict__ G, uint64_t n, const uint32_t *__restrict__ pre,
+                               uint32_t *__restrict__ list) {
+    const uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t g = G[i];
+    uint32_t at = pre[i];
+    while (g) {
+        list[at++] = (uint32_t)(i * 32 + __ffs(g) - 1);
+        g &= g - 1;
     }
 }
 
@@ -348,13 +380,18 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     p.chunks = d_words / kChunkWords;
     const uint64_t g_words = (p.chunks + 31) / 32;
 
-    void *blk[6] = {};
-    const size_t sz[6] = {d_words * 8, g_words * 4, 3 * p.chunks * 4, 3 * (p.chunks + 1) * 4,
-                          scan_scratch_words(p.chunks) * 8, 256};
+    if (p.chunks > 0xFFFFFFFFull) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup grid too large");
+    // scratch: D, G, G popcounts + prefix, touched list, scan scratch, status
+    void *blk[7] = {};
+    const size_t sz[7] = {d_words * 8, g_words * 4, g_words * 4, (g_words + 1) * 4, p.chunks * 4,
+                          scan_scratch_words(std::max<uint64_t>(p.chunks, g_words)) * 8, 256};
+    void *blk2[2] = {};  // per touched chunk: counts and their prefixes (sized once the count is known)
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaMallocFromPoolAsync(&blk[i], sz[i], pool, st);
+    for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = cudaMallocFromPoolAsync(&blk[i], sz[i], pool, st);
     auto release = [&]() {
         for (void *b : blk)
+            if (b) cudaFreeAsync(b, st);
+        for (void *b : blk2)
             if (b) cudaFreeAsync(b, st);
     };
     auto fail = [&](cudaError_t err, const char *what) {
@@ -366,28 +403,45 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     if (e != cudaSuccess) return fail(e, "scratch");
     p.D = static_cast<uint32_t *>(blk[0]);
     p.G = static_cast<uint32_t *>(blk[1]);
-    p.cnt = static_cast<uint32_t *>(blk[2]);
-    uint32_t *pre = static_cast<uint32_t *>(blk[3]);
-    p.pre = pre;
-    auto *scan = static_cast<unsigned long long *>(blk[4]);
-    uint32_t *status = static_cast<uint32_t *>(blk[5]);
+    uint32_t *gcnt = static_cast<uint32_t *>(blk[2]);
+    uint32_t *gpre = static_cast<uint32_t *>(blk[3]);
+    uint32_t *list = static_cast<uint32_t *>(blk[4]);
+    p.list = list;
+    auto *scan = static_cast<unsigned long long *>(blk[5]);
+    uint32_t *status = static_cast<uint32_t *>(blk[6]);
     if ((e = cudaMemsetAsync(p.D, 0, sz[0], st)) != cudaSuccess || (e = cudaMemsetAsync(p.G, 0, sz[1], st)) ||
         (e = cudaMemsetAsync(status, 0, 4, st)))
         return fail(e, "memset");
     k_dedup_mark<<<(mark_total + 255) / 256, 256, 0, st>>>(p, mark_total);
-    const unsigned blocks =
-        (unsigned)std::max<uint64_t>(1, std::min<uint64_t>((p.chunks + kDedupWarps - 1) / kDedupWarps,
-                                                          (uint64_t)num_sms * 16));
-    k_dedup_keys<false><<<blocks, kDedupWarps * 32, 0, st>>>(p);
+    k_touched_count<<<(unsigned)((g_words + 255) / 256), 256, 0, st>>>(p.G, g_words, gcnt);
     count_launches(2);
+    if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "mark");
+    if ((e = launch_scan(gcnt, gpre, g_words, scan, status, st)) != cudaSuccess) return fail(e, "scan");
+    k_touched_list<<<(unsigned)((g_words + 255) / 256), 256, 0, st>>>(p.G, g_words, gpre, list);
+    count_launches(1);
+    uint32_t h[4] = {0, 0, 0, 0};
+    if ((e = cudaMemcpyAsync(h, gpre + g_words, 4, cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
+        return fail(e, "touched chunks");
+    p.ntouched = h[0];
+    const uint64_t nt = p.ntouched;
+    if ((e = cudaMallocFromPoolAsync(&blk2[0], 3 * std::max<uint64_t>(nt, 1) * 4, pool, st)) ||
+        (e = cudaMallocFromPoolAsync(&blk2[1], 3 * (nt + 1) * 4, pool, st)))
+        return fail(e, "scratch");
+    p.cnt = static_cast<uint32_t *>(blk2[0]);
+    uint32_t *pre = static_cast<uint32_t *>(blk2[1]);
+    p.pre = pre;
+    const unsigned blocks = (unsigned)std::max<uint64_t>(
+        1, std::min<uint64_t>((nt + kDedupWarps - 1) / kDedupWarps, (uint64_t)num_sms * 16));
+    if (nt > 0) {
+        k_dedup_keys<false><<<blocks, kDedupWarps * 32, 0, st>>>(p);
+        count_launches(1);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "count");
     for (int k = 0; k < 3; ++k)
-        if ((e = launch_scan(p.cnt + k * p.chunks, pre + k * (p.chunks + 1), p.chunks, scan, status, st)) !=
-            cudaSuccess)
+        if ((e = launch_scan(p.cnt + k * nt, pre + k * (nt + 1), nt, scan, status, st)) != cudaSuccess)
             return fail(e, "scan");
-    uint32_t h[4] = {0, 0, 0, 0};
     for (int k = 0; k < 3; ++k)
-        if ((e = cudaMemcpyAsync(h + k, pre + k * (p.chunks + 1) + p.chunks, 4, cudaMemcpyDeviceToHost, st)))
+        if ((e = cudaMemcpyAsync(h + k, pre + k * (nt + 1) + nt, 4, cudaMemcpyDeviceToHost, st)))
             return fail(e, "read totals");
     if ((e = cudaMemcpyAsync(h + 3, status, 4, cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
         return fail(e, "read totals");
@@ -407,8 +461,10 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
         out[k] = p.out[k] = static_cast<uint64_t *>(o);
         n_out[k] = h[k];
     }
-    k_dedup_keys<true><<<blocks, kDedupWarps * 32, 0, st>>>(p);
-    count_launches(1);
+    if (nt > 0) {
+        k_dedup_keys<true><<<blocks, kDedupWarps * 32, 0, st>>>(p);
+        count_launches(1);
+    }
     if ((e = cudaGetLastError()) != cudaSuccess) {
         for (int j = 0; j < 3; ++j) {
             if (out[j]) cudaFreeAsync(out[j], st);
