@@ -685,7 +685,7 @@ cudaError_t launch_index_range(const int32_t *idx, int64_t n, int32_t *mm, cudaS
     return cudaGetLastError();
 }
 
-uint32_t index_blocks(int64_t n) { return (uint32_t)std::max<int64_t>(1, std::min<int64_t>((n + 2047) / 2048, 256)); }
+uint32_t index_blocks(int64_t n) { return (uint32_t)std::max<int64_t>(1, std::min<int64_t>((n + 2047) / 2048, 2048)); }
 
 cudaError_t launch_index_ranges(const IndexJob *jobs, int n, const uint32_t *block_off, uint32_t total_blocks,
                                 int32_t *mm, cudaStream_t st) {
