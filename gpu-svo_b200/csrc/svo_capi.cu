@@ -388,6 +388,7 @@ int batch_phase_a(svo_batch *b) {
     uint32_t *d_bbox_off = batch_alloc<uint32_t>(b, n + 1, err);
     uint32_t big_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(2 * tris, 1 << 16), 0x7FFFFFFFu);
     uint4 *big = batch_alloc<uint4>(b, big_cap, err);
+    uint64_t *small = big ? batch_alloc<uint64_t>(b, std::max<uint64_t>(tris, 1), err) : nullptr;
     if (err != cudaSuccess) return cuda_fail(err, "batch scratch");
     GridParams *gp = reinterpret_cast<GridParams *>(b->meta + ml.gp);
     uint32_t *totals = reinterpret_cast<uint32_t *>(b->meta + ml.totals);
@@ -428,7 +429,8 @@ int batch_phase_a(svo_batch *b) {
         tm.mark(StageTimer::kBbox, st);
         SVO_TRY(cudaMemsetAsync(b->bits, 0, words * 8, st), "memset bitmaps");
         SVO_TRY(cudaMemsetAsync(b->cnt, 0, blocks * 4, st), "memset counts");
-        SVO_TRY(launch_voxelize(bd, (int64_t)tris, strict, ctx->tune, big, big_cap, counters, ctx->num_sms, st),
+        SVO_TRY(launch_voxelize(bd, (int64_t)tris, strict, ctx->tune, big, big_cap, counters, ctx->num_sms, st,
+                                small),
                 "voxelize");
         tm.mark(StageTimer::kVox, st);
         SVO_TRY(launch_pyramid(bd, ctas, st), "pyramid");

@@ -158,8 +158,12 @@ struct IndexJob {
 uint32_t index_blocks(int64_t n);
 cudaError_t launch_index_ranges(const IndexJob *jobs, int n, const uint32_t *block_off, uint32_t total_blocks,
                                 int32_t *mm, cudaStream_t st);
+// counters: 4 u32 (queue entries, queue cursor, -, small-list length); small:
+// room for one u64 per triangle, or null (then no in-warp tier unless big is
+// null too, which walks every large triangle in the warp that set it up).
 cudaError_t launch_voxelize(const BatchDev &b, int64_t total_tris, bool strict, const VoxTuning &tune,
-                            uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st);
+                            uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st,
+                            uint64_t *small = nullptr);
 // Builds levels 1.. of every mesh's pyramid and the per-block counts.
 cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, cudaStream_t st);
 // Exclusive scan of n u32 values; out has n + 1 entries (out[n] = total).

@@ -542,18 +542,19 @@ __device__ __forceinline__ void warp_packed(const BatchDev &bd, const Tri *st, i
 // One thread per triangle of the batch (global index -> mesh by tri_off):
 // setup, then
 //   tier 0 (grid bbox <= serial_max voxels): its own serial row-by-row test;
-//   tier 1 (<= inplace_max 4^3 bricks, or any size when INPLACE): its bricks
-//     are walked by this warp right after setup (warp_packed), shared with the
-//     warp's other tier-1 triangles;
+//   tier 1 (<= inplace_max 4^3 bricks, or any size when INPLACE): with a
+//     small-triangle list, its index is appended there for
+//     k_voxelize_small; INPLACE (no list or queue), its bricks are walked by
+//     this warp right away (warp_packed);
 //   tier 2 (more bricks): queue entries of <= warp_max bricks for
 //     k_voxelize_bricks, which balances them across the GPU.
 template <bool S, bool INPLACE>
-__global__ void __launch_bounds__(256, 2) k_voxelize(BatchDev bd, int64_t total, VoxTuning tune,
-                                                                    uint4 *__restrict__ big, uint32_t big_cap,
-                                                                    uint32_t *__restrict__ big_count) {
-    __shared__ Tri s_tri[8][32];  // the warp's tier-1 triangles
+__global__ void __launch_bounds__(256, INPLACE ? 2 : 3)
+    k_voxelize(BatchDev bd, int64_t total, VoxTuning tune, uint4 *__restrict__ big, uint32_t big_cap,
+               uint32_t *__restrict__ big_count, uint64_t *__restrict__ small, uint32_t *__restrict__ small_count) {
+    __shared__ Tri s_tri[INPLACE ? 8 : 1][32];  // INPLACE: the warp's tier-1 triangles
     const int lane = threadIdx.x & 31;
-    Tri *st = s_tri[threadIdx.x >> 5];
+    Tri *st = s_tri[INPLACE ? (threadIdx.x >> 5) : 0];
     const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = warp0; base < total; base += stride) {
@@ -578,7 +579,7 @@ __global__ void __launch_bounds__(256, 2) k_voxelize(BatchDev bd, int64_t total,
                     for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
                 sink.flush();
             } else if (tier == 1) {
-                st[lane] = t;
+                if (INPLACE) st[lane] = t;
             } else {
                 const uint32_t eb = tune.warp_max;
                 const uint32_t ne = (nb + eb - 1) / eb;
@@ -589,11 +590,56 @@ __global__ void __launch_bounds__(256, 2) k_voxelize(BatchDev bd, int64_t total,
                 }
             }
         }
-        if (__any_sync(0xFFFFFFFFu, tier == 1)) {
-            __syncwarp();
-            warp_packed<S>(bd, st, m, tier == 1 ? nb : 0u, lane);
-            __syncwarp();  // st is rewritten by the next round
+        if (INPLACE) {
+            if (__any_sync(0xFFFFFFFFu, tier == 1)) {
+                __syncwarp();
+                warp_packed<S>(bd, st, m, tier == 1 ? nb : 0u, lane);
+                __syncwarp();  // st is rewritten by the next round
+            }
+        } else {
+            // warp-aggregated append to the small-triangle list (room for every triangle)
+            const uint32_t mask = __ballot_sync(0xFFFFFFFFu, tier == 1);
+            if (mask) {
+                uint32_t at = 0;
+                if (lane == __ffs(mask) - 1) at = atomicAdd(small_count, (uint32_t)__popc(mask));
+                at = __shfl_sync(0xFFFFFFFFu, at, __ffs(mask) - 1);
+                if (tier == 1) small[at + __popc(mask & ((1u << lane) - 1u))] = (uint64_t)gid;
+            }
         }
+    }
+}
+
+// The small-triangle list: each lane sets up one listed triangle (32
+// different triangles per warp), stages it in shared memory, and the warp
+// walks their bricks packed 32 per round (warp_packed).
+template <bool S>
+__global__ void __launch_bounds__(256, 2) k_voxelize_small(BatchDev bd, const uint64_t *__restrict__ small,
+                                                           const uint32_t *__restrict__ small_count) {
+    __shared__ Tri s_tri[8][32];
+    const int lane = threadIdx.x & 31;
+    Tri *st = s_tri[threadIdx.x >> 5];
+    const uint32_t n = *small_count;
+    const uint64_t warp0 = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) - lane;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t base = warp0; base < n; base += stride) {
+        const uint64_t i = base + lane;
+        uint32_t nb = 0;
+        int m = 0;
+        if (i < n) {
+            const uint64_t gid = small[i];
+            m = find_segment(bd.tri_off, bd.n, gid);
+            const MeshDev &md = bd.mesh[m];
+            const GridParams g = *md.gp;
+            float p[3][3];
+            load_tri(md.pts, md.tris, (int64_t)(gid - bd.tri_off[m]), p);
+            Tri t;
+            tri_setup<S>(g, md.res, p[0], p[1], p[2], t);
+            nb = brick_count(t);
+            st[lane] = t;
+        }
+        __syncwarp();
+        warp_packed<S>(bd, st, m, nb, lane);
+        __syncwarp();
     }
 }
 
@@ -704,18 +750,21 @@ cudaError_t launch_bbox(const BatchDev &b, uint32_t total_blocks, cudaStream_t s
 }
 
 cudaError_t launch_voxelize(const BatchDev &b, int64_t total, bool strict, const VoxTuning &tune, uint4 *big,
-                            uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st) {
-    // counters[0] = queue entries, counters[1] = queue cursor
+                            uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st, uint64_t *small) {
+    // counters[0] = queue entries, counters[1] = queue cursor, counters[3] = small-list length
     cudaError_t e = cudaMemsetAsync(counters, 0, 2 * sizeof(uint32_t), st);
+    if (e == cudaSuccess && small) e = cudaMemsetAsync(counters + 3, 0, sizeof(uint32_t), st);
     if (e != cudaSuccess) return e;
     if (total > 0) {
         const int64_t want = (total + 255) / 256;
         const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(want, (int64_t)num_sms * 16));
         const bool inplace = big == nullptr || big_cap == 0;
-        // Few triangles: the in-warp tier would leave most SMs idle, the queue spreads the bricks.
+        // Few triangles, or no small-triangle list: the queue spreads the bricks over all SMs.
         VoxTuning tn = tune;
-        if (!inplace && total < (int64_t)num_sms * 256) tn.inplace_max = 0;
-#define SVO_VOX(S_, I_) k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(b, total, tn, big, big_cap, counters)
+        if (!inplace && (total < (int64_t)num_sms * 256 || !small)) tn.inplace_max = 0;
+        uint32_t *small_count = counters + 3;
+#define SVO_VOX(S_, I_) \
+    k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(b, total, tn, big, big_cap, counters, small, small_count)
         if (strict) {
             if (inplace) SVO_VOX(true, true); else SVO_VOX(true, false);
         } else {
@@ -724,6 +773,12 @@ cudaError_t launch_voxelize(const BatchDev &b, int64_t total, bool strict, const
 #undef SVO_VOX
         count_launches(1);
         if (!inplace) {
+            if (tn.inplace_max > 0) {
+                const int sblocks = num_sms * 2;
+                if (strict) k_voxelize_small<true><<<sblocks, 256, 0, st>>>(b, small, small_count);
+                else k_voxelize_small<false><<<sblocks, 256, 0, st>>>(b, small, small_count);
+                count_launches(1);
+            }
             const int bblocks = num_sms * 4;
             if (strict)
                 k_voxelize_bricks<true><<<bblocks, 256, 0, st>>>(b, big, counters, big_cap, counters + 1,
