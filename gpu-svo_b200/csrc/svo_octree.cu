@@ -372,10 +372,6 @@ __device__ __forceinline__ uint32_t rank_of(const EmitParams &P, int l, uint64_t
     return P.lv[l].wpre[w] + (uint32_t)__popcll(P.lv[l].bits[w] & ((1ull << (c & 63)) - 1ull));
 }
 
-__device__ __forceinline__ bool bit_of(const uint64_t *bits, uint64_t c) {
-    return (bits[c >> 6] >> (c & 63)) & 1ull;
-}
-
 template <bool S>
 __device__ __forceinline__ void node_info(const EmitParams &P, const float go[3], uint32_t t, NodeInfo &ni) {
     int l = 0;
@@ -389,8 +385,15 @@ __device__ __forceinline__ void node_info(const EmitParams &P, const float go[3]
         ni.code = P.lv[l].K1[0];
         ni.pc = ni.code >> 3;
     }
-    ni.real = l >= 1 && bit_of(P.lv[l].bits, ni.code);
-    ni.child0 = ni.real ? P.lv[l - 1].off + 8u * rank_of(P, l, ni.code) : kNone;
+    ni.real = false;
+    ni.child0 = kNone;
+    if (l >= 1) {  // one word load serves both the bit test and the rank
+        const uint64_t w = ni.code >> 6;
+        const uint64_t wd = P.lv[l].bits[w];
+        const uint32_t wp = P.lv[l].wpre[w];
+        ni.real = (wd >> (ni.code & 63)) & 1ull;
+        if (ni.real) ni.child0 = P.lv[l - 1].off + 8u * (wp + (uint32_t)__popcll(wd & ((1ull << (ni.code & 63)) - 1ull)));
+    }
     if (l < P.T) {
         const uint32_t pl = (l + 1 < P.T) ? 8u * rank_of(P, l + 2, ni.pc >> 3) + (uint32_t)(ni.pc & 7) : 0u;
         ni.parent = P.lv[l + 1].off + pl;
@@ -434,15 +437,31 @@ __device__ __forceinline__ void full_neighbors(const EmitParams &P, const NodeIn
         }
     }
     const uint32_t own = self - (uint32_t)(ni.code & 7);  // child 0 of the node's own group
+    // the 7 other groups: codes first, then all word loads (in range even for
+    // groups outside the grid, which fall back to the node's own group), then
+    // existence and rank from the loaded words
+    uint64_t q[8];
+    bool in[8];
+#pragma unroll
+    for (int b = 1; b < 8; ++b) {
+        in[b] = !(((b & 1) && !ok[0]) || ((b & 2) && !ok[1]) || ((b & 4) && !ok[2]));
+        q[b] = in[b] ? (((b & 1) ? step[0] : m[0]) | ((b & 2) ? step[1] : m[1]) | ((b & 4) ? step[2] : m[2])) : pc;
+    }
+    uint64_t wd[8];
+    uint32_t wp[8];
+    const bool top = l1 >= P.T;  // the root level: rank 0
+#pragma unroll
+    for (int b = 1; b < 8; ++b) {
+        wd[b] = P.lv[l1].bits[q[b] >> 6];
+        wp[b] = top ? 0u : P.lv[l1].wpre[q[b] >> 6];
+    }
     uint32_t base[8];
     base[0] = own;
 #pragma unroll
     for (int b = 1; b < 8; ++b) {
-        base[b] = kNone;
-        if (((b & 1) && !ok[0]) || ((b & 2) && !ok[1]) || ((b & 4) && !ok[2])) continue;
-        const uint64_t q = ((b & 1) ? step[0] : m[0]) | ((b & 2) ? step[1] : m[1]) | ((b & 4) ? step[2] : m[2]);
-        if (!bit_of(P.lv[l1].bits, q)) continue;
-        base[b] = P.lv[ni.l].off + 8u * ((l1 < P.T) ? rank_of(P, l1, q) : 0u);
+        const uint32_t sh = (uint32_t)(q[b] & 63);
+        const bool ex = in[b] && ((wd[b] >> sh) & 1ull);
+        base[b] = ex ? P.lv[ni.l].off + 8u * (wp[b] + (uint32_t)__popcll(wd[b] & ((1ull << sh) - 1ull))) : kNone;
     }
 #pragma unroll
     for (int j = 0; j < 27; ++j) {
@@ -488,7 +507,9 @@ constexpr int kEmitBufBytes = 32 * 336;  // per warp
 // (`one`, read through the constant cache); otherwise each warp looks up its
 // mesh in the batch table (global memory, L1-cached).
 template <bool S, bool FULL, bool VE, bool ONE>
-__global__ void __launch_bounds__(kEmitWarps * 32)
+// 5 CTAs per SM: the shared-memory staging allows 5, and 102 registers hold
+// every variant without spills.
+__global__ void __launch_bounds__(kEmitWarps * 32, 5)
     k_emit(EmitBatch eb, const __grid_constant__ EmitParams one, uint64_t total) {
     extern __shared__ uint4 smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
