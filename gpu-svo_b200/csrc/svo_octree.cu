@@ -69,7 +69,7 @@ __device__ __forceinline__ uint32_t nz_bytes(uint64_t v) {
 // of level 0 per thread, 16-byte streaming loads).  No fence or completion
 // counter, so a CTA retires as soon as its stores are issued; the levels
 // above 4 come from k_pyramid_top.
-__global__ void __launch_bounds__(256) k_pyramid(BatchDev bd) {
+__global__ void __launch_bounds__(256, 8) k_pyramid(BatchDev bd) {
     __shared__ uint64_t s1[256];
     __shared__ uint64_t s2[32];
     __shared__ uint64_t s3[4];
@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(256) k_pyramid_top(BatchDev bd) {
 // kStatusScanTimeout and the host fails the build.
 // ---------------------------------------------------------------------------
 constexpr int kScanThreads = 256;
-constexpr int kScanItems = 8;
+constexpr int kScanItems = 16;
 constexpr uint64_t kScanTile = kScanThreads * kScanItems;
 constexpr int kSpinLimit = 1 << 22;
 
@@ -507,9 +507,10 @@ constexpr int kEmitBufBytes = 32 * 336;  // per warp
 // (`one`, read through the constant cache); otherwise each warp looks up its
 // mesh in the batch table (global memory, L1-cached).
 template <bool S, bool FULL, bool VE, bool ONE>
-// 5 CTAs per SM: the shared-memory staging allows 5, and 102 registers hold
-// every variant without spills.
-__global__ void __launch_bounds__(kEmitWarps * 32, 5)
+// 5 CTAs per SM for the full-neighbour and single-mesh variants (the
+// shared-memory staging allows 5; 102 registers hold them without spills);
+// the batched parity variant measured faster with the compiler's own choice.
+__global__ void __launch_bounds__(kEmitWarps * 32, (FULL || ONE) ? 5 : 1)
     k_emit(EmitBatch eb, const __grid_constant__ EmitParams one, uint64_t total) {
     extern __shared__ uint4 smem[];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;

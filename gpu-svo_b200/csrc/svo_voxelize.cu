@@ -646,7 +646,7 @@ __global__ void __launch_bounds__(256, 2) k_voxelize_small(BatchDev bd, const ui
 // Queued triangles: each warp takes an entry (triangle, brick range) and
 // walks its bricks.
 template <bool S>
-__global__ void __launch_bounds__(256, 4) k_voxelize_bricks(BatchDev bd, const uint4 *__restrict__ big,
+__global__ void __launch_bounds__(256, 3) k_voxelize_bricks(BatchDev bd, const uint4 *__restrict__ big,
                                                             const uint32_t *__restrict__ big_count,
                                                             uint32_t big_cap, uint32_t *__restrict__ cursor,
                                                             bool split) {
