@@ -377,6 +377,43 @@ __device__ __forceinline__ void brick_voxels(const Tri &t, const GridParams &g, 
     }
 }
 
+// Two bricks per round, one per half-warp: lane r = lane & 15 of a half
+// tests the 4 voxels of row (y, z) = (r & 3, r >> 2) of its half's brick,
+// hoisted like the serial tier (row_prep: the YZ edge tests reject whole
+// rows; then voxel_test per x -- the same arithmetic as voxel_pass).  The
+// half's 64-bit hit mask (local Morton order) is OR-reduced over its 16 lanes
+// and written with two atomicOr.  t, g, bm and the brick may differ between
+// the halves; `on` is false for a half without a brick.  All 32 lanes call.
+template <bool S>
+__device__ __forceinline__ void brick_rows(const Tri &t, const GridParams &g, uint32_t *__restrict__ bm, int sx,
+                                           int sy, int sz, bool on, int lane) {
+    const int r = lane & 15, ly = r & 3, lz = r >> 2;
+    const int y = 4 * sy + ly, z = 4 * sz + lz;
+    uint64_t hits = 0;
+    if (on && y >= t.lo[1] && y <= t.hi[1] && z >= t.lo[2] && z <= t.hi[2]) {
+        Row rw;
+        if (row_prep<S>(t, g, y, z, rw)) {
+            const int x0 = max(4 * sx, t.lo[0]), x1 = min(4 * sx + 3, t.hi[0]);
+            const int yz = ((ly & 1) << 1) | ((lz & 1) << 2) | ((ly >> 1) << 4) | ((lz >> 1) << 5);
+            for (int x = x0; x <= x1; ++x) {
+                const int lx = x - 4 * sx;
+                if (voxel_test<S>(t, g, rw, x)) hits |= 1ull << (yz | (lx & 1) | ((lx >> 1) << 3));
+            }
+        }
+    }
+    uint32_t lo = (uint32_t)hits, hi = (uint32_t)(hits >> 32);
+#pragma unroll
+    for (int d = 8; d > 0; d >>= 1) {
+        lo |= __shfl_xor_sync(0xFFFFFFFFu, lo, d);
+        hi |= __shfl_xor_sync(0xFFFFFFFFu, hi, d);
+    }
+    if (on && r == 0) {
+        uint32_t *w = bm + (morton3((uint32_t)sx, (uint32_t)sy, (uint32_t)sz) << 1);
+        if (lo) atomicOr(w, lo);
+        if (hi) atomicOr(w + 1, hi);
+    }
+}
+
 // Brick j (row-major over the triangle's brick box) of triangle t: its brick
 // coordinates, and whether it survives the culling test.
 template <bool S>
@@ -408,11 +445,15 @@ __device__ __forceinline__ void warp_bricks(const Tri &t, const GridParams &g, u
         const bool live = j < b1 && brick_live<S>(t, g, j, bx, by, bz);
         uint32_t m = __ballot_sync(0xFFFFFFFFu, live);
         while (m && !split) {
-            // one surviving brick at a time
-            const int src = __ffs(m) - 1;
+            // two surviving bricks at a time, one per half-warp
+            const int sa = __ffs(m) - 1;
             m &= m - 1;
-            brick_voxels<S>(t, g, bm, __shfl_sync(0xFFFFFFFFu, bx, src), __shfl_sync(0xFFFFFFFFu, by, src),
-                            __shfl_sync(0xFFFFFFFFu, bz, src), lane);
+            const int sb = m ? __ffs(m) - 1 : -1;
+            if (m) m &= m - 1;
+            const bool on = (lane < 16) || sb >= 0;
+            const int src = (lane < 16 || sb < 0) ? sa : sb;
+            brick_rows<S>(t, g, bm, __shfl_sync(0xFFFFFFFFu, bx, src), __shfl_sync(0xFFFFFFFFu, by, src),
+                          __shfl_sync(0xFFFFFFFFu, bz, src), on, lane);
         }
         while (m) {
             // up to 4 surviving bricks: lane = (brick, sub-brick)
@@ -523,18 +564,23 @@ __device__ __forceinline__ void warp_packed(const BatchDev &bd, const Tri *st, i
         }
         uint32_t lm = __ballot_sync(0xFFFFFFFFu, live);
         while (lm) {
-            const int s = __ffs(lm) - 1;
+            // two surviving bricks at a time, one per half-warp, each with its own triangle
+            const int sa = __ffs(lm) - 1;
             lm &= lm - 1;
+            const int sb = lm ? __ffs(lm) - 1 : -1;
+            if (lm) lm &= lm - 1;
+            const bool on = (lane < 16) || sb >= 0;
+            const int s = (lane < 16 || sb < 0) ? sa : sb;
             const int own = __shfl_sync(0xFFFFFFFFu, src, s);
+            const int mm = __shfl_sync(0xFFFFFFFFu, m, own);
             if (own != cur) {
                 cur = own;
                 ct = st[own];
-                const int mm = __shfl_sync(0xFFFFFFFFu, m, own);
                 cg = *bd.mesh[mm].gp;
                 cbm = reinterpret_cast<uint32_t *>(bd.mesh[mm].bits);
             }
-            brick_voxels<S>(ct, cg, cbm, __shfl_sync(0xFFFFFFFFu, bx, s), __shfl_sync(0xFFFFFFFFu, by, s),
-                            __shfl_sync(0xFFFFFFFFu, bz, s), lane);
+            brick_rows<S>(ct, cg, cbm, __shfl_sync(0xFFFFFFFFu, bx, s), __shfl_sync(0xFFFFFFFFu, by, s),
+                          __shfl_sync(0xFFFFFFFFu, bz, s), on, lane);
         }
     }
 }
