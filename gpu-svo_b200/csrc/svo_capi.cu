@@ -1063,6 +1063,72 @@ int svo_batch_emit(svo_batch *b, int first, int count, svo_result **out, int *st
 
 void svo_batch_free(svo_batch *b) { batch_destroy(b); }
 
+int svo_ctx_autotune(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, void *stream,
+                     svo_tuning *best) {
+    if (!ctx || !descs || n <= 0) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument or empty sample");
+    const VoxTuning saved = ctx->tune;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // device ms of the voxelizer stage of the counting phase, best of 2 (after one untimed run)
+    auto measure = [&](const VoxTuning &t, float &ms) -> int {
+        ctx->tune = t;
+        ms = 1e30f;
+        for (int rep = 0; rep < 3; ++rep) {
+            svo_batch *b = nullptr;
+            const int rc = batch_create(ctx, descs, n, flags | SVO_FLAG_TIMINGS, st, &b);
+            if (rc != SVO_OK) {
+                batch_destroy(b);
+                return rc;
+            }
+            if (rep > 0 && b->timed) ms = std::min(ms, b->timings_a[2]);
+            batch_destroy(b);
+        }
+        return SVO_OK;
+    };
+    VoxTuning cur = saved, win = saved;
+    cur.split = 0;
+    float best_ms = 1e30f;
+    int rc = SVO_OK;
+    // stage 1: the serial / small-triangle thresholds; stage 2: queue entry size
+    for (uint32_t sm : {32u, 64u, 128u, 256u}) {
+        for (uint32_t ip : {16u, 32u, 64u}) {
+            VoxTuning t = cur;
+            t.serial_max = sm;
+            t.inplace_max = ip;
+            t.warp_max = 256;
+            float ms = 0.0f;
+            if ((rc = measure(t, ms)) != SVO_OK) break;
+            if (ms < best_ms) {
+                best_ms = ms;
+                win = t;
+            }
+        }
+        if (rc != SVO_OK) break;
+    }
+    for (uint32_t wm : {64u, 128u, 512u, 1024u}) {
+        if (rc != SVO_OK) break;
+        VoxTuning t = win;
+        t.warp_max = wm;
+        float ms = 0.0f;
+        if ((rc = measure(t, ms)) != SVO_OK) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            win = t;
+        }
+    }
+    if (rc != SVO_OK) {
+        ctx->tune = saved;
+        return rc;
+    }
+    ctx->tune = win;
+    if (best) {
+        best->serial_max = win.serial_max;
+        best->warp_max = win.warp_max;
+        best->split = win.split;
+        best->inplace_max = win.inplace_max;
+    }
+    return SVO_OK;
+}
+
 void svo_result_free(svo_result *r) {
     if (!r) return;
     cudaSetDevice(r->device);

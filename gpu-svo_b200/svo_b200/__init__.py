@@ -105,6 +105,7 @@ def lib() -> C.CDLL:
         L.svo_ctx_destroy.restype = None
         L.svo_ctx_set_tuning.argtypes = [vp, C.POINTER(Tuning)]
         L.svo_ctx_get_tuning.argtypes = [vp, C.POINTER(Tuning)]
+        L.svo_ctx_autotune.argtypes = [vp, C.POINTER(MeshDesc), C.c_int, C.c_uint32, vp, C.POINTER(Tuning)]
         L.svo_load_obj.argtypes = [C.c_char_p, C.POINTER(vp), i64p, C.POINTER(vp), i64p]
         L.svo_free_host.argtypes = [vp]
         L.svo_free_host.restype = None
@@ -248,6 +249,14 @@ class Context:
         cur = self.tuning
         v = tuple(int(x) for x in value) + cur[len(value):]
         _check(lib().svo_ctx_set_tuning(self._h, C.byref(Tuning(*v))))
+
+    def autotune(self, meshes, flags: int = 0, stream: int = 0) -> tuple:
+        """svo_ctx_autotune over sample meshes [(points, tris, res), ...]: installs
+        and returns the fastest (serial_max, warp_max, split, inplace_max)."""
+        descs, keep = _descs(meshes, flags)
+        t = Tuning()
+        _check(lib().svo_ctx_autotune(self._h, descs, len(meshes), flags, stream or None, C.byref(t)))
+        return (t.serial_max, t.warp_max, t.split, t.inplace_max)
 
     def build(self, points, tris, res, flags: int = 0, stream: int = 0) -> "Result":
         """svo_build.  points float32[n,3] and tris int32[m,3] (tris=None: soup),

@@ -167,6 +167,14 @@ typedef struct svo_mesh_desc {
 int svo_build_batch(svo_ctx *ctx, const svo_mesh_desc *descs, int n, void *stream,
                     svo_result **out, int *status_out);
 
+/* Autotuner for the work split: runs the counting phase of the sample meshes
+ * (a batch, as svo_batch_create) for a grid of candidate splits, times the
+ * voxelizer stage on the device, installs the fastest split in the context
+ * and returns it in *best (may be null).  Results do not depend on the split.
+ * No counterpart in the reference. */
+int svo_ctx_autotune(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, void *stream,
+                     svo_tuning *best);
+
 /* The same in two steps, for callers that bound device memory:
  * svo_batch_create runs the counting phase of every mesh (voxelization,
  * octree level sizes; about res^3/7 bytes of scratch per mesh) and knows each

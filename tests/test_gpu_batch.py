@@ -96,3 +96,23 @@ def test_batch_distribution_slice(gpu_ctx, svo_mod):
         s = gpu_ctx.build(p, t, res, svo_mod.FLAG_NO_VERT_EDGE)
         assert r.nodes().tobytes() == s.nodes().tobytes()
         assert r.keys().tobytes() == s.keys().tobytes()
+
+
+def test_autotune_keeps_results(gpu_ctx, svo_mod):
+    """The autotuner only changes the voxelizer work split, never the octree."""
+    from svo_b200 import meshgen
+
+    meshes = meshgen.batch(12, seed=5)
+    ref, st, rc = gpu_ctx.build_batch(meshes, svo_mod.FLAG_NO_VERT_EDGE)
+    assert rc == 0
+    saved = gpu_ctx.tuning
+    try:
+        t = gpu_ctx.autotune(meshes, svo_mod.FLAG_NO_VERT_EDGE)
+        assert gpu_ctx.tuning == t and t[0] > 0 and t[1] > 0
+        got, st, rc = gpu_ctx.build_batch(meshes, svo_mod.FLAG_NO_VERT_EDGE)
+        assert rc == 0
+        for a, b in zip(ref, got):
+            assert a.nodes().tobytes() == b.nodes().tobytes()
+            assert a.keys().tobytes() == b.keys().tobytes()
+    finally:
+        gpu_ctx.tuning = saved
