@@ -8,6 +8,7 @@
 // The reference's equivalent (src/SVO.cu:341-735) synchronises with the host
 // at least six times per level and reallocates its node array per level.
 #include <atomic>
+#include <mutex>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -19,12 +20,23 @@
 
 using namespace svo;
 
+// Extra streams over which an emission wave spreads its per-mesh launches
+// (fork from and join back to the build stream with events).
+struct AuxStreams {
+    static constexpr int kCount = 3;
+    cudaStream_t s[kCount] = {};
+    cudaEvent_t fork = nullptr;
+    cudaEvent_t join[kCount] = {};
+};
+
 struct svo_ctx {
     int device = 0;
     int num_sms = 148;
     cudaMemPool_t pool = nullptr;      // per-build scratch
     cudaMemPool_t out_pool = nullptr;  // result arrays, kept apart so scratch never splits their blocks
     VoxTuning tune;
+    std::mutex aux_mu;                 // builds on other threads take sets of their own
+    std::vector<AuxStreams *> aux_free, aux_all;
 };
 
 // One device block that holds the output arrays of several results (a wave of
@@ -508,6 +520,38 @@ uint64_t output_bytes(const MeshHost &mh, uint32_t flags) {
     return b;
 }
 
+AuxStreams *aux_acquire(svo_ctx *ctx) {
+    std::lock_guard<std::mutex> lk(ctx->aux_mu);
+    if (!ctx->aux_free.empty()) {
+        AuxStreams *a = ctx->aux_free.back();
+        ctx->aux_free.pop_back();
+        return a;
+    }
+    auto *a = new AuxStreams();
+    bool ok = cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming) == cudaSuccess;
+    for (int i = 0; i < AuxStreams::kCount && ok; ++i)
+        ok = cudaStreamCreateWithFlags(&a->s[i], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&a->join[i], cudaEventDisableTiming) == cudaSuccess;
+    if (!ok) {
+        cudaGetLastError();
+        for (int i = 0; i < AuxStreams::kCount; ++i) {
+            if (a->s[i]) cudaStreamDestroy(a->s[i]);
+            if (a->join[i]) cudaEventDestroy(a->join[i]);
+        }
+        if (a->fork) cudaEventDestroy(a->fork);
+        delete a;
+        return nullptr;
+    }
+    ctx->aux_all.push_back(a);
+    return a;
+}
+
+void aux_release(svo_ctx *ctx, AuxStreams *a) {
+    if (!a) return;
+    std::lock_guard<std::mutex> lk(ctx->aux_mu);
+    ctx->aux_free.push_back(a);
+}
+
 size_t arena_round(size_t b) { return (b + 255) / 256 * 256; }
 
 template <class T>
@@ -518,7 +562,10 @@ T *arena_take(unsigned char *&at, uint64_t count) {
 }
 
 // Meshes of at least this many nodes are emitted by a launch of their own.
-constexpr uint64_t kOwnEmitNodes = 1u << 20;
+#ifndef SVO_OWN_EMIT_NODES
+#define SVO_OWN_EMIT_NODES (1ull << 17)
+#endif
+constexpr uint64_t kOwnEmitNodes = SVO_OWN_EMIT_NODES;
 
 // Phase B for meshes [first, first + count).
 int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *status_out) {
@@ -715,15 +762,35 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         tm.mark(StageTimer::kCompact, st);
         // Large meshes get launches of their own (parameters in the kernel's
         // constant space); the rest share one launch over the mesh table.
+        // With two or more of them, they spread round-robin over the build
+        // stream and three more, so that one kernel's tail overlaps the next.
         std::vector<EmitParams> ep_small;
         std::vector<uint64_t> off_small(1, 0);
+        int n_own = 0;
+        for (int j = 0; j < n; ++j) n_own += (n == 1 || ep[j].N >= kOwnEmitNodes) ? 1 : 0;
+        AuxStreams *aux = n_own >= 2 ? aux_acquire(ctx) : nullptr;
+        if (aux) {
+            check(cudaEventRecord(aux->fork, st), "fork");
+            for (int i = 0; i < AuxStreams::kCount; ++i) check(cudaStreamWaitEvent(aux->s[i], aux->fork, 0), "fork");
+        }
+        int k_own = 0;
         for (int j = 0; j < n; ++j) {
             if (n == 1 || ep[j].N >= kOwnEmitNodes) {
-                check(launch_emit(EmitBatch{nullptr, 1, nullptr}, &ep[j], ep[j].N, flags, ctx->num_sms, st), "emit");
+                const int lane = aux ? k_own % (AuxStreams::kCount + 1) : 0;
+                cudaStream_t es = lane == 0 ? st : aux->s[lane - 1];
+                ++k_own;
+                check(launch_emit(EmitBatch{nullptr, 1, nullptr}, &ep[j], ep[j].N, flags, ctx->num_sms, es), "emit");
             } else {
                 ep_small.push_back(ep[j]);
                 off_small.push_back(off_small.back() + (ep[j].N + 31) / 32 * 32);
             }
+        }
+        if (aux) {
+            for (int i = 0; i < AuxStreams::kCount; ++i) {
+                check(cudaEventRecord(aux->join[i], aux->s[i]), "join");
+                check(cudaStreamWaitEvent(st, aux->join[i], 0), "join");
+            }
+            aux_release(ctx, aux);
         }
         if (!ep_small.empty()) {
             EmitParams *d_eps = S.get<EmitParams>(ep_small.size());
@@ -951,6 +1018,14 @@ int svo_ctx_device(const svo_ctx *ctx, int *device) {
 void svo_ctx_destroy(svo_ctx *ctx) {
     if (!ctx) return;
     cudaSetDevice(ctx->device);
+    for (AuxStreams *a : ctx->aux_all) {
+        for (int i = 0; i < AuxStreams::kCount; ++i) {
+            cudaStreamDestroy(a->s[i]);
+            cudaEventDestroy(a->join[i]);
+        }
+        cudaEventDestroy(a->fork);
+        delete a;
+    }
     if (ctx->pool) cudaMemPoolDestroy(ctx->pool);
     if (ctx->out_pool) cudaMemPoolDestroy(ctx->out_pool);
     delete ctx;
