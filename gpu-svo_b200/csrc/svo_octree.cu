@@ -819,7 +819,7 @@ cudaError_t launch_emit(const EmitBatch &b, const EmitParams *one, uint64_t tota
     if (total == 0) return cudaSuccess;
     const uint64_t warps = (total + 31) / 32;
     const unsigned blocks = (unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>((warps + kEmitWarps - 1) / kEmitWarps, (uint64_t)num_sms * 12));
+        1, std::min<uint64_t>((warps + kEmitWarps - 1) / kEmitWarps, 0x7FFFFFFFull));
     const size_t shmem = (size_t)kEmitWarps * kEmitBufBytes;
     const bool s = (flags & SVO_FLAG_STRICT_FP) != 0, f = (flags & SVO_FLAG_FULL_NEIGHBORS) != 0,
                ve = (flags & SVO_FLAG_NO_VERT_EDGE) == 0;
