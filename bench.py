@@ -41,6 +41,7 @@ L2_FLUSH_BYTES = 256 << 20
 # 8 vertices x 16 B, 12 edges x 28 B written; one 8-byte group code read per
 # 8 sibling nodes.
 EMIT_BYTES_PER_NODE = 168 + 8 * 16 + 12 * 28 + 1
+TUNING_KEYS = ("serial_max", "warp_max", "split", "inplace_max", "serial_packed")
 
 
 def parse_args():
@@ -58,6 +59,7 @@ def parse_args():
     ap.add_argument("--res", type=int, default=0, help="override the workload's resolution")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--tune", type=int, default=1, help="single-mesh workloads: autotune the voxelizer split first")
     return ap.parse_args()
 
 
@@ -130,6 +132,10 @@ def dist_done() -> None:
 # clocks during the timed region
 # ---------------------------------------------------------------------------
 class ClockSampler:
+    """SM clocks and clock-event reasons sampled while the timed steps run:
+    NVML every 5 ms in a thread (read-only queries), else `nvidia-smi -lms 100`.
+    Entering waits for the first sample, so even a short timed region is
+    covered."""
     QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
@@ -138,16 +144,58 @@ class ClockSampler:
         self.dev = device_index
         self.proc = None
         self.lines: list[str] = []
+        self.times: list[float] = []
+        self.t_start = 0.0
+        self._stop = threading.Event()
+        self._t = None
+
+    def _nvml_handle(self):
+        import pynvml as N
+
+        N.nvmlInit()
+        try:
+            import torch
+
+            p = torch.cuda.get_device_properties(self.dev)
+            bus = f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+            return N, N.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return N, N.nvmlDeviceGetHandleByIndex(self.dev)
+
+    def _poll_nvml(self, N, h):
+        R = {"hw_slowdown": N.nvmlClocksEventReasonHwSlowdown,
+             "hw_thermal_slowdown": N.nvmlClocksEventReasonHwThermalSlowdown,
+             "sw_thermal_slowdown": N.nvmlClocksEventReasonSwThermalSlowdown,
+             "sw_power_cap": N.nvmlClocksEventReasonSwPowerCap}
+        smax = N.nvmlDeviceGetMaxClockInfo(h, N.NVML_CLOCK_SM)
+        while True:
+            sm = N.nvmlDeviceGetClockInfo(h, N.NVML_CLOCK_SM)
+            bits = N.nvmlDeviceGetCurrentClocksEventReasons(h)
+            act = ["Active" if bits & R[k] else "Not Active" for k in
+                   ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")]
+            self.lines.append(", ".join([str(self.dev), str(sm), str(smax), "", hex(bits)] + act))
+            self.times.append(time.time())
+            if self._stop.wait(0.005):
+                break
 
     def __enter__(self):
         try:
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self._t = threading.Thread(target=self._read, daemon=True)
+            N, h = self._nvml_handle()
+            self._t = threading.Thread(target=self._poll_nvml, args=(N, h), daemon=True)
             self._t.start()
-        except (FileNotFoundError, OSError):
-            self.proc = None
+        except Exception:
+            try:
+                self.proc = subprocess.Popen(
+                    ["nvidia-smi", f"--id={self.dev}", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
+                     "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self._t = threading.Thread(target=self._read, daemon=True)
+                self._t.start()
+            except (FileNotFoundError, OSError):
+                self.proc = None
+        t0 = time.time()
+        while self._t is not None and not self.lines and time.time() - t0 < 5.0 and self._t.is_alive():
+            time.sleep(0.001)
+        self.t_start = time.time()
         return self
 
     def _read(self):
@@ -155,17 +203,24 @@ class ClockSampler:
             self.lines.append(line.strip())
 
     def __exit__(self, *a):
+        self._stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except subprocess.TimeoutExpired:
                 self.proc.kill()
+        elif self._t is not None:
+            self._t.join(timeout=5)
 
     def summary(self) -> dict:
         sm, smax, reasons = [], None, set()
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for line in self.lines:
+        lines = self.lines
+        if self.times:  # NVML samples: those taken while the timed steps ran, if any
+            inside = [l for l, t in zip(self.lines, self.times) if t >= self.t_start]
+            lines = inside or self.lines[-1:]
+        for line in lines:
             f = [x.strip() for x in line.split(",")]
             if len(f) < 9:
                 continue
@@ -278,6 +333,9 @@ def run_ours(args, rank: int, world: int):
     d_pts = torch.from_numpy(pts).cuda()
     d_tris = torch.from_numpy(tris).cuda() if tris is not None else None
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
+    # voxelizer work split for this mesh (svo_ctx_autotune, before any timing;
+    # results do not depend on it)
+    tuning = ctx.autotune([(d_pts, d_tris, res)], bflags, sid) if args.tune else ctx.tuning
 
     def step(flags=0):
         flush.fill_(1)  # L2 flush before each step, outside the timed span
@@ -393,7 +451,7 @@ def run_ours(args, rank: int, world: int):
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
             "config": {"workload": wname, "triangles": nt, "resolution": res, "parallelism": f"replicas{world}",
                        "l2_flush": "256 MiB device write before every step, outside the timed span",
-                       **info},
+                       "tuning": dict(zip(TUNING_KEYS, tuning)), **info},
             "nodes_per_s": nodes_per_s,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
             "gpu_launches": launches,
@@ -517,8 +575,8 @@ def run_batch(args, rank: int, world: int):
             "config": {"workload": "batch256_seed3", "meshes": len(meshes), "triangles": nt,
                        "resolutions": "64/128/256/512", "nodes": nodes, "flags": flags,
                        "emit_waves": nwaves, "wave_bytes": budget, "parallelism": f"replicas{world}",
-                       "tuning": dict(zip(("serial_max", "warp_max", "split", "inplace_max"), tuning)),
-                       "plain_tuning": dict(zip(("serial_max", "warp_max", "split", "inplace_max"), pctx.tuning)),
+                       "tuning": dict(zip(TUNING_KEYS, tuning)),
+                       "plain_tuning": dict(zip(TUNING_KEYS, pctx.tuning)),
                        "l2_flush": "256 MiB device write before every step, outside the timed span"},
             "nodes_per_s": world * nodes * args.steps / (t_batch / 1e3),
             "plain": {"value": plain_value, "unit": "tris/s", "ms_per_step": t_plain / args.steps,

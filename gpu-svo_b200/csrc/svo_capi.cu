@@ -1034,10 +1034,13 @@ void svo_ctx_destroy(svo_ctx *ctx) {
 int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t) {
     if (!ctx || !t) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
     if (t->warp_max == 0) return fail(SVO_ERR_INVALID_ARGUMENT, "warp_max must be positive");
+    if (t->serial_max > (1u << 16)) return fail(SVO_ERR_INVALID_ARGUMENT, "serial_max must be <= 65536");
+    if (t->serial_packed > 1) return fail(SVO_ERR_INVALID_ARGUMENT, "serial_packed must be 0 or 1");
     ctx->tune.serial_max = t->serial_max;
     ctx->tune.warp_max = t->warp_max;
     ctx->tune.split = t->split;
     ctx->tune.inplace_max = t->inplace_max;
+    ctx->tune.serial_packed = t->serial_packed;
     return SVO_OK;
 }
 
@@ -1047,6 +1050,7 @@ int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t) {
     t->warp_max = ctx->tune.warp_max;
     t->split = ctx->tune.split;
     t->inplace_max = ctx->tune.inplace_max;
+    t->serial_packed = ctx->tune.serial_packed;
     return SVO_OK;
 }
 
@@ -1163,12 +1167,14 @@ int svo_ctx_autotune(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t f
     cur.split = 0;
     float best_ms = 1e30f;
     int rc = SVO_OK;
-    // stage 1: the serial / small-triangle thresholds; stage 2: queue entry size
+    // stage 1: the serial / small-triangle thresholds and the serial tier's
+    // layout; stage 2: queue entry size
     for (uint32_t sm : {32u, 64u, 128u, 256u}) {
-        for (uint32_t ip : {16u, 32u, 64u}) {
+        for (uint32_t cand = 0; cand < 6; ++cand) {
             VoxTuning t = cur;
             t.serial_max = sm;
-            t.inplace_max = ip;
+            t.inplace_max = cand % 3 == 0 ? 16u : cand % 3 == 1 ? 32u : 64u;
+            t.serial_packed = cand / 3;
             t.warp_max = 256;
             float ms = 0.0f;
             if ((rc = measure(t, ms)) != SVO_OK) break;
@@ -1200,6 +1206,7 @@ int svo_ctx_autotune(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t f
         best->warp_max = win.warp_max;
         best->split = win.split;
         best->inplace_max = win.inplace_max;
+        best->serial_packed = win.serial_packed;
     }
     return SVO_OK;
 }

@@ -21,6 +21,7 @@ struct VoxTuning {
     uint32_t warp_max = 256;     // 4x4x4 bricks per queue entry (one warp walks one entry)
     uint32_t split = 0;          // cull 2x2x2 sub-bricks of surviving bricks too
     uint32_t inplace_max = 32;   // bricks of a triangle walked by the warp that set it up
+    uint32_t serial_packed = 0;  // serial tier: rows packed across the warp's lanes (else one triangle per lane)
 };
 
 // Occupancy bitmap pyramid: level 0 is the voxel grid (one bit per Morton

@@ -585,22 +585,64 @@ __device__ __forceinline__ void warp_packed(const BatchDev &bd, const Tri *st, i
     }
 }
 
+// The rows (y, z) of the warp's serial-tier triangles (lane i's triangle
+// st[i], mesh sm[i], with nrows > 0 rows along x), packed 32 per round: each
+// lane takes one row, copies its triangle's setup from shared memory and
+// tests the row along x with the serial arithmetic (row_prep: YZ tests
+// reject the whole row; voxel_test per x), so lanes stay busy whatever the
+// triangles' shapes.
+template <bool S>
+__device__ __forceinline__ void warp_rows(const BatchDev &bd, const Tri *st, const int *sm, uint32_t nrows,
+                                          int lane) {
+    uint32_t incl = nrows;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += y;
+    }
+    const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+    const uint32_t excl = incl - nrows;
+    for (uint32_t base = 0; base < total; base += 32) {
+        const uint32_t item = base + lane;
+        int pos = 0;  // owner lane: the number of lanes whose inclusive count is <= item
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const uint32_t v = __shfl_sync(0xFFFFFFFFu, incl, pos + step - 1);
+            if (v <= item) pos += step;
+        }
+        const int src = item < total ? pos : 0;
+        const uint32_t j = item - __shfl_sync(0xFFFFFFFFu, excl, src);
+        if (item < total) {
+            const Tri &t = st[src];
+            const int mm = sm[src];
+            const GridParams g = *bd.mesh[mm].gp;
+            const uint32_t ny = (uint32_t)(t.hi[1] - t.lo[1] + 1);
+            HitSink sink{reinterpret_cast<uint32_t *>(bd.mesh[mm].bits)};
+            row_segment<S>(t, g, t.lo[1] + (int)(j % ny), t.lo[2] + (int)(j / ny), t.lo[0], t.hi[0], sink);
+            sink.flush();
+        }
+    }
+}
+
 // One thread per triangle of the batch (global index -> mesh by tri_off):
 // setup, then
-//   tier 0 (grid bbox <= serial_max voxels): its own serial row-by-row test;
+//   tier 0 (grid bbox <= serial_max voxels): the serial row-by-row test, by
+//     this thread (serial_packed 0) or packed one row per lane (ROWS);
 //   tier 1 (<= inplace_max 4^3 bricks, or any size when INPLACE): with a
 //     small-triangle list, its index is appended there for
 //     k_voxelize_small; INPLACE (no list or queue), its bricks are walked by
 //     this warp right away (warp_packed);
 //   tier 2 (more bricks): queue entries of <= warp_max bricks for
 //     k_voxelize_bricks, which balances them across the GPU.
-template <bool S, bool INPLACE>
+template <bool S, bool INPLACE, bool ROWS>
 __global__ void __launch_bounds__(256, INPLACE ? 2 : 3)
     k_voxelize(BatchDev bd, int64_t total, VoxTuning tune, uint4 *__restrict__ big, uint32_t big_cap,
                uint32_t *__restrict__ big_count, uint64_t *__restrict__ small, uint32_t *__restrict__ small_count) {
-    __shared__ Tri s_tri[INPLACE ? 8 : 1][32];  // INPLACE: the warp's tier-1 triangles
+    __shared__ Tri s_tri[8][32];  // the warp's serial-tier triangles, then (INPLACE) its tier-1 ones
+    __shared__ int s_mesh[8][32];  // their meshes
     const int lane = threadIdx.x & 31;
-    Tri *st = s_tri[INPLACE ? (threadIdx.x >> 5) : 0];
+    Tri *st = s_tri[threadIdx.x >> 5];
+    int *sm = s_mesh[threadIdx.x >> 5];
     const int64_t warp0 = (blockIdx.x * (int64_t)blockDim.x + threadIdx.x) - lane;
     const int64_t stride = (int64_t)gridDim.x * blockDim.x;
     for (int64_t base = warp0; base < total; base += stride) {
@@ -619,13 +661,7 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3)
                                  (uint64_t)(t.hi[2] - t.lo[2] + 1);
             nb = brick_count(t);
             tier = vol <= (uint64_t)tune.serial_max ? 0 : (INPLACE || nb <= tune.inplace_max) ? 1 : 2;
-            if (tier == 0) {
-                HitSink sink{reinterpret_cast<uint32_t *>(md.bits)};
-                for (int z = t.lo[2]; z <= t.hi[2]; ++z)
-                    for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
-                sink.flush();
-            } else if (tier == 1) {
-                if (INPLACE) st[lane] = t;
+            if (tier == 1 || tier == 0) {
             } else {
                 const uint32_t eb = tune.warp_max;
                 const uint32_t ne = (nb + eb - 1) / eb;
@@ -636,8 +672,29 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3)
                 }
             }
         }
+        if (ROWS) {  // the warp's serial-tier rows, packed across lanes
+            if (__any_sync(0xFFFFFFFFu, tier == 0)) {
+                const uint32_t nrows =
+                    tier == 0 ? (uint32_t)(t.hi[1] - t.lo[1] + 1) * (uint32_t)(t.hi[2] - t.lo[2] + 1) : 0u;
+                if (tier == 0) {
+                    st[lane] = t;
+                    sm[lane] = m;
+                }
+                __syncwarp();
+                warp_rows<S>(bd, st, sm, nrows, lane);
+                __syncwarp();  // st is rewritten below or by the next round
+            }
+        } else if (tier == 0) {  // each lane walks its own triangle's rows
+            const MeshDev &md = bd.mesh[m];
+            const GridParams g = *md.gp;
+            HitSink sink{reinterpret_cast<uint32_t *>(md.bits)};
+            for (int z = t.lo[2]; z <= t.hi[2]; ++z)
+                for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
+            sink.flush();
+        }
         if (INPLACE) {
             if (__any_sync(0xFFFFFFFFu, tier == 1)) {
+                if (tier == 1) st[lane] = t;
                 __syncwarp();
                 warp_packed<S>(bd, st, m, tier == 1 ? nb : 0u, lane);
                 __syncwarp();  // st is rewritten by the next round
@@ -809,13 +866,19 @@ cudaError_t launch_voxelize(const BatchDev &b, int64_t total, bool strict, const
         VoxTuning tn = tune;
         if (!inplace && (total < (int64_t)num_sms * 256 || !small)) tn.inplace_max = 0;
         uint32_t *small_count = counters + 3;
-#define SVO_VOX(S_, I_) \
-    k_voxelize<S_, I_><<<blocks, 256, 0, st>>>(b, total, tn, big, big_cap, counters, small, small_count)
+#define SVO_VOX(S_, I_, R_) \
+    k_voxelize<S_, I_, R_><<<blocks, 256, 0, st>>>(b, total, tn, big, big_cap, counters, small, small_count)
+#define SVO_VOX2(S_, I_) \
+    do {                   \
+        if (tn.serial_packed) SVO_VOX(S_, I_, true); \
+        else SVO_VOX(S_, I_, false);                 \
+    } while (0)
         if (strict) {
-            if (inplace) SVO_VOX(true, true); else SVO_VOX(true, false);
+            if (inplace) SVO_VOX2(true, true); else SVO_VOX2(true, false);
         } else {
-            if (inplace) SVO_VOX(false, true); else SVO_VOX(false, false);
+            if (inplace) SVO_VOX2(false, true); else SVO_VOX2(false, false);
         }
+#undef SVO_VOX2
 #undef SVO_VOX
         count_launches(1);
         if (!inplace) {

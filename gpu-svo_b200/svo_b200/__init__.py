@@ -64,7 +64,7 @@ class _Aabb(C.Structure):
 
 class Tuning(C.Structure):
     _fields_ = [("serial_max", C.c_uint32), ("warp_max", C.c_uint32), ("split", C.c_uint32),
-                ("inplace_max", C.c_uint32)]
+                ("inplace_max", C.c_uint32), ("serial_packed", C.c_uint32)]
 
 
 class MeshDesc(C.Structure):
@@ -239,10 +239,10 @@ class Context:
 
     @property
     def tuning(self) -> tuple:
-        """(serial_max, warp_max, split, inplace_max) of the voxelizer work split."""
+        """(serial_max, warp_max, split, inplace_max, serial_packed) of the voxelizer work split."""
         t = Tuning()
         _check(lib().svo_ctx_get_tuning(self._h, C.byref(t)))
-        return (t.serial_max, t.warp_max, t.split, t.inplace_max)
+        return (t.serial_max, t.warp_max, t.split, t.inplace_max, t.serial_packed)
 
     @tuning.setter
     def tuning(self, value) -> None:
@@ -252,11 +252,11 @@ class Context:
 
     def autotune(self, meshes, flags: int = 0, stream: int = 0) -> tuple:
         """svo_ctx_autotune over sample meshes [(points, tris, res), ...]: installs
-        and returns the fastest (serial_max, warp_max, split, inplace_max)."""
+        and returns the fastest (serial_max, warp_max, split, inplace_max, serial_packed)."""
         descs, keep = _descs(meshes, flags)
         t = Tuning()
         _check(lib().svo_ctx_autotune(self._h, descs, len(meshes), flags, stream or None, C.byref(t)))
-        return (t.serial_max, t.warp_max, t.split, t.inplace_max)
+        return (t.serial_max, t.warp_max, t.split, t.inplace_max, t.serial_packed)
 
     def build(self, points, tris, res, flags: int = 0, stream: int = 0) -> "Result":
         """svo_build.  points float32[n,3] and tris int32[m,3] (tris=None: soup),

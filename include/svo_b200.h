@@ -97,7 +97,9 @@ int svo_ctx_device(const svo_ctx *ctx, int *device);
 int svo_ctx_reserve(svo_ctx *ctx, uint64_t result_bytes, uint64_t scratch_bytes, void *stream);
 
 /* Voxelizer work split: triangles whose grid bbox has at most serial_max
- * voxels are tested by one thread; triangles of at most inplace_max 4x4x4
+ * (<= 65536) voxels are tested row by row without culling, the rows of a
+ * warp's such triangles handed out one row per lane per round
+ * (serial_packed = 1) or one triangle per lane (0, the default); triangles of at most inplace_max 4x4x4
  * bricks are walked by the warp that set them up, packed 32 bricks per round
  * across the warp's triangles; larger ones are cut into queue entries of at
  * most warp_max bricks, one warp per entry.  Results do not depend on these
@@ -108,6 +110,7 @@ typedef struct svo_tuning {
     uint32_t warp_max;
     uint32_t split; /* also cull the 2x2x2 sub-bricks of surviving bricks (queue tier) */
     uint32_t inplace_max;
+    uint32_t serial_packed;
 } svo_tuning;
 int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t);
 int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t);

@@ -116,3 +116,31 @@ def test_autotune_keeps_results(gpu_ctx, svo_mod):
             assert a.keys().tobytes() == b.keys().tobytes()
     finally:
         gpu_ctx.tuning = saved
+
+
+def test_tuning_variants_keep_results(gpu_ctx, svo_mod):
+    """Every voxelizer work split (tier thresholds, serial-tier row layout,
+    queue entry size, sub-brick culling) gives the same octree."""
+    from svo_b200 import meshgen
+
+    meshes = meshgen.batch(6, seed=11)
+    pts, tris, _ = meshgen.torus_slivers(20000)
+    meshes.append((pts, tris, 128))
+    meshes.append((pts, tris, 512))
+    saved = gpu_ctx.tuning
+    try:
+        ref = [gpu_ctx.build(p, t, r, svo_mod.FLAG_NO_VERT_EDGE) for p, t, r in meshes]
+        for tune in [(64, 256, 0, 32, 0), (64, 256, 0, 32, 1), (1, 256, 0, 32, 1), (4096, 256, 0, 32, 1),
+                     (0, 7, 1, 0, 1), (256, 1024, 0, 64, 0), (256, 64, 1, 16, 1)]:
+            gpu_ctx.tuning = tune
+            assert gpu_ctx.tuning == tune
+            for (p, t, r), a in zip(meshes, ref):
+                b = gpu_ctx.build(p, t, r, svo_mod.FLAG_NO_VERT_EDGE)
+                assert a.nodes().tobytes() == b.nodes().tobytes(), tune
+                assert a.keys().tobytes() == b.keys().tobytes(), tune
+        with pytest.raises(svo_mod.SvoError):
+            gpu_ctx.tuning = (1 << 17, 256, 0, 32, 1)
+        with pytest.raises(svo_mod.SvoError):
+            gpu_ctx.tuning = (64, 256, 0, 32, 2)
+    finally:
+        gpu_ctx.tuning = saved
