@@ -16,13 +16,16 @@
 //   1. mark a candidate bitmap D over Q = P >> 1 (each bit stands for the 8
 //      lattice points 2Q + r) from the node groups of levels >= 1 -- every
 //      level-0 corner is also a corner of a level-1 node;
-//   2. walk D's set bits in order and derive, per Q, the 8 points' keys from
-//      8 parent-bitmap lookups (coarser levels only for r = 0);
-//   3. count per 2048-bit chunk of D, scan, and emit: the keys come out in
+//   2. walk D's set bits in order and derive, per Q, what its 8 points need
+//      from 8 parent-bitmap lookups per level (coarser levels only for
+//      r = 0), packed into one 64-bit state per Q (q_state below), counting
+//      keys per 2048-bit chunk of D;
+//   3. scan the counts and expand the states into keys: the keys come out in
 //      Morton order because D is in Morton order and each point's keys are
-//      produced in (level, axis) order.
-// D has R^3 bits (1 GiB at R = 2048); a 1-bit-per-chunk summary lets the two
-// walks skip untouched chunks without reading them.
+//      produced in (level, axis) order.  Each warp stages its keys in shared
+//      memory and stores them coalesced.
+// D has R^3 bits (1 GiB at R = 2048); a 1-bit-per-chunk summary lets the walk
+// skip untouched chunks without reading them.
 #include <cstdio>
 
 #include "svo_host.h"
@@ -33,6 +36,7 @@ namespace {
 
 constexpr int kDedupWarps = 8;
 constexpr uint64_t kChunkWords = 32;  // u64 words of D per chunk (2048 bits)
+constexpr uint32_t kStageKeys = 512;  // keys of one kind a warp stages in shared memory
 
 struct DedupLevel {
     const uint64_t *bits;  // occupancy bitmap of this level
@@ -51,8 +55,13 @@ struct DedupParams {
     uint64_t chunks;
     const uint32_t *list;       // the touched chunks (a set bit in G), in order
     uint64_t ntouched;
-    uint32_t *cnt;              // [3][ntouched]
-    const uint32_t *pre;        // [3][ntouched + 1]
+    unsigned long long *nq;     // set bits of D (counted while marking)
+    uint32_t *qn;               // [ntouched] set bits per touched chunk
+    const uint32_t *qpre;       // [ntouched + 1] their prefix: the first state of each chunk
+    uint64_t *qs;               // one state per set bit of D, in order
+    uint64_t ntiles;            // tiles of 32 consecutive states
+    uint32_t *tcnt;             // [3][ntiles] keys per tile and kind
+    const uint32_t *tpre;       // [3][ntiles + 1] their prefixes
     uint64_t *out[3];
 };
 
@@ -63,9 +72,12 @@ __device__ __forceinline__ void mark_chunk(const DedupParams &p, uint64_t bit) {
     if (!(*(volatile uint32_t *)g & m)) atomicOr(g, m);
 }
 
-__device__ __forceinline__ void mark_bit(const DedupParams &p, uint64_t bit) {
-    atomicOr(p.D + (bit >> 5), 1u << (bit & 31));
+// Returns 1 when the bit was not set before.
+__device__ __forceinline__ uint32_t mark_bit(const DedupParams &p, uint64_t bit) {
+    const uint32_t m = 1u << (bit & 31);
+    const uint32_t old = atomicOr(p.D + (bit >> 5), m);
     mark_chunk(p, bit);
+    return (old & m) ? 0u : 1u;
 }
 
 // Marks the Q of every corner of every node at levels >= 1.
@@ -74,15 +86,17 @@ __device__ __forceinline__ void mark_bit(const DedupParams &p, uint64_t bit) {
 //     of D gets the sub-points k' with k'_i = 0 wherever e_i = 1;
 //   level l >= 2: Q = (2g + {0,1,2}^3) << (l - 1), one bit each;
 //   the root (level T): Q = (root + {0,1}^3) << (T - 1).
+//   Also counts the bits it sets first (*p.nq: the set bits of D).
 __global__ void k_dedup_mark(const __grid_constant__ DedupParams p, uint32_t total) {
+    uint32_t fresh = 0;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         if (t == total - 1) {
             const uint64_t rc = *p.root;
             const uint32_t r[3] = {compact3(rc), compact3(rc >> 1), compact3(rc >> 2)};
             const int sh = p.T - 1;
             for (int d = 0; d < 8; ++d)
-                mark_bit(p, morton3((r[0] + (d & 1)) << sh, (r[1] + ((d >> 1) & 1)) << sh,
-                                    (r[2] + ((d >> 2) & 1)) << sh));
+                fresh += mark_bit(p, morton3((r[0] + (d & 1)) << sh, (r[1] + ((d >> 1) & 1)) << sh,
+                                             (r[2] + ((d >> 2) & 1)) << sh));
             continue;
         }
         int l = 1;
@@ -96,17 +110,20 @@ __global__ void k_dedup_mark(const __grid_constant__ DedupParams p, uint32_t tot
                 if (e & 1) m &= 0x55u;
                 if (e & 2) m &= 0x33u;
                 if (e & 4) m &= 0x0Fu;
-                atomicOr(p.D + (byte >> 2), m << (8 * (byte & 3)));
+                m <<= 8 * (byte & 3);
+                fresh += __popc(m & ~atomicOr(p.D + (byte >> 2), m));
                 mark_chunk(p, byte << 3);
             }
         } else {
             const int sh = l - 1;
             for (int k = 0; k < 27; ++k) {
                 const uint32_t kx = k % 3, ky = (k / 3) % 3, kz = k / 9;
-                mark_bit(p, morton3((2 * g[0] + kx) << sh, (2 * g[1] + ky) << sh, (2 * g[2] + kz) << sh));
+                fresh += mark_bit(p, morton3((2 * g[0] + kx) << sh, (2 * g[1] + ky) << sh, (2 * g[2] + kz) << sh));
             }
         }
     }
+    fresh = __reduce_add_sync(0xFFFFFFFFu, fresh);
+    if ((threadIdx.x & 31) == 0 && fresh) atomicAdd(p.nq, (unsigned long long)fresh);
 }
 
 // Bit e of the result: cell v - e exists at the level whose occupancy bitmap
@@ -182,86 +199,95 @@ __device__ __forceinline__ uint32_t coarse_ex(const DedupParams &p, const DedupT
     return (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) ? 1u << (dx | dy << 1 | dz << 2) : 0u;
 }
 
-// What one Q needs for all its keys: the level-0 parent mask E0 (the 8
-// points 2Q + r at level 0) and the cells around 2Q at level 1.  Levels >= 2
-// apply only to Q even in every coordinate and are computed where needed.
-struct QState {
-    uint32_t E0, ex1;
+// What one Q needs for all its keys, packed into 64 bits:
+//   bits 0-35  qc, the Morton code of Q
+//   bits 36-43 E0, the level-1 parent mask around Q (the 8 points 2Q + r at
+//              level 0 follow from it through the tables)
+//   bits 44-50 key kinds of the point 2Q at level 1
+//   bits 51-57 key kinds of the point 2Q at level 2 (Q a multiple of 8 in
+//              Morton code, i.e. even in every coordinate)
+//   bit  58    levels >= 3 apply as well (Q a multiple of 64); they are
+//              derived where needed, from the coarser bitmaps
+constexpr uint64_t kQcMask = (1ull << 36) - 1;
+
+__device__ __forceinline__ uint64_t q_state(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                            uint64_t root, uint64_t qc) {
+    const uint32_t E0 = cell_mask(p.lv[1].bits, qc, sx[1]);
+    uint64_t s = qc | (uint64_t)E0 << 36 | (uint64_t)tb.kinds[coarse_ex(p, tb, sx, root, 1, qc)] << 44;
+    if (p.T >= 2 && (qc & 7) == 0) {
+        s |= (uint64_t)tb.kinds[coarse_ex(p, tb, sx, root, 2, qc >> 3)] << 51;
+        if (p.T >= 3 && (qc & 63) == 0) s |= 1ull << 58;
+    }
+    return s;
+}
+
+// Key kinds of the point 2Q at levels >= 3 (state bit 58): vertex flag into
+// v, edges/faces of level l at bits 3(l - 3)..3(l - 3) + 2 of eh/fh.
+__device__ __forceinline__ void q_deep(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                       uint64_t root, uint64_t qc, uint32_t &v, uint32_t &eh, uint32_t &fh) {
+    uint64_t uc = qc >> 6;
+    for (int l = 3; l <= p.T; ++l) {
+        if (l > 3) {
+            if (uc & 7) break;
+            uc >>= 3;
+        }
+        const uint32_t k = tb.kinds[coarse_ex(p, tb, sx, root, l, uc)];
+        v |= k & 1;
+        eh |= ((k >> 1) & 7) << (3 * (l - 3));
+        fh |= ((k >> 4) & 7) << (3 * (l - 3));
+    }
+}
+
+// The keys of one Q as slot masks, each kind in output order:
+//   v: bit r = vertex of the point 2Q + r (r = 0 at any level);
+//   el/fl: bits 3l + axis for the point 2Q at levels 0..2, then bits
+//          9 + 3(r - 1) + axis for the points r = 1..7 at level 0;
+//   eh/fh: the point 2Q at levels 3..T (bit 3(l - 3) + axis), which come
+//          between bits 8 and 9 of el/fl in the output.
+struct QMasks {
+    uint32_t v, el, fl, eh, fh;
 };
 
-__device__ __forceinline__ QState q_eval(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                         uint64_t root, uint64_t qc) {
-    return QState{cell_mask(p.lv[1].bits, qc, sx[1]), coarse_ex(p, tb, sx, root, 1, qc)};
+__device__ __forceinline__ QMasks q_masks(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                          uint64_t root, uint64_t s) {
+    const uint32_t E0 = (uint32_t)(s >> 36) & 0xFFu, k1 = (uint32_t)(s >> 44) & 0x7Fu, k2 = (uint32_t)(s >> 51) & 0x7Fu;
+    const uint32_t k0 = tb.kinds[tb.around[E0 * 8]];
+    QMasks m;
+    m.v = (k0 | k1 | k2) & 1u;
+    m.el = ((k0 >> 1) & 7) | ((k1 >> 1) & 7) << 3 | ((k2 >> 1) & 7) << 6;
+    m.fl = ((k0 >> 4) & 7) | ((k1 >> 4) & 7) << 3 | ((k2 >> 4) & 7) << 6;
+    m.eh = m.fh = 0;
+    if ((s >> 58) & 1) q_deep(p, tb, sx, root, s & kQcMask, m.v, m.eh, m.fh);
+#pragma unroll
+    for (int r = 1; r < 8; ++r) {
+        const uint32_t k = tb.kinds[tb.around[E0 * 8 + r]];
+        m.v |= (k & 1u) << r;
+        m.el |= ((k >> 1) & 7) << (9 + 3 * (r - 1));
+        m.fl |= ((k >> 4) & 7) << (9 + 3 * (r - 1));
+    }
+    return m;
 }
 
-// Keys of the 8 points per kind (vertices, edges, faces).
+// Keys per kind of one Q from its state (cnt0 covers the 8 points at level 0).
 __device__ __forceinline__ void q_count(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                        uint64_t root, uint64_t qc, const QState &q, uint32_t c[3]) {
-    const uint32_t k0 = tb.cnt0[q.E0];
-    c[0] += k0 & 0xFF;
-    c[1] += (k0 >> 8) & 0xFF;
-    c[2] += k0 >> 16;
-    const bool v0 = tb.kinds[tb.around[q.E0 * 8]] & 1;
-    uint32_t k = tb.kinds[q.ex1];
-    bool v = v0 || (k & 1);
-    c[1] += __popc((k >> 1) & 7);
-    c[2] += __popc((k >> 4) & 7);
-    uint64_t uc = qc;
-    for (int l = 2; l <= p.T; ++l) {
-        if (uc & 7) break;
-        uc >>= 3;
-        k = tb.kinds[coarse_ex(p, tb, sx, root, l, uc)];
-        v |= k & 1;
-        c[1] += __popc((k >> 1) & 7);
-        c[2] += __popc((k >> 4) & 7);
-    }
-    c[0] += (v && !v0) ? 1u : 0u;  // a vertex of coarser nodes only
-}
-
-// Writes the keys of the 8 points at the cursors o[] (vertices, edges,
-// faces), each kind in output order: point, then level, then axis.
-__device__ __forceinline__ void q_write(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                        uint64_t root, uint64_t qc, const QState &q, uint64_t *o[3]) {
-    {  // r = 0: level 0, level 1, then every level l with 2Q a multiple of 2^l
-        const uint64_t pc = qc << 3;
-        uint32_t k = tb.kinds[tb.around[q.E0 * 8]];
-        bool v = k & 1;
-        for (uint32_t a = 0; a < 3; ++a)
-            if ((k >> (1 + a)) & 1) *o[1]++ = (pc << 6) | a;
-        for (uint32_t a = 0; a < 3; ++a)
-            if ((k >> (4 + a)) & 1) *o[2]++ = (pc << 6) | a;
-        uint64_t uc = qc;
-        for (int l = 1; l <= p.T; ++l) {
-            if (l >= 2) {
-                if (uc & 7) break;
-                uc >>= 3;
-            }
-            k = tb.kinds[l == 1 ? q.ex1 : coarse_ex(p, tb, sx, root, l, uc)];
-            v |= k & 1;
-            for (uint32_t a = 0; a < 3; ++a)
-                if ((k >> (1 + a)) & 1) *o[1]++ = (pc << 6) | ((uint64_t)l << 2) | a;
-            for (uint32_t a = 0; a < 3; ++a)
-                if ((k >> (4 + a)) & 1) *o[2]++ = (pc << 6) | ((uint64_t)l << 2) | a;
-        }
-        if (v) *o[0]++ = pc;
-    }
-    for (uint32_t r = 1; r < 8; ++r) {
-        const uint64_t pc = (qc << 3) | r;
-        const uint32_t k = tb.kinds[tb.around[q.E0 * 8 + r]];
-        if (k & 1) *o[0]++ = pc;
-        for (uint32_t a = 0; a < 3; ++a)
-            if ((k >> (1 + a)) & 1) *o[1]++ = (pc << 6) | a;
-        for (uint32_t a = 0; a < 3; ++a)
-            if ((k >> (4 + a)) & 1) *o[2]++ = (pc << 6) | a;
-    }
+                                        uint64_t root, uint64_t s, uint32_t c[3]) {
+    const uint32_t E0 = (uint32_t)(s >> 36) & 0xFFu, k1 = (uint32_t)(s >> 44) & 0x7Fu, k2 = (uint32_t)(s >> 51) & 0x7Fu;
+    const uint32_t k0 = tb.cnt0[E0];
+    uint32_t v = k1 | k2;
+    uint32_t e = ((k1 >> 1) & 7) | ((k2 >> 1) & 7) << 3, f = ((k1 >> 4) & 7) | ((k2 >> 4) & 7) << 3;
+    uint32_t eh = 0, fh = 0;
+    if ((s >> 58) & 1) q_deep(p, tb, sx, root, s & kQcMask, v, eh, fh);
+    const bool v0 = tb.kinds[tb.around[E0 * 8]] & 1;
+    c[0] += (k0 & 0xFF) + ((!v0 && (v & 1)) ? 1u : 0u);
+    c[1] += ((k0 >> 8) & 0xFF) + __popc(e) + __popc(eh);
+    c[2] += (k0 >> 16) + __popc(f) + __popc(fh);
 }
 
 // One warp per touched chunk of D.  The chunk's set bits are listed in order
-// in shared memory, then taken 32 at a time (lane i the i-th): counts per
-// kind (EMIT false, one total per chunk) or keys written at the chunk's
-// scanned offset plus the warp prefix of the batch (EMIT true).
-template <bool EMIT>
-__global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_keys(const __grid_constant__ DedupParams p) {
+// in shared memory, then taken 32 at a time (lane i the i-th): each Q's
+// state is stored at its rank (the chunk's first state + its index) and its
+// keys are counted per kind into the rank's tile of 32 states.
+__global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_state(const __grid_constant__ DedupParams p) {
     __shared__ DedupTables tb;
     __shared__ uint16_t list[kDedupWarps][2048];
     __shared__ uint64_t sx[kMaxLevels];  // dilated side of each level
@@ -287,45 +313,136 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_keys(const __grid_co
         for (uint32_t k = incl - n; word; word &= word - 1, ++k)
             lst[k] = (uint16_t)(lane * 64 + __ffsll((long long)word) - 1);
         __syncwarp();
-        uint32_t c[3] = {0, 0, 0};
-        uint64_t base[3] = {0, 0, 0};
-        if (EMIT)
-            for (int k = 0; k < 3; ++k) base[k] = p.pre[k * (p.ntouched + 1) + i];
+        const uint32_t q0 = p.qpre[i];
         for (uint32_t j0 = 0; j0 < total; j0 += 32) {
             const uint32_t j = j0 + lane;
             const bool act = j < total;
-            const uint64_t qc = ch * 2048 + (act ? lst[j] : 0);
-            const QState q = act ? q_eval(p, tb, sx, root, qc) : QState{0, 0};
-            if (!EMIT) {
-                if (act) q_count(p, tb, sx, root, qc, q, c);
-                continue;
+            uint32_t c[3] = {0, 0, 0};
+            if (act) {
+                const uint64_t s = q_state(p, tb, sx, root, ch * 2048 + lst[j]);
+                p.qs[q0 + j] = s;
+                q_count(p, tb, sx, root, s, c);
             }
-            uint32_t cq[3] = {0, 0, 0};
-            if (act) q_count(p, tb, sx, root, qc, q, cq);
-            uint64_t *o[3];
+            // a round spans at most two tiles: one atomic per tile and kind
+            const uint32_t tile = act ? (q0 + j) >> 5 : 0xFFFFFFFFu;
+            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, tile);
+            if (act) {
 #pragma unroll
-            for (int k = 0; k < 3; ++k) {
-                uint32_t x = cq[k];
-#pragma unroll
-                for (int d = 1; d < 32; d <<= 1) {
-                    const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
-                    if (lane >= d) x += y;
+                for (int k = 0; k < 3; ++k) {
+                    const uint32_t sum = __reduce_add_sync(peers, c[k]);
+                    if (lane == __ffs(peers) - 1 && sum) atomicAdd(p.tcnt + k * p.ntiles + tile, sum);
                 }
-                o[k] = p.out[k] + base[k] + (x - cq[k]);
-                base[k] += __shfl_sync(0xFFFFFFFFu, x, 31);
             }
-            if (act) q_write(p, tb, sx, root, qc, q, o);
         }
         __syncwarp();
-        if (!EMIT) {
-#pragma unroll
-            for (int k = 0; k < 3; ++k) {
-#pragma unroll
-                for (int d = 16; d > 0; d >>= 1) c[k] += __shfl_xor_sync(0xFFFFFFFFu, c[k], d);
-            }
-            if (lane < 3) p.cnt[lane * p.ntouched + i] = lane == 0 ? c[0] : lane == 1 ? c[1] : c[2];
+    }
+}
+
+// Stage position of key i: XOR-swizzled within rows of 16 keys, so that
+// lanes writing runs that start 16 keys apart hit different banks.
+__device__ __forceinline__ uint32_t stage_at(uint32_t i) { return i ^ ((i >> 4) & 15u); }
+
+// Key offsets of the edge/face slots of el/fl: (r << 6) | (l << 2) | axis.
+struct KeyOffsets {
+    uint16_t lo[32];
+};
+
+__device__ void init_offsets(KeyOffsets &t) {
+    if (threadIdx.x < 32) {
+        const uint32_t s = threadIdx.x;
+        uint32_t off = 0;
+        if (s < 9) off = (s / 3) << 2 | (s % 3);
+        else if (s < 30) off = (1 + (s - 9) / 3) << 6 | ((s - 9) % 3);
+        t.lo[s] = (uint16_t)off;
+    }
+}
+
+// Writes the keys of one Q (code qc) for one kind at positions at, at + 1, ...
+// of o (through stage_at when STAGED).  Vertices: v's bits; edges/faces:
+// lo's bits 0-8, then hi's, then lo's bits 9-29.
+template <int KIND, bool STAGED>
+__device__ __forceinline__ void put_keys(uint64_t *o, uint32_t at, uint32_t lo, uint32_t hi, uint64_t qc,
+                                         const KeyOffsets &ko) {
+    if (KIND == 0) {
+        const uint64_t b = qc << 3;
+        for (uint32_t m = lo; m; m &= m - 1, ++at) o[STAGED ? stage_at(at) : at] = b | (uint64_t)(__ffs(m) - 1);
+        return;
+    }
+    const uint64_t b = qc << 9;
+    const uint32_t nh = __popc(hi);
+    uint32_t k = at;
+    for (uint32_t m = lo; m; m &= m - 1, ++k) {
+        const int s = __ffs(m) - 1;
+        const uint32_t pos = k + (s >= 9 ? nh : 0u);
+        o[STAGED ? stage_at(pos) : pos] = b | ko.lo[s];
+    }
+    if (hi) {  // levels >= 3 of the point 2Q
+        uint32_t pos = at + __popc(lo & 0x1FFu);
+        for (uint32_t m = hi; m; m &= m - 1, ++pos) {
+            const int s = __ffs(m) - 1, l = 3 + s / 3;
+            o[STAGED ? stage_at(pos) : pos] = b | (uint64_t)((l << 2) | (s % 3));
         }
     }
+}
+
+// One kind's keys of the warp's 32 Qs: lane offsets by a warp scan; staged
+// in shared memory and stored coalesced when they fit, else stored directly.
+template <int KIND>
+__device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t lo, uint32_t hi, uint64_t qc,
+                                          uint64_t *stage, const KeyOffsets &ko, int lane) {
+    const uint32_t c = __popc(lo) + __popc(hi);
+    uint32_t x = c;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+        if (lane >= d) x += y;
+    }
+    const uint32_t tot = __shfl_sync(0xFFFFFFFFu, x, 31);
+    if (tot <= kStageKeys) {
+        put_keys<KIND, true>(stage, x - c, lo, hi, qc, ko);
+        __syncwarp();
+        for (uint32_t i = lane; i < tot; i += 32) out[base + i] = stage[stage_at(i)];
+        __syncwarp();
+    } else {
+        put_keys<KIND, false>(out + base, x - c, lo, hi, qc, ko);
+    }
+}
+
+// One warp per tile of 32 consecutive states, expanded into keys at the
+// tile's scanned offsets.
+__global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_write(const __grid_constant__ DedupParams p,
+                                                                 uint64_t nq) {
+    __shared__ DedupTables tb;
+    __shared__ KeyOffsets ko;
+    __shared__ uint64_t stage[kDedupWarps][kStageKeys];
+    __shared__ uint64_t sx[kMaxLevels];
+    if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
+    init_offsets(ko);
+    init_tables(tb);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
+    const uint64_t root = *p.root;
+    uint64_t *stg = stage[warp];
+    for (uint64_t t = (uint64_t)blockIdx.x * kDedupWarps + warp; t < p.ntiles; t += nwarps) {
+        const uint64_t r = t * 32 + lane;
+        const bool act = r < nq;
+        const uint64_t s = act ? p.qs[r] : 0;
+        const QMasks m = act ? q_masks(p, tb, sx, root, s) : QMasks{0, 0, 0, 0, 0};
+        const uint64_t qc = s & kQcMask;
+        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, ko, lane);
+        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, ko, lane);
+        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, ko, lane);
+    }
+}
+
+// Set bits per touched chunk (one warp per chunk).
+__global__ void k_chunk_bits(const __grid_constant__ DedupParams p) {
+    const uint64_t w = (blockIdx.x * (uint64_t)blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= p.ntouched) return;
+    const uint64_t *D64 = reinterpret_cast<const uint64_t *>(p.D);
+    const uint32_t n = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)__popcll(D64[(uint64_t)p.list[w] * kChunkWords + lane]));
+    if (lane == 0) p.qn[w] = n;
 }
 
 // The touched chunks in order: per-word popcounts of G, then (after a scan)
@@ -362,6 +479,7 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     }
     const int T = ep.T;
     if (T < 1) return dedup_fail(SVO_ERR_DEGENERATE, "dedup needs at least two levels");
+    if (T > 12) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup of more than 13 levels");
     if ((uint64_t)ep.N * 12 > 0xFFFFFFFFull) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup of more than 357M nodes");
     DedupParams p{};
     p.T = T;
@@ -385,7 +503,7 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     void *blk[7] = {};
     const size_t sz[7] = {d_words * 8, g_words * 4, g_words * 4, (g_words + 1) * 4, p.chunks * 4,
                           scan_scratch_words(std::max<uint64_t>(p.chunks, g_words)) * 8, 256};
-    void *blk2[2] = {};  // per touched chunk: counts and their prefixes (sized once the count is known)
+    void *blk2[6] = {};  // sized once the counts are known: states per chunk, the states, keys per tile
     cudaError_t e = cudaSuccess;
     for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = cudaMallocFromPoolAsync(&blk[i], sz[i], pool, st);
     auto release = [&]() {
@@ -409,8 +527,9 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     p.list = list;
     auto *scan = static_cast<unsigned long long *>(blk[5]);
     uint32_t *status = static_cast<uint32_t *>(blk[6]);
+    p.nq = reinterpret_cast<unsigned long long *>(static_cast<char *>(blk[6]) + 8);
     if ((e = cudaMemsetAsync(p.D, 0, sz[0], st)) != cudaSuccess || (e = cudaMemsetAsync(p.G, 0, sz[1], st)) ||
-        (e = cudaMemsetAsync(status, 0, 4, st)))
+        (e = cudaMemsetAsync(status, 0, 16, st)))
         return fail(e, "memset");
     k_dedup_mark<<<(mark_total + 255) / 256, 256, 0, st>>>(p, mark_total);
     k_touched_count<<<(unsigned)((g_words + 255) / 256), 256, 0, st>>>(p.G, g_words, gcnt);
@@ -420,28 +539,47 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     k_touched_list<<<(unsigned)((g_words + 255) / 256), 256, 0, st>>>(p.G, g_words, gpre, list);
     count_launches(1);
     uint32_t h[4] = {0, 0, 0, 0};
-    if ((e = cudaMemcpyAsync(h, gpre + g_words, 4, cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
+    unsigned long long h_nq = 0;
+    if ((e = cudaMemcpyAsync(h, gpre + g_words, 4, cudaMemcpyDeviceToHost, st)) ||
+        (e = cudaMemcpyAsync(&h_nq, p.nq, 8, cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
         return fail(e, "touched chunks");
     p.ntouched = h[0];
     const uint64_t nt = p.ntouched;
-    if ((e = cudaMallocFromPoolAsync(&blk2[0], 3 * std::max<uint64_t>(nt, 1) * 4, pool, st)) ||
-        (e = cudaMallocFromPoolAsync(&blk2[1], 3 * (nt + 1) * 4, pool, st)))
-        return fail(e, "scratch");
-    p.cnt = static_cast<uint32_t *>(blk2[0]);
-    uint32_t *pre = static_cast<uint32_t *>(blk2[1]);
-    p.pre = pre;
-    const unsigned blocks = (unsigned)std::max<uint64_t>(
-        1, std::min<uint64_t>((nt + kDedupWarps - 1) / kDedupWarps, (uint64_t)num_sms * 16));
+    if (h_nq > 0xFFFFFFFFull) {
+        release();
+        return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup of more than 2^32 lattice cells");
+    }
+    const uint64_t ntiles = (h_nq + 31) / 32;
+    p.ntiles = ntiles;
+    const size_t sz2[6] = {std::max<uint64_t>(nt, 1) * 4, (nt + 1) * 4, std::max<uint64_t>(h_nq, 1) * 8,
+                           3 * std::max<uint64_t>(ntiles, 1) * 4, 3 * (ntiles + 1) * 4,
+                           scan_scratch_words(std::max<uint64_t>(std::max<uint64_t>(nt, ntiles), 1)) * 8};
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaMallocFromPoolAsync(&blk2[i], sz2[i], pool, st);
+    if (e != cudaSuccess) return fail(e, "scratch");
+    p.qn = static_cast<uint32_t *>(blk2[0]);
+    uint32_t *qpre = static_cast<uint32_t *>(blk2[1]);
+    p.qpre = qpre;
+    p.qs = static_cast<uint64_t *>(blk2[2]);
+    p.tcnt = static_cast<uint32_t *>(blk2[3]);
+    uint32_t *tpre = static_cast<uint32_t *>(blk2[4]);
+    p.tpre = tpre;
+    auto *scan2 = static_cast<unsigned long long *>(blk2[5]);
+    if ((e = cudaMemsetAsync(p.tcnt, 0, sz2[3], st)) != cudaSuccess) return fail(e, "memset");
     if (nt > 0) {
-        k_dedup_keys<false><<<blocks, kDedupWarps * 32, 0, st>>>(p);
+        const unsigned blocks = (unsigned)std::min<uint64_t>((nt + kDedupWarps - 1) / kDedupWarps, (uint64_t)num_sms * 16);
+        k_chunk_bits<<<(unsigned)((nt + 7) / 8), 256, 0, st>>>(p);
+        count_launches(1);
+        if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "chunk bits");
+        if ((e = launch_scan(p.qn, qpre, nt, scan2, status, st)) != cudaSuccess) return fail(e, "scan");
+        k_dedup_state<<<blocks, kDedupWarps * 32, 0, st>>>(p);
         count_launches(1);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "count");
     for (int k = 0; k < 3; ++k)
-        if ((e = launch_scan(p.cnt + k * nt, pre + k * (nt + 1), nt, scan, status, st)) != cudaSuccess)
+        if ((e = launch_scan(p.tcnt + k * ntiles, tpre + k * (ntiles + 1), ntiles, scan2, status, st)) != cudaSuccess)
             return fail(e, "scan");
     for (int k = 0; k < 3; ++k)
-        if ((e = cudaMemcpyAsync(h + k, pre + k * (nt + 1) + nt, 4, cudaMemcpyDeviceToHost, st)))
+        if ((e = cudaMemcpyAsync(h + k, tpre + k * (ntiles + 1) + ntiles, 4, cudaMemcpyDeviceToHost, st)))
             return fail(e, "read totals");
     if ((e = cudaMemcpyAsync(h + 3, status, 4, cudaMemcpyDeviceToHost, st)) || (e = cudaStreamSynchronize(st)))
         return fail(e, "read totals");
@@ -461,8 +599,10 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
         out[k] = p.out[k] = static_cast<uint64_t *>(o);
         n_out[k] = h[k];
     }
-    if (nt > 0) {
-        k_dedup_keys<true><<<blocks, kDedupWarps * 32, 0, st>>>(p);
+    if (ntiles > 0) {
+        const unsigned wblocks =
+            (unsigned)std::min<uint64_t>((ntiles + kDedupWarps - 1) / kDedupWarps, (uint64_t)num_sms * 16);
+        k_dedup_write<<<wblocks, kDedupWarps * 32, 0, st>>>(p, h_nq);
         count_launches(1);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) {
