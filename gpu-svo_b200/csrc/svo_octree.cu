@@ -174,6 +174,7 @@ constexpr int kScanThreads = 256;
 constexpr int kScanItems = 16;
 constexpr uint64_t kScanTile = kScanThreads * kScanItems;
 constexpr int kSpinLimit = 1 << 22;
+constexpr uint64_t kScanSplitTiles = 64;  // from this many tiles on (aligned data): reduce-then-scan
 
 __device__ __forceinline__ unsigned long long ld_relaxed(unsigned long long *p) {
     return cuda::atomic_ref<unsigned long long, cuda::thread_scope_device>(*p).load(
@@ -263,6 +264,120 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restric
     }
     const uint64_t last_tile = (n + kScanTile - 1) / kScanTile - 1;
     if (tile == last_tile && t == kScanThreads - 1) out[n] = s_prefix + aggregate;
+}
+
+// Reduce-then-scan for long, 16-byte aligned arrays: tile sums, one CTA
+// scanning them, then each tile scanned again with its prefix added.  Three
+// streaming passes, no inter-CTA waiting; every thread moves its 16 items
+// with 16-byte loads and stores.
+__device__ __forceinline__ uint32_t block_sum(uint32_t v, uint32_t *s_warp) {
+    v = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31) == 0) s_warp[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t t = 0;
+    for (int w = 0; w < (int)(blockDim.x >> 5); ++w) t += s_warp[w];
+    return t;
+}
+
+__device__ __forceinline__ void load_items(const uint32_t *in, uint64_t base, uint64_t n, uint32_t v[kScanItems]) {
+    if (base + kScanItems <= n) {
+        const uint4 *p = reinterpret_cast<const uint4 *>(in + base);
+#pragma unroll
+        for (int q = 0; q < kScanItems / 4; ++q) {
+            const uint4 x = __ldcs(p + q);
+            v[4 * q] = x.x;
+            v[4 * q + 1] = x.y;
+            v[4 * q + 2] = x.z;
+            v[4 * q + 3] = x.w;
+        }
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k) v[k] = base + k < n ? in[base + k] : 0u;
+    }
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_reduce(const uint32_t *__restrict__ in, uint64_t n,
+                                                              uint32_t *__restrict__ tsum) {
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    uint32_t v[kScanItems];
+    load_items(in, blockIdx.x * kScanTile + (uint64_t)threadIdx.x * kScanItems, n, v);
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) sum += v[k];
+    sum = block_sum(sum, s_warp);
+    if (threadIdx.x == 0) tsum[blockIdx.x] = sum;
+}
+
+// Exclusive prefix of the tile sums (one CTA of 1024 threads) and the grand
+// total at *total.
+__global__ void __launch_bounds__(1024) k_scan_tiles(const uint32_t *__restrict__ tsum, uint32_t *__restrict__ tpre,
+                                                     uint64_t tiles, uint32_t *__restrict__ total) {
+    __shared__ uint32_t s_warp[32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    uint32_t carry = 0;
+    for (uint64_t base = 0; base < tiles; base += 1024) {
+        const uint64_t i = base + t;
+        const uint32_t v = i < tiles ? tsum[i] : 0u;
+        uint32_t incl = v;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+            if (lane >= d) incl += o;
+        }
+        if (lane == 31) s_warp[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            uint32_t w = s_warp[lane];
+#pragma unroll
+            for (int d = 1; d < 32; d <<= 1) {
+                const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, w, d);
+                if (lane >= d) w += o;
+            }
+            s_warp[lane] = w;  // inclusive warp totals
+        }
+        __syncthreads();
+        if (i < tiles) tpre[i] = carry + (warp ? s_warp[warp - 1] : 0u) + incl - v;
+        carry += s_warp[31];
+        __syncthreads();  // s_warp is rewritten by the next round
+    }
+    if (t == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_down(const uint32_t *__restrict__ in, uint32_t *__restrict__ out,
+                                                            uint64_t n, const uint32_t *__restrict__ tpre) {
+    __shared__ uint32_t s_warp[kScanThreads / 32];
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint64_t base = blockIdx.x * kScanTile + (uint64_t)t * kScanItems;
+    uint32_t v[kScanItems];
+    load_items(in, base, n, v);
+    uint32_t sum = 0;
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) sum += v[k];
+    uint32_t incl = sum;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const uint32_t o = __shfl_up_sync(0xFFFFFFFFu, incl, d);
+        if (lane >= d) incl += o;
+    }
+    if (lane == 31) s_warp[warp] = incl;
+    __syncthreads();
+    uint32_t run = tpre[blockIdx.x] + incl - sum;
+    for (int w = 0; w < warp; ++w) run += s_warp[w];
+    uint32_t o[kScanItems];
+#pragma unroll
+    for (int k = 0; k < kScanItems; ++k) {
+        o[k] = run;
+        run += v[k];
+    }
+    if (base + kScanItems <= n) {
+        uint4 *q = reinterpret_cast<uint4 *>(out + base);
+#pragma unroll
+        for (int j = 0; j < kScanItems / 4; ++j) q[j] = make_uint4(o[4 * j], o[4 * j + 1], o[4 * j + 2], o[4 * j + 3]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < kScanItems; ++k)
+            if (base + k < n) out[base + k] = o[k];
+    }
 }
 
 __global__ void k_level_totals(BatchDev bd) {
@@ -785,6 +900,16 @@ size_t scan_scratch_words(uint64_t n) { return 1 + (n + kScanTile - 1) / kScanTi
 cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned long long *scratch,
                         uint32_t *status, cudaStream_t st) {
     const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles >= kScanSplitTiles && tiles <= 0x7FFFFFFFull &&
+        ((reinterpret_cast<uintptr_t>(in) | reinterpret_cast<uintptr_t>(out)) & 15) == 0) {
+        // tile sums and their prefixes live in the look-back scratch (tiles + 1 u64 words)
+        uint32_t *tsum = reinterpret_cast<uint32_t *>(scratch), *tpre = tsum + tiles;
+        k_scan_reduce<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, n, tsum);
+        k_scan_tiles<<<1, 1024, 0, st>>>(tsum, tpre, tiles, out + n);
+        k_scan_down<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, tpre);
+        count_launches(3);
+        return cudaGetLastError();
+    }
     cudaError_t e = cudaMemsetAsync(scratch, 0, scan_scratch_words(n) * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     if (tiles == 0) return cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
