@@ -177,6 +177,7 @@ struct MeshHost {
     bool tris_on_device = false;
     Pyramid py;
     uint64_t bits_off = 0, cnt_off = 0;  // into the batch's bitmap / count buffers
+    uint32_t cta0 = 0;                   // first pyramid CTA (level-0 region) in the batch
     int status = SVO_OK;
     std::string error;
     GridParams gp{};
@@ -231,6 +232,7 @@ struct svo_batch {
     std::vector<void *> allocs;             // phase A buffers (pool)
     uint64_t *bits = nullptr;
     uint32_t *cnt = nullptr, *pre = nullptr;
+    uint8_t *rflag = nullptr;               // level-0 regions that triangles reach (one byte per pyramid CTA)
     unsigned char *meta = nullptr;
     MeshDev *d_mesh = nullptr;
     std::vector<MeshDev> h_mesh;
@@ -381,6 +383,7 @@ int batch_phase_a(svo_batch *b) {
         blocks += mh.py.total_blocks;
         tri_off[k] = tris;
         cta_off[k] = ctas;
+        mh.cta0 = ctas;
         bbox_off[k] = bblocks;
         tris += (uint64_t)mh.n_tris;
         ctas += mh.py.ctas;
@@ -401,6 +404,7 @@ int batch_phase_a(svo_batch *b) {
     uint32_t big_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(2 * tris, 1 << 16), 0x7FFFFFFFu);
     uint4 *big = batch_alloc<uint4>(b, big_cap, err);
     uint64_t *small = big ? batch_alloc<uint64_t>(b, std::max<uint64_t>(tris, 1), err) : nullptr;
+    uint8_t *rflag = b->rflag = batch_alloc<uint8_t>(b, std::max<uint32_t>(ctas, 1), err);
     if (err != cudaSuccess) return cuda_fail(err, "batch scratch");
     GridParams *gp = reinterpret_cast<GridParams *>(b->meta + ml.gp);
     uint32_t *totals = reinterpret_cast<uint32_t *>(b->meta + ml.totals);
@@ -424,12 +428,13 @@ int batch_phase_a(svo_batch *b) {
         d.totals = totals + kMaxLevels * k;
         d.done = done + k;
         d.py = mh.py;
+        d.regions = mh.py.words[0] >= kRegionWords ? 1 : 0;
     }
     SVO_TRY(upload(b->d_mesh, b->h_mesh, st), "upload meshes");
     SVO_TRY(upload(d_tri_off, tri_off, st), "upload");
     SVO_TRY(upload(d_cta_off, cta_off, st), "upload");
     SVO_TRY(upload(d_bbox_off, bbox_off, st), "upload");
-    const BatchDev bd{b->d_mesh, n, d_tri_off, d_cta_off, d_bbox_off};
+    const BatchDev bd{b->d_mesh, n, d_tri_off, d_cta_off, d_bbox_off, rflag};
     const bool strict = (b->flags & SVO_FLAG_STRICT_FP) != 0;
     StageTimer tm((b->flags & SVO_FLAG_TIMINGS) != 0);
     for (int attempt = 0; attempt < 2; ++attempt) {
@@ -439,13 +444,14 @@ int batch_phase_a(svo_batch *b) {
         count_launches(1);
         SVO_TRY(launch_bbox(bd, bblocks, st), "bbox");
         tm.mark(StageTimer::kBbox, st);
-        SVO_TRY(cudaMemsetAsync(b->bits, 0, words * 8, st), "memset bitmaps");
+        SVO_TRY(cudaMemsetAsync(rflag, 0, std::max<uint32_t>(ctas, 1), st), "memset regions");
         SVO_TRY(cudaMemsetAsync(b->cnt, 0, blocks * 4, st), "memset counts");
+        SVO_TRY(launch_regions(bd, (int64_t)tris, ctas, ctx->num_sms, st), "zero bitmaps");
         SVO_TRY(launch_voxelize(bd, (int64_t)tris, strict, ctx->tune, big, big_cap, counters, ctx->num_sms, st,
                                 small),
                 "voxelize");
         tm.mark(StageTimer::kVox, st);
-        SVO_TRY(launch_pyramid(bd, ctas, st), "pyramid");
+        SVO_TRY(launch_pyramid(bd, ctas, ctx->num_sms, st), "pyramid");
         tm.mark(StageTimer::kPyr, st);
         SVO_TRY(launch_scan(b->cnt, b->pre, blocks, scan, counters + 2, st), "scan");
         SVO_TRY(launch_level_totals(bd, st), "totals");
@@ -704,6 +710,7 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 k0.out = r->keys;
                 k0.wpre = nullptr;
                 std::memset(k0.koff, 0, sizeof(k0.koff));
+                k0.rflag = mh.py.words[0] >= kRegionWords ? b->rflag + mh.cta0 : nullptr;
                 jobs.push_back(k0);
                 word_off.push_back(word_off.back() + mh.py.words[0]);
             }

@@ -49,7 +49,7 @@ struct MeshDev {
     int64_t n_pts;
     int64_t n_tris;
     int res[3];
-    int pad_;
+    int regions;             // 1: level 0 is zeroed and read only in the regions triangles reach
     GridParams *gp;
     uint32_t *mm;            // bbox scratch (6 u32)
     uint64_t *bits;          // this mesh's pyramid (level l at bits + py.woff[l])
@@ -67,7 +67,12 @@ struct BatchDev {
     const uint64_t *tri_off;   // global index of each mesh's first triangle
     const uint32_t *cta_off;   // first pyramid CTA of each mesh
     const uint32_t *bbox_off;  // first bbox-reduction block of each mesh
+    uint8_t *rflag = nullptr;  // per pyramid CTA (a 2048-word region of level 0): a triangle reaches it
 };
+
+// Level-0 regions (2048 words: 64 x 64 x 32 voxels) are tracked from this
+// level-0 size on (resolution >= 1024).
+constexpr uint64_t kRegionWords = 1ull << 24;
 
 // Per-level inputs of the node emission kernel.
 struct EmitLevel {
@@ -115,6 +120,7 @@ struct CompactJob {
     uint64_t *out;
     uint32_t *wpre;  // optional: rank at each non-empty word of levels >= 1 (indexed from woff[1])
     uint64_t koff[kMaxLevels];
+    const uint8_t *rflag;  // region-mode mesh: its level-0 region flags (unflagged regions read as empty)
 };
 struct CompactBatch {
     const CompactJob *job;
@@ -166,7 +172,12 @@ cudaError_t launch_voxelize(const BatchDev &b, int64_t total_tris, bool strict, 
                             uint4 *big, uint32_t big_cap, uint32_t *counters, int num_sms, cudaStream_t st,
                             uint64_t *small = nullptr);
 // Builds levels 1.. of every mesh's pyramid and the per-block counts.
-cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, cudaStream_t st);
+cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, int num_sms, cudaStream_t st);
+// Flags the level-0 regions that triangles of region-mode meshes reach, then
+// zeroes level 0 where needed (every region of other meshes, the flagged ones
+// of region-mode meshes) and each mesh's levels >= 3.  Replaces a memset of
+// the whole pyramid; rflag must be zeroed (total_ctas bytes).
+cudaError_t launch_regions(const BatchDev &b, int64_t total_tris, uint32_t total_ctas, int num_sms, cudaStream_t st);
 // Exclusive scan of n u32 values; out has n + 1 entries (out[n] = total).
 // scratch: >= scan_scratch_words(n) u64 words, zeroed by the call.
 size_t scan_scratch_words(uint64_t n);

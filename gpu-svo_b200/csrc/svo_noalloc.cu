@@ -176,7 +176,7 @@ extern "C" int svo_voxelize_keys_noalloc(const float *points, int64_t n_points, 
     if ((rc = cuda(launch_voxelize(bd, nt, (flags & SVO_FLAG_STRICT_FP) != 0, tune, nullptr, 0, counters,
                                    prop.multiProcessorCount, st))))
         return rc;
-    if ((rc = cuda(launch_pyramid(bd, py.ctas, st)))) return rc;
+    if ((rc = cuda(launch_pyramid(bd, py.ctas, prop.multiProcessorCount, st)))) return rc;
     if ((rc = cuda(launch_scan(cnt, pre, py.total_blocks, scan, &gp->status, st)))) return rc;
     if ((rc = cuda(launch_level_totals(bd, st)))) return rc;
     uint32_t h_tot = 0, h_status = 0;

@@ -65,74 +65,87 @@ __device__ __forceinline__ uint32_t nz_bytes(uint64_t v) {
     return (uint32_t)((m * 0x0102040810204080ull) >> 56);
 }
 
-// Levels 1..4 of one 2048-word chunk of level 0 per CTA (one 512-bit block
-// of level 0 per thread, 16-byte streaming loads).  No fence or completion
-// counter, so a CTA retires as soon as its stores are issued; the levels
-// above 4 come from k_pyramid_top.
-__global__ void __launch_bounds__(256, 8) k_pyramid(BatchDev bd) {
+// Levels 1..4 of 2048-word chunks of level 0 (regions), a persistent grid
+// taking them in turn (one 512-bit block of level 0 per thread, 16-byte
+// streaming loads); the levels above 4 come from k_pyramid_top.  A
+// region-mode mesh's region that no triangle reaches is empty and is not read
+// (its level-0 words are not zeroed in memory): its words of levels 1..4 are
+// written as zeros and its counts stay at their memset zero.
+__global__ void __launch_bounds__(256, 8) k_pyramid(BatchDev bd, uint32_t total) {
     __shared__ uint64_t s1[256];
     __shared__ uint64_t s2[32];
     __shared__ uint64_t s3[4];
-    const int m = find_segment(bd.cta_off, bd.n, (uint32_t)blockIdx.x);
-    const MeshDev &md = bd.mesh[m];
-    const Pyramid &py = md.py;
-    uint64_t *__restrict__ bits = md.bits;
-    uint32_t *__restrict__ cnt = md.cnt;
-    const uint32_t b = blockIdx.x - bd.cta_off[m], t = threadIdx.x;
-    {
-        const uint4 *src = reinterpret_cast<const uint4 *>(bits + py.woff[0] + (uint64_t)b * 2048 + t * 8);
-        uint64_t w1 = 0;
-        uint32_t c0 = 0;
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint4 v = __ldcs(src + q);
-            const uint64_t a = ((uint64_t)v.y << 32) | v.x, c = ((uint64_t)v.w << 32) | v.z;
-            c0 += __popcll(a) + __popcll(c);
-            w1 |= (uint64_t)nz_bytes(a) << (16 * q);
-            w1 |= (uint64_t)nz_bytes(c) << (16 * q + 8);
+    const uint32_t t = threadIdx.x;
+    for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+        const int m = find_segment(bd.cta_off, bd.n, g);
+        const MeshDev &md = bd.mesh[m];
+        const Pyramid &py = md.py;
+        uint64_t *__restrict__ bits = md.bits;
+        uint32_t *__restrict__ cnt = md.cnt;
+        const uint32_t b = g - bd.cta_off[m];
+        if (md.regions && !bd.rflag[g]) {  // the same for the whole CTA
+            bits[py.woff[1] + (uint64_t)b * 256 + t] = 0;
+            if (t < 32) bits[py.woff[2] + (uint64_t)b * 32 + t] = 0;
+            if (t < 4) bits[py.woff[3] + (uint64_t)b * 4 + t] = 0;
+            if (t == 0) reinterpret_cast<uint32_t *>(bits + py.woff[4])[b] = 0;
+            continue;
         }
-        cnt[py.coff[0] + (uint64_t)b * 256 + t] = c0;
-        bits[py.woff[1] + (uint64_t)b * 256 + t] = w1;
-        s1[t] = w1;
-    }
-    __syncthreads();
-    if (t < 32) {
-        uint64_t w = 0;
-        uint32_t c = 0;
+        {
+            const uint4 *src = reinterpret_cast<const uint4 *>(bits + py.woff[0] + (uint64_t)b * 2048 + t * 8);
+            uint64_t w1 = 0;
+            uint32_t c0 = 0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint64_t v = s1[8 * t + k];
-            c += __popcll(v);
-            w |= (uint64_t)nz_bytes(v) << (8 * k);
+            for (int q = 0; q < 4; ++q) {
+                const uint4 v = __ldcs(src + q);
+                const uint64_t a = ((uint64_t)v.y << 32) | v.x, c = ((uint64_t)v.w << 32) | v.z;
+                c0 += __popcll(a) + __popcll(c);
+                w1 |= (uint64_t)nz_bytes(a) << (16 * q);
+                w1 |= (uint64_t)nz_bytes(c) << (16 * q + 8);
+            }
+            cnt[py.coff[0] + (uint64_t)b * 256 + t] = c0;
+            bits[py.woff[1] + (uint64_t)b * 256 + t] = w1;
+            s1[t] = w1;
         }
-        cnt[py.coff[1] + (uint64_t)b * 32 + t] = c;
-        bits[py.woff[2] + (uint64_t)b * 32 + t] = w;
-        s2[t] = w;
-    }
-    __syncthreads();
-    if (t < 4) {
-        uint64_t w = 0;
-        uint32_t c = 0;
+        __syncthreads();
+        if (t < 32) {
+            uint64_t w = 0;
+            uint32_t c = 0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint64_t v = s2[8 * t + k];
-            c += __popcll(v);
-            w |= (uint64_t)nz_bytes(v) << (8 * k);
+            for (int k = 0; k < 8; ++k) {
+                const uint64_t v = s1[8 * t + k];
+                c += __popcll(v);
+                w |= (uint64_t)nz_bytes(v) << (8 * k);
+            }
+            cnt[py.coff[1] + (uint64_t)b * 32 + t] = c;
+            bits[py.woff[2] + (uint64_t)b * 32 + t] = w;
+            s2[t] = w;
         }
-        cnt[py.coff[2] + (uint64_t)b * 4 + t] = c;
-        bits[py.woff[3] + (uint64_t)b * 4 + t] = w;
-        s3[t] = w;
-    }
-    __syncthreads();
-    if (t == 0) {
-        uint32_t w = 0, c = 0;
+        __syncthreads();
+        if (t < 4) {
+            uint64_t w = 0;
+            uint32_t c = 0;
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            c += __popcll(s3[k]);
-            w |= nz_bytes(s3[k]) << (8 * k);
+            for (int k = 0; k < 8; ++k) {
+                const uint64_t v = s2[8 * t + k];
+                c += __popcll(v);
+                w |= (uint64_t)nz_bytes(v) << (8 * k);
+            }
+            cnt[py.coff[2] + (uint64_t)b * 4 + t] = c;
+            bits[py.woff[3] + (uint64_t)b * 4 + t] = w;
+            s3[t] = w;
         }
-        atomicAdd(cnt + py.coff[3] + b / 2, c);
-        reinterpret_cast<uint32_t *>(bits + py.woff[4])[b] = w;
+        __syncthreads();
+        if (t == 0) {
+            uint32_t w = 0, c = 0;
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                c += __popcll(s3[k]);
+                w |= nz_bytes(s3[k]) << (8 * k);
+            }
+            if (c) atomicAdd(cnt + py.coff[3] + b / 2, c);
+            reinterpret_cast<uint32_t *>(bits + py.woff[4])[b] = w;
+        }
+        __syncthreads();  // s1..s3 are rewritten by the next region
     }
 }
 
@@ -410,7 +423,7 @@ __global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total
         l = job.l0;
         while (l + 1 < job.l1 && gw >= py.woff[l + 1]) ++l;
         w = gw - py.woff[l];
-        v = job.bits[gw];
+        v = (l == 0 && job.rflag && !job.rflag[w >> 11]) ? 0ull : job.bits[gw];
         if (v) r = job.pre[py.coff[l] + (w >> 3)] - job.pre[py.coff[l]];
     }
     const uint32_t pc = __popcll(v);
@@ -887,9 +900,9 @@ cudaError_t unique_impl(const T *in, uint64_t n, T *out, uint32_t *tile_counts, 
 
 }  // namespace
 
-cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, cudaStream_t st) {
+cudaError_t launch_pyramid(const BatchDev &b, uint32_t total_ctas, int num_sms, cudaStream_t st) {
     if (total_ctas == 0) return cudaSuccess;
-    k_pyramid<<<total_ctas, 256, 0, st>>>(b);
+    k_pyramid<<<std::min<uint32_t>(total_ctas, (uint32_t)num_sms * 8), 256, 0, st>>>(b, total_ctas);
     k_pyramid_top<<<b.n, 256, 0, st>>>(b);
     count_launches(2);
     return cudaGetLastError();

@@ -146,6 +146,20 @@ struct Tri {
 __device__ __forceinline__ int f2i_rz(float f) { return __float2int_rz(f); }
 __device__ __forceinline__ int clampi(int f, int a, int b) { return max(a, min(f, b)); }
 
+// Voxel bbox of a triangle (vertices relative to the grid origin), clamped
+// to the grid: src/SVO.cu:58-66.  The region marker and the voxel test use
+// this one function, so the regions cover every voxel the test can set.
+__device__ __forceinline__ void tri_box(const GridParams &g, const int res[3], const float v[3][3], int lo[3],
+                                        int hi[3]) {
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const float mn = cminf(v[0][a], cminf(v[1][a], v[2][a]));
+        const float mx = cmaxf(v[0][a], cmaxf(v[1][a], v[2][a]));
+        lo[a] = clampi(f2i_rz(__fdiv_rn(mn, g.unit[a])), 0, res[a] - 1);
+        hi[a] = clampi(f2i_rz(__fdiv_rn(mx, g.unit[a])), 0, res[a] - 1);
+    }
+}
+
 template <bool S>
 __device__ __forceinline__ void tri_setup(const GridParams &g, const int res[3], const float *p0,
                                           const float *p1, const float *p2, Tri &t) {
@@ -178,13 +192,7 @@ __device__ __forceinline__ void tri_setup(const GridParams &g, const int res[3],
     t.n[1] = c1;
     t.n[2] = c2;
     const float *u = g.unit;
-#pragma unroll
-    for (int a = 0; a < 3; ++a) {
-        const float mn = cminf(v[0][a], cminf(v[1][a], v[2][a]));
-        const float mx = cmaxf(v[0][a], cmaxf(v[1][a], v[2][a]));
-        t.lo[a] = clampi(f2i_rz(__fdiv_rn(mn, u[a])), 0, res[a] - 1);
-        t.hi[a] = clampi(f2i_rz(__fdiv_rn(mx, u[a])), 0, res[a] - 1);
-    }
+    tri_box(g, res, v, t.lo, t.hi);
     float ca[3], cb[3];
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
@@ -849,6 +857,80 @@ cudaError_t launch_bbox(const BatchDev &b, uint32_t total_blocks, cudaStream_t s
     k_bbox_reduce<<<total_blocks, 256, 0, st>>>(b);
     k_grid_setup<<<(b.n + 127) / 128, 128, 0, st>>>(b);
     count_launches(2);
+    return cudaGetLastError();
+}
+
+namespace {
+
+// Flags the level-0 regions (Morton code >> 17: x >> 6, y >> 6, z >> 5) that
+// each triangle's voxel bbox overlaps, for region-mode meshes.  The bbox is
+// tri_box's widened by one voxel on each side, with a product by the
+// reciprocal voxel size in place of the division: the two differ by a few
+// ulps at coordinates <= 2048, far less than the margin, so the flagged
+// regions cover every voxel the voxel test can set.
+__global__ void __launch_bounds__(256) k_region_mark(BatchDev bd, int64_t total) {
+    for (int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gid < total;
+         gid += (int64_t)gridDim.x * blockDim.x) {
+        const int m = find_segment(bd.tri_off, bd.n, (uint64_t)gid);
+        const MeshDev &md = bd.mesh[m];
+        if (!md.regions) continue;
+        const GridParams g = *md.gp;
+        float p[3][3];
+        load_tri(md.pts, md.tris, gid - (int64_t)bd.tri_off[m], p);
+        int lo[3], hi[3];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const float v0 = __fsub_rn(p[0][a], g.origin[a]), v1 = __fsub_rn(p[1][a], g.origin[a]),
+                        v2 = __fsub_rn(p[2][a], g.origin[a]);
+            const float inv = __frcp_rn(g.unit[a]);
+            // the margin is applied before the conversion, so +-inf and NaN clamp as in tri_box
+            lo[a] = clampi(f2i_rz(__fsub_rn(__fmul_rn(cminf(v0, cminf(v1, v2)), inv), 1.0f)), 0, md.res[a] - 1);
+            hi[a] = clampi(f2i_rz(__fadd_rn(__fmul_rn(cmaxf(v0, cmaxf(v1, v2)), inv), 1.0f)), 0, md.res[a] - 1);
+        }
+        uint8_t *flag = bd.rflag + bd.cta_off[m];
+        for (uint32_t rz = (uint32_t)lo[2] >> 5; rz <= (uint32_t)hi[2] >> 5; ++rz)
+            for (uint32_t ry = (uint32_t)lo[1] >> 6; ry <= (uint32_t)hi[1] >> 6; ++ry)
+                for (uint32_t rx = (uint32_t)lo[0] >> 6; rx <= (uint32_t)hi[0] >> 6; ++rx) {
+                    uint8_t *f = flag + (morton3(rx << 6, ry << 6, rz << 5) >> 17);
+                    if (!*f) *f = 1;
+                }
+    }
+}
+
+// Level-0 regions, a persistent grid taking them in turn: zeroes each unless
+// it is a region-mode mesh's unflagged region.  The pyramid writes every word of levels 1 and 2 and the
+// first 4 * ctas of level 3; the words after those (level-3 padding, level 4,
+// which the pyramid writes as 32-bit halves, and levels >= 5) are zeroed
+// here, spread over the mesh's CTAs.
+__global__ void __launch_bounds__(256) k_region_zero(BatchDev bd, uint32_t total) {
+    for (uint32_t g = blockIdx.x; g < total; g += gridDim.x) {
+        const int m = find_segment(bd.cta_off, bd.n, g);
+        const MeshDev &md = bd.mesh[m];
+        const uint32_t r = g - bd.cta_off[m];
+        if (!md.regions || bd.rflag[g]) {
+            uint4 *w = reinterpret_cast<uint4 *>(md.bits + md.py.woff[0] + (uint64_t)r * 2048);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) w[threadIdx.x + 256 * q] = make_uint4(0, 0, 0, 0);
+        }
+        const uint64_t z0 = md.py.woff[3] + 4ull * md.py.ctas;
+        for (uint64_t i = z0 + (uint64_t)r * 256 + threadIdx.x; i < md.py.total_words; i += (uint64_t)md.py.ctas * 256)
+            md.bits[i] = 0;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_regions(const BatchDev &b, int64_t total_tris, uint32_t total_ctas, int num_sms,
+                           cudaStream_t st) {
+    if (total_tris > 0) {
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((total_tris + 255) / 256, (int64_t)num_sms * 8));
+        k_region_mark<<<blocks, 256, 0, st>>>(b, total_tris);
+        count_launches(1);
+    }
+    if (total_ctas > 0) {
+        k_region_zero<<<std::min<uint32_t>(total_ctas, (uint32_t)num_sms * 8), 256, 0, st>>>(b, total_ctas);
+        count_launches(1);
+    }
     return cudaGetLastError();
 }
 
