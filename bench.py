@@ -60,6 +60,8 @@ def parse_args():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--tune", type=int, default=1, help="single-mesh workloads: autotune the voxelizer split first")
+    ap.add_argument("--tuning", default="", help="single-mesh workloads: use this split instead "
+                    "(serial_max,warp_max,split,inplace_max,serial_packed)")
     return ap.parse_args()
 
 
@@ -335,7 +337,11 @@ def run_ours(args, rank: int, world: int):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.int32, device="cuda")
     # voxelizer work split for this mesh (svo_ctx_autotune, before any timing;
     # results do not depend on it)
-    tuning = ctx.autotune([(d_pts, d_tris, res)], bflags, sid) if args.tune else ctx.tuning
+    if args.tuning:
+        ctx.tuning = tuple(int(x) for x in args.tuning.split(","))
+        tuning = ctx.tuning
+    else:
+        tuning = ctx.autotune([(d_pts, d_tris, res)], bflags, sid) if args.tune else ctx.tuning
 
     def step(flags=0):
         flush.fill_(1)  # L2 flush before each step, outside the timed span
