@@ -445,6 +445,21 @@ __global__ void k_chunk_bits(const __grid_constant__ DedupParams p) {
     if (lane == 0) p.qn[w] = n;
 }
 
+// Zeroes the 2048-word regions of D that can hold a candidate: every lattice
+// cell Q has coordinates <= side / 2 (corners of the grid's cells), and a
+// region -- an aligned box of 64 x 64 x 32 Q -- holds one iff its lowest
+// corner does.  At side 2048 that is 9,537 of 65,536 regions; only the
+// touched chunks of D are read later, all inside these.
+__global__ void __launch_bounds__(256) k_dedup_zero(uint64_t *__restrict__ D, uint64_t regions, uint32_t half) {
+    for (uint64_t b = blockIdx.x; b < regions; b += gridDim.x) {
+        const uint64_t c = b << 17;
+        if (compact3(c) > half || compact3(c >> 1) > half || compact3(c >> 2) > half) continue;
+        uint4 *w = reinterpret_cast<uint4 *>(D + b * 2048);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) w[threadIdx.x + 256 * q] = make_uint4(0, 0, 0, 0);
+    }
+}
+
 // The touched chunks in order: per-word popcounts of G, then (after a scan)
 // the chunk index of every set bit.
 __global__ void k_touched_count(const uint32_t *__restrict__ G, uint64_t n, uint32_t *__restrict__ cnt) {
@@ -528,8 +543,16 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     auto *scan = static_cast<unsigned long long *>(blk[5]);
     uint32_t *status = static_cast<uint32_t *>(blk[6]);
     p.nq = reinterpret_cast<unsigned long long *>(static_cast<char *>(blk[6]) + 8);
-    if ((e = cudaMemsetAsync(p.D, 0, sz[0], st)) != cudaSuccess || (e = cudaMemsetAsync(p.G, 0, sz[1], st)) ||
-        (e = cudaMemsetAsync(status, 0, 16, st)))
+    if (d_words % 2048 == 0) {
+        const uint64_t regions = d_words / 2048;
+        k_dedup_zero<<<(unsigned)std::min<uint64_t>(regions, (uint64_t)num_sms * 8), 256, 0, st>>>(
+            reinterpret_cast<uint64_t *>(p.D), regions, (uint32_t)(side / 2));
+        count_launches(1);
+        e = cudaGetLastError();
+    } else {
+        e = cudaMemsetAsync(p.D, 0, sz[0], st);
+    }
+    if (e != cudaSuccess || (e = cudaMemsetAsync(p.G, 0, sz[1], st)) || (e = cudaMemsetAsync(status, 0, 16, st)))
         return fail(e, "memset");
     k_dedup_mark<<<(mark_total + 255) / 256, 256, 0, st>>>(p, mark_total);
     k_touched_count<<<(unsigned)((g_words + 255) / 256), 256, 0, st>>>(p.G, g_words, gcnt);
