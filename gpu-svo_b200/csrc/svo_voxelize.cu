@@ -368,23 +368,6 @@ __device__ __forceinline__ bool brick_reject(const Tri &t, const GridParams &g, 
     return false;
 }
 
-// The 64 voxels of brick (sx, sy, sz) of triangle t (the same in every
-// lane): 2 voxels per lane, one ballot and one atomicOr per bitmap word.
-template <bool S>
-__device__ __forceinline__ void brick_voxels(const Tri &t, const GridParams &g, uint32_t *__restrict__ bm, int sx,
-                                             int sy, int sz, int lane) {
-#pragma unroll
-    for (int h = 0; h < 2; ++h) {
-        const int lm = lane + 32 * h;  // local Morton index in the brick
-        const int x = 4 * sx + ((lm & 1) | ((lm >> 2) & 2));
-        const int y = 4 * sy + (((lm >> 1) & 1) | ((lm >> 3) & 2));
-        const int z = 4 * sz + (((lm >> 2) & 1) | ((lm >> 4) & 2));
-        const bool in = x >= t.lo[0] && x <= t.hi[0] && y >= t.lo[1] && y <= t.hi[1] && z >= t.lo[2] && z <= t.hi[2];
-        const uint32_t w = __ballot_sync(0xFFFFFFFFu, in && voxel_pass<S>(t, g, x, y, z));
-        if (lane == h && w) atomicOr(bm + ((morton3((uint32_t)sx, (uint32_t)sy, (uint32_t)sz) << 1) | h), w);
-    }
-}
-
 // Two bricks per round, one per half-warp: lane r = lane & 15 of a half
 // tests the 4 voxels of row (y, z) = (r & 3, r >> 2) of its half's brick,
 // hoisted like the serial tier (row_prep: the YZ edge tests reject whole
