@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <new>
 #include <string>
 #include <thread>
 #include <vector>
@@ -139,64 +140,119 @@ void svo_free_host(void *p) { std::free(p); }
 // on the whole file: lines up to 254 characters are taken, an unterminated
 // last line hits end-of-file and is dropped, and a longer line (on which the
 // reference loops forever) is an error.  Each line then goes through the same
-// sscanf patterns.
+// sscanf patterns.  Large files are cut at line starts into chunks parsed by
+// separate threads and joined in file order; face indices are absolute, so
+// the result does not depend on the cut.
 int svo_load_obj(const char *path, float **points, int64_t *n_points, int32_t **tris, int64_t *n_tris) {
     if (!path || !points || !n_points || !tris || !n_tris) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
     FILE *f = std::fopen(path, "rb");
     if (!f) return fail(SVO_ERR_IO, std::string("cannot open ") + path);
     std::string data;
     {
+        // one read into a buffer of the file's size (then any remainder, for
+        // files whose size is not known up front)
+        long len = -1;
+        if (std::fseek(f, 0, SEEK_END) == 0) len = std::ftell(f);
+        std::rewind(f);
+        if (len > 0) {
+            data.resize((size_t)len);
+            data.resize(std::fread(&data[0], 1, (size_t)len, f));
+        }
         char buf[1 << 16];
         size_t k;
         while ((k = std::fread(buf, 1, sizeof(buf), f)) > 0) data.append(buf, k);
         std::fclose(f);
     }
-    std::vector<float> P;
-    std::vector<int32_t> T;
-    size_t pos = 0;
     const size_t size = data.size();
-    char line[256];
-    while (pos < size) {
-        const void *nl = std::memchr(data.data() + pos, '\n', size - pos);
-        const size_t end = nl ? (size_t)((const char *)nl - data.data()) : size;
-        const size_t len = end - pos;
-        if (len >= 255) return fail(SVO_ERR_PARSE, "line longer than 254 characters");
-        if (!nl) break;  // unterminated last line: getline sets eofbit first
-        std::memcpy(line, data.data() + pos, len);
-        line[len] = '\0';
-        pos = end + 1;
-        float x, y, z;
-        int f0, f0_, f1, f1_, f2, f2_;
-        if (line[0] == 'v' && line[1] == ' ') {
-            if (std::sscanf(line, "v %f %f %f", &x, &y, &z) == 3) {
-                P.push_back(x);
-                P.push_back(y);
-                P.push_back(z);
-            }
-        } else if (line[0] == 'f' && line[1] == ' ') {
-            if (std::sscanf(line, "f %d//%d %d//%d %d//%d", &f0, &f0_, &f1, &f1_, &f2, &f2_) == 6 ||
-                std::sscanf(line, "f %d/%d %d/%d %d/%d", &f0, &f0_, &f1, &f1_, &f2, &f2_) == 6 ||
-                std::sscanf(line, "f %d %d %d", &f0, &f1, &f2) == 3) {
-                T.push_back(f0 - 1);
-                T.push_back(f1 - 1);
-                T.push_back(f2 - 1);
-            }
-        }
+    constexpr size_t kMinChunk = 256 << 10;
+    const size_t hw = std::max(1u, std::thread::hardware_concurrency());
+    const size_t nc = std::max<size_t>(1, std::min(hw, size / kMinChunk));
+    // chunk c holds the lines that start in [start[c], start[c + 1])
+    std::vector<size_t> start(nc + 1, size);
+    start[0] = 0;
+    for (size_t c = 1; c < nc; ++c) {
+        const size_t at = c * (size / nc) - 1;
+        const void *nl = std::memchr(data.data() + at, '\n', size - at);
+        start[c] = std::max(start[c - 1], nl ? (size_t)((const char *)nl - data.data()) + 1 : size);
     }
-    const int64_t np = (int64_t)P.size() / 3;
-    for (int32_t v : T)
-        if (v < 0 || v >= np) return fail(SVO_ERR_PARSE, "face index out of range");
-    *points = (float *)std::malloc(std::max<size_t>(1, P.size()) * sizeof(float));
-    *tris = (int32_t *)std::malloc(std::max<size_t>(1, T.size()) * sizeof(int32_t));
+    std::vector<std::vector<float>> P(nc);
+    std::vector<std::vector<int32_t>> T(nc);
+    std::vector<int> err(nc, SVO_OK);
+    auto parse = [&](size_t c) {
+        try {
+            char line[256];
+            size_t pos = start[c];
+            while (pos < start[c + 1]) {
+                const void *nl = std::memchr(data.data() + pos, '\n', size - pos);
+                const size_t end = nl ? (size_t)((const char *)nl - data.data()) : size;
+                const size_t len = end - pos;
+                if (len >= 255) {
+                    err[c] = SVO_ERR_PARSE;
+                    return;
+                }
+                if (!nl) break;  // unterminated last line: getline sets eofbit first
+                std::memcpy(line, data.data() + pos, len);
+                line[len] = '\0';
+                pos = end + 1;
+                float x, y, z;
+                int f0, f0_, f1, f1_, f2, f2_;
+                if (line[0] == 'v' && line[1] == ' ') {
+                    if (std::sscanf(line, "v %f %f %f", &x, &y, &z) == 3) {
+                        P[c].push_back(x);
+                        P[c].push_back(y);
+                        P[c].push_back(z);
+                    }
+                } else if (line[0] == 'f' && line[1] == ' ') {
+                    if (std::sscanf(line, "f %d//%d %d//%d %d//%d", &f0, &f0_, &f1, &f1_, &f2, &f2_) == 6 ||
+                        std::sscanf(line, "f %d/%d %d/%d %d/%d", &f0, &f0_, &f1, &f1_, &f2, &f2_) == 6 ||
+                        std::sscanf(line, "f %d %d %d", &f0, &f1, &f2) == 3) {
+                        T[c].push_back(f0 - 1);
+                        T[c].push_back(f1 - 1);
+                        T[c].push_back(f2 - 1);
+                    }
+                }
+            }
+        } catch (const std::bad_alloc &) {
+            err[c] = SVO_ERR_OUT_OF_MEMORY;
+        }
+    };
+    if (nc == 1) {
+        parse(0);
+    } else {
+        std::vector<std::thread> th;
+        th.reserve(nc);
+        for (size_t c = 0; c < nc; ++c) th.emplace_back(parse, c);
+        for (auto &t : th) t.join();
+    }
+    for (size_t c = 0; c < nc; ++c) {
+        if (err[c] == SVO_ERR_PARSE) return fail(SVO_ERR_PARSE, "line longer than 254 characters");
+        if (err[c] != SVO_OK) return fail(err[c], "out of host memory");
+    }
+    size_t np3 = 0, nt3 = 0;
+    for (size_t c = 0; c < nc; ++c) {
+        np3 += P[c].size();
+        nt3 += T[c].size();
+    }
+    const int64_t np = (int64_t)np3 / 3;
+    for (size_t c = 0; c < nc; ++c)
+        for (int32_t v : T[c])
+            if (v < 0 || v >= np) return fail(SVO_ERR_PARSE, "face index out of range");
+    *points = (float *)std::malloc(std::max<size_t>(1, np3) * sizeof(float));
+    *tris = (int32_t *)std::malloc(std::max<size_t>(1, nt3) * sizeof(int32_t));
     if (!*points || !*tris) {
         std::free(*points);
         std::free(*tris);
         return fail(SVO_ERR_OUT_OF_MEMORY, "malloc failed");
     }
-    std::memcpy(*points, P.data(), P.size() * sizeof(float));
-    std::memcpy(*tris, T.data(), T.size() * sizeof(int32_t));
+    size_t po = 0, to = 0;
+    for (size_t c = 0; c < nc; ++c) {
+        if (!P[c].empty()) std::memcpy(*points + po, P[c].data(), P[c].size() * sizeof(float));
+        if (!T[c].empty()) std::memcpy(*tris + to, T[c].data(), T[c].size() * sizeof(int32_t));
+        po += P[c].size();
+        to += T[c].size();
+    }
     *n_points = np;
-    *n_tris = (int64_t)T.size() / 3;
+    *n_tris = (int64_t)nt3 / 3;
     return SVO_OK;
 }
 

@@ -83,3 +83,60 @@ def test_bunny(bunny_path, oracle_mod, svo_mod):
     p1, t1 = svo_mod.load_obj(bunny_path)
     assert p0.shape == (14290, 3) and t0.shape == (28576, 3)
     assert p0.tobytes() == p1.tobytes() and np.array_equal(t0, t1)
+
+
+def _big_obj(seed, n_v, n_f):
+    """A multi-megabyte OBJ mixing every line form the loader meets (so the
+    product loader cuts it into chunks parsed in parallel)."""
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=(n_v, 3)).astype(np.float32)
+    f = rng.integers(1, n_v + 1, size=(n_f, 3))
+    out = ["# generated\n"]
+    vi = fi = 0
+    while vi < n_v or fi < n_f:
+        r = rng.integers(0, 12)
+        if vi < n_v and (r < 5 or fi >= n_f):
+            x, y, z = (float(c) for c in v[vi])
+            sep = " " if r else "   "
+            out.append(f"v{sep}{x!r}{sep}{y:.9g} {z:.3e}\n" if r % 2 else f"v {x} {y} {z}\r\n")
+            vi += 1
+        elif fi < n_f and vi >= max(f[fi]):  # faces only after their vertices (any order is valid)
+            a, b, c = f[fi]
+            form = rng.integers(0, 4)
+            out.append([f"f {a} {b} {c}\n", f"f {a}//{a} {b}//{b} {c}//{c}\n", f"f {a}/1 {b}/2 {c}/3\n",
+                        f"f {a}/1/1 {b}/2/2 {c}/3/3\n"][form])
+            fi += 1
+        elif r < 8:
+            out.append(["vn 0 0 1\n", "vt 0.5 0.5\n", "\n", "# " + "x" * 200 + "\n"][r - 5 if r < 8 else 0])
+        elif vi < n_v:
+            x, y, z = (float(c) for c in v[vi])
+            out.append(f"v {x} {y} {z}\n")
+            vi += 1
+        else:
+            a, b, c = f[fi]
+            out.append(f"f {a} {b} {c}\n")
+            fi += 1
+    return "".join(out)
+
+
+def test_big_file_matches_oracle(tmp_path, oracle_mod, svo_mod):
+    text = _big_obj(11, 60000, 120000)
+    assert len(text) > 4 << 20
+    for name, t in (("big.obj", text), ("big_unterminated.obj", text + "v 1 2 3")):
+        path = _write(tmp_path, name, t)
+        p0, t0 = oracle_mod.load_obj(path)
+        p1, t1 = svo_mod.load_obj(path)
+        assert p0.shape[0] == 60000 and t0.shape[0] > 80000
+        assert p0.tobytes() == p1.tobytes() and np.array_equal(t0, t1)
+
+
+def test_big_file_errors(tmp_path, oracle_mod, svo_mod):
+    text = _big_obj(12, 40000, 80000)
+    mid = text.index("\n", len(text) * 2 // 3) + 1
+    for bad, code in (("v " + "1 " * 130 + "\n", 7), ("f 1 2 999999\n", 7)):
+        path = _write(tmp_path, "bad_big.obj", text[:mid] + bad + text[mid:])
+        with pytest.raises(oracle_mod.OracleError) as e0:
+            oracle_mod.load_obj(path)
+        with pytest.raises(svo_mod.SvoError) as e1:
+            svo_mod.load_obj(path)
+        assert e0.value.code == code and e1.value.code == code
