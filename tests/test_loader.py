@@ -140,3 +140,43 @@ def test_big_file_errors(tmp_path, oracle_mod, svo_mod):
         with pytest.raises(svo_mod.SvoError) as e1:
             svo_mod.load_obj(path)
         assert e0.value.code == code and e1.value.code == code
+
+
+@pytest.mark.parametrize("mb", [0.25, 0.5, 1.0, 2.0, 3.3])
+def test_chunk_cuts(tmp_path, oracle_mod, svo_mod, mb):
+    """Files around the loader's 256 KB chunk size, made of maximal (254
+    character) vertex lines, CRLF lines and faces in every form, so that the
+    cut points fall inside lines of each kind."""
+    target = int(mb * (1 << 20))
+    out, nv, size = [], 0, 0
+    k = 0
+    while size < target:
+        r = k % 5
+        if r == 0:
+            line = "v 1 2 3" + " " * 246 + "\n"       # 254 characters + newline
+            nv += 1
+        elif r == 1:
+            line = f"v {k * 0.5} {-k} 1e-3\r\n"
+            nv += 1
+        elif r == 2 and nv >= 3:
+            line = f"f {nv} {nv - 1} {nv - 2}\n"
+        elif r == 3 and nv >= 3:
+            line = f"f {nv}//1 {nv - 1}//2 {nv - 2}//3\n"
+        else:
+            line = f"f {nv}/4 {max(1, nv - 2)}/5 {max(1, nv - 1)}/6\n" if nv >= 3 else "# start\n"
+        out.append(line)
+        size += len(line)
+        k += 1
+    path = _write(tmp_path, "cuts.obj", "".join(out))
+    p0, t0 = oracle_mod.load_obj(path)
+    p1, t1 = svo_mod.load_obj(path)
+    assert p0.tobytes() == p1.tobytes() and np.array_equal(t0, t1)
+    assert t0.shape[0] > 0
+
+
+def test_empty_and_blank_files(tmp_path, oracle_mod, svo_mod):
+    for name, text in (("empty.obj", ""), ("blank.obj", "\n" * 300000), ("comments.obj", "# x\n" * 100000)):
+        path = _write(tmp_path, name, text)
+        p0, t0 = oracle_mod.load_obj(path)
+        p1, t1 = svo_mod.load_obj(path)
+        assert p0.shape == p1.shape == (0, 3) and t0.shape == t1.shape == (0, 3)
