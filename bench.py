@@ -3,11 +3,14 @@
 (voxelize -> octree levels -> node records + vertex/edge arrays, bit-exact
 with the reference's semantics) of a seeded synthetic mesh.
 
-Default workload: 1,000,000-triangle torus + sliver soup at resolution 512
-(svo_b200.meshgen.torus_slivers).  `value` is whole-job triangles/s with the
+Default workload: the 4,999,122-triangle heightfield at resolution 2048
+(depth 11) with full neighbour tables and vertex/edge/face dedup
+(svo_b200.meshgen.heightfield).  `value` is whole-job triangles/s with the
 mesh already resident in HBM; `e2e` is the same metric through the C ABI with
 pinned host buffers (host->device copy of the mesh and device->host copy of
-the whole octree -- nodes, vertices, edges, keys -- inside the timed region).
+the whole octree -- nodes, vertices, edges, keys, dedup lists -- inside the
+timed region).  `--workload torus_slivers` is the 1M-triangle soup at
+resolution 512.
 
   python bench.py [--gpus N --steps K --warmup W] [--impl ours|reference]
 
@@ -41,6 +44,9 @@ L2_FLUSH_BYTES = 256 << 20
 # 8 vertices x 16 B, 12 edges x 28 B written; one 8-byte group code read per
 # 8 sibling nodes.
 EMIT_BYTES_PER_NODE = 168 + 8 * 16 + 12 * 28 + 1
+# Every stride-th triangle of a single-mesh workload is the bounded sample the
+# CPU legs (the oracle) build, with the workload's own flags.
+CPU_STRIDE = {"torus_slivers": 16, "heightfield": 128, "icosphere_l5": 1}
 TUNING_KEYS = ("serial_max", "warp_max", "split", "inplace_max", "serial_packed")
 
 
@@ -50,8 +56,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["torus_slivers", "icosphere_l5", "heightfield", "batch256", "serve"],
-                    default="torus_slivers")
+    ap.add_argument("--workload", choices=["heightfield", "torus_slivers", "icosphere_l5", "batch256", "serve"],
+                    default="heightfield")
     ap.add_argument("--rates", default="200,500,1000,2000,5000", help="serve: Poisson arrival rates (req/s)")
     ap.add_argument("--window", type=float, default=1.0, help="serve: seconds of arrivals per rate")
     ap.add_argument("--flags", type=int, default=-1, help="override the workload's build flags (SVO_FLAG_*)")
@@ -263,6 +269,15 @@ def time_cpu_build(pts, tris, res, threads: int, flags: int = 0) -> float:
     return dt
 
 
+def cpu_sample_text(stride: int, wname: str, nt: int, res: int, flags: int) -> str:
+    import svo_b200 as S
+
+    extra = [n for b, n in ((S.FLAG_FULL_NEIGHBORS, "full neighbour tables"), (S.FLAG_DEDUP, "dedup lists"))
+             if flags & b]
+    return (f"every {stride}th triangle of {wname} ({nt} triangles), res {res}, full build (voxels, levels, "
+            f"nodes, vertex/edge arrays{''.join(', ' + e for e in extra)})")
+
+
 def batch_cpu_sample(meshes, stride: int = 32):
     """Every stride-th mesh of the batch, resolutions capped at 256 (a bounded sample)."""
     return [(p, t, min(r, 256)) for p, t, r in meshes[::stride]]
@@ -287,15 +302,14 @@ def run_reference(args, rank: int):
     else:
         pts, tris, res, wname, wflags = workload(args.workload)
         flags = wflags if args.flags < 0 else args.flags
-        stride = {"torus_slivers": 16, "heightfield": 8}.get(args.workload, 1)
+        stride = CPU_STRIDE[args.workload]
         spts, stris = cpu_sample(pts, tris, stride)
         nt = stris.shape[0]
 
         def one():
             return time_cpu_build(spts, stris, res, threads, flags)
 
-        sample = (f"every {stride}th triangle of {wname} ({nt} triangles), res {res}, full build "
-                  f"(voxels, levels, nodes, vertex/edge arrays)")
+        sample = cpu_sample_text(stride, wname, nt, res, flags)
     for _ in range(args.warmup):
         one()
     times = [one() for _ in range(args.steps)]
@@ -393,16 +407,31 @@ def run_ours(args, rank: int, world: int):
     achieved = emit_bytes / (emit_ms / 1e3) / 1e9 if emit_ms > 0 else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "emit_traffic_per_node.json")
+    tsrc = None
     if os.path.exists(tpath):
-        traffic = json.load(open(tpath))["dram_bytes_per_node"] * info["nodes"]
+        # DRAM bytes per node of the k_emit variant this build runs, from an
+        # ncu capture of a smaller case, scaled by this build's node count
+        ent = json.load(open(tpath)).get("full_neighbors" if bflags & S.FLAG_FULL_NEIGHBORS else "default")
+        if ent:
+            traffic = ent["dram_bytes_per_node"] * info["nodes"]
+            tsrc = f"ncu: {ent['dram_bytes_per_node']} DRAM B/node of k_emit on {ent['case']}, x this build's nodes"
+    # whole-build algorithmic bytes: soup read 36 B per triangle, 8 B per
+    # surface-voxel key, the node records and vertex/edge arrays as written,
+    # 8 B per dedup key
+    build_bytes = (36 * nt + 8 * info["keys"] + 168 * info["nodes"] + 16 * info["vertices"]
+                   + 28 * info["edges"] + 8 * sum(info.get("dedup_keys", [])))
+    build_ms = dist_max(sum(step_ms)) / args.steps
+    build_gbs = build_bytes / (build_ms / 1e3) / 1e9
     roofline = {
         "kernel": "k_emit (node records + vertex/edge arrays)",
         "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-        "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+        "frac": (achieved / peak) if achieved else None, "traffic": traffic, "traffic_source": tsrc,
         "peak_source": "measured" if peaks else "fallback",
         "algorithmic_bytes": emit_bytes, "launch_ms": emit_ms,
         "stage_ms": stage,
-        "build_bytes_alg": 36 * nt + 8 * info["keys"] + EMIT_BYTES_PER_NODE * info["nodes"],
+        "build_bytes_alg": build_bytes, "build_gbs": build_gbs, "build_frac": build_gbs / peak,
+        "build_note": "whole build: algorithmic bytes (36 B/triangle + 8 B/key + 168 B/node + 16 B/vertex + "
+                      "28 B/edge + 8 B/dedup key) / ms_per_step, of measured copy bandwidth",
     }
 
     # end to end through the C ABI with pinned host buffers
@@ -443,12 +472,12 @@ def run_ours(args, rank: int, world: int):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        stride = 16 if args.workload == "torus_slivers" else 1
+        stride = CPU_STRIDE[args.workload]
         spts, stris = cpu_sample(pts, tris, stride)
         threads = os.cpu_count() or 1
-        dt = time_cpu_build(spts, stris, res, threads)
+        dt = min(time_cpu_build(spts, stris, res, threads, bflags) for _ in range(2))
         cpu = {"value": stris.shape[0] / dt, "unit": "tris/s", "cores": threads, "kind": "port",
-               "sample": f"every {stride}th triangle ({stris.shape[0]}), res {res}, one full oracle build"}
+               "sample": cpu_sample_text(stride, wname, stris.shape[0], res, bflags) + "; best of 2 oracle builds"}
 
     if rank == 0:
         line = {

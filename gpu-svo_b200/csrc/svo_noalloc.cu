@@ -35,6 +35,7 @@ constexpr int kMaxDevices = 64;
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 unsigned char *g_scratch_addr[kMaxDevices] = {};
+int g_num_sms[kMaxDevices] = {};
 std::mutex g_scratch_mu;
 
 int noalloc_fail(int code, const char *msg) {
@@ -42,16 +43,22 @@ int noalloc_fail(int code, const char *msg) {
     return code;
 }
 
-// Device address of the scratch array on the current device (looked up once).
-cudaError_t scratch_address(int device, unsigned char **out) {
+// Device address of the scratch array on the current device and the device's
+// SM count (looked up once per device, with that device current).
+cudaError_t scratch_address(int device, unsigned char **out, int *num_sms) {
     std::lock_guard<std::mutex> lock(g_scratch_mu);
     if (!g_scratch_addr[device]) {
-        void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        int sms = 0;
+        cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
         if (e != cudaSuccess) return e;
+        void *p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_num_sms[device] = sms;
         g_scratch_addr[device] = static_cast<unsigned char *>(p);
     }
     *out = g_scratch_addr[device];
+    *num_sms = g_num_sms[device];
     return cudaSuccess;
 }
 
@@ -104,11 +111,9 @@ extern "C" int svo_voxelize_keys_noalloc(const float *points, int64_t n_points, 
     cudaError_t e = cudaGetDevice(&device);
     if (e != cudaSuccess || device < 0 || device >= kMaxDevices)
         return noalloc_fail(SVO_ERR_CUDA, "cudaGetDevice failed");
-    cudaDeviceProp prop;
-    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess)
-        return noalloc_fail(SVO_ERR_CUDA, "cudaGetDeviceProperties failed");
     unsigned char *base = nullptr;
-    if ((e = scratch_address(device, &base)) != cudaSuccess)
+    int num_sms = 0;
+    if ((e = scratch_address(device, &base, &num_sms)) != cudaSuccess)
         return noalloc_fail(SVO_ERR_CUDA, cudaGetErrorString(e));
 
     const Pyramid py = make_pyramid(res_x, res_y, res_z);
@@ -174,9 +179,9 @@ extern "C" int svo_voxelize_keys_noalloc(const float *points, int64_t n_points, 
     VoxTuning tune;
     tune.warp_max = 0xFFFFFFFFu;  // no big-triangle queue: warps take every large triangle
     if ((rc = cuda(launch_voxelize(bd, nt, (flags & SVO_FLAG_STRICT_FP) != 0, tune, nullptr, 0, counters,
-                                   prop.multiProcessorCount, st))))
+                                   num_sms, st))))
         return rc;
-    if ((rc = cuda(launch_pyramid(bd, py.ctas, prop.multiProcessorCount, st)))) return rc;
+    if ((rc = cuda(launch_pyramid(bd, py.ctas, num_sms, st)))) return rc;
     if ((rc = cuda(launch_scan(cnt, pre, py.total_blocks, scan, &gp->status, st)))) return rc;
     if ((rc = cuda(launch_level_totals(bd, st)))) return rc;
     uint32_t h_tot = 0, h_status = 0;

@@ -98,10 +98,10 @@ def _check(rc: int) -> None:
 
 
 def _copy(ptr: int, n: int, dtype) -> np.ndarray:
-    if n == 0:
-        return np.zeros(0, dtype=dtype)
-    buf = (C.c_char * (n * np.dtype(dtype).itemsize)).from_address(ptr)
-    return np.frombuffer(bytes(buf), dtype=dtype).copy()
+    out = np.empty(n, dtype=dtype)
+    if n:
+        C.memmove(out.ctypes.data, ptr, out.nbytes)
+    return out
 
 
 def load_obj(path: str):
@@ -181,7 +181,8 @@ def voxelize(points, tris, res, flags: int = 0, threads: int = 0) -> np.ndarray:
 
 
 class Result:
-    """Outputs of the oracle's create(), copied into numpy arrays."""
+    """Outputs of the oracle's create(); each array is copied into numpy on
+    first access (the handle keeps the oracle's own copy until close())."""
 
     def __init__(self, handle):
         L = lib()
@@ -189,16 +190,42 @@ class Result:
         lc = np.zeros(64, dtype=np.int64)
         n = L.oracle_result_level_counts(handle, lc.ctypes.data, 64)
         self.level_counts = lc[:n].copy()
-        self.nodes = _copy(L.oracle_result_nodes(handle), L.oracle_result_num_nodes(handle), NODE_DTYPE)
-        self.vertices = _copy(L.oracle_result_vertices(handle), L.oracle_result_num_vertices(handle), VERTEX_DTYPE)
-        self.edges = _copy(L.oracle_result_edges(handle), L.oracle_result_num_edges(handle), EDGE_DTYPE)
-        self.keys = _copy(L.oracle_result_keys(handle), L.oracle_result_num_keys(handle), np.uint64)
         self.bbox = _copy(L.oracle_result_bbox(handle), 9, np.float32)
-        self.dedup = [
-            _copy(L.oracle_result_dedup(handle, k), max(0, L.oracle_result_num_dedup(handle, k)), np.uint64)
-            for k in range(3)
-        ]
         self._handle = handle
+        self._cache = {}
+
+    def _get(self, name, fetch):
+        if name not in self._cache:
+            if not self._handle:
+                raise OracleError(-1, "result already closed")
+            self._cache[name] = fetch(lib(), self._handle)
+        return self._cache[name]
+
+    @property
+    def nodes(self) -> np.ndarray:
+        return self._get("nodes", lambda L, h: _copy(L.oracle_result_nodes(h), L.oracle_result_num_nodes(h),
+                                                      NODE_DTYPE))
+
+    @property
+    def vertices(self) -> np.ndarray:
+        return self._get("vertices", lambda L, h: _copy(L.oracle_result_vertices(h),
+                                                         L.oracle_result_num_vertices(h), VERTEX_DTYPE))
+
+    @property
+    def edges(self) -> np.ndarray:
+        return self._get("edges", lambda L, h: _copy(L.oracle_result_edges(h), L.oracle_result_num_edges(h),
+                                                      EDGE_DTYPE))
+
+    @property
+    def keys(self) -> np.ndarray:
+        return self._get("keys", lambda L, h: _copy(L.oracle_result_keys(h), L.oracle_result_num_keys(h),
+                                                     np.uint64))
+
+    @property
+    def dedup(self) -> list:
+        return self._get("dedup", lambda L, h: [
+            _copy(L.oracle_result_dedup(h, k), max(0, L.oracle_result_num_dedup(h, k)), np.uint64)
+            for k in range(3)])
 
     def write_tree(self, path: str) -> None:
         _check(lib().oracle_write_tree(self._handle, path.encode()))

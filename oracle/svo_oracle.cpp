@@ -21,6 +21,7 @@
 #include <new>
 #include <string>
 #include <thread>
+#include <utility>
 #include <vector>
 
 namespace {
@@ -33,6 +34,29 @@ int fail(int code, const std::string &msg) {
 }
 
 constexpr uint32_t kNone = 0xFFFFFFFFu;  // UINT_MAX, the reference's "no index"
+
+// Allocator whose resize() leaves trivial elements uninitialised, so that large
+// output arrays are first touched by the threads that fill them.
+template <class T>
+struct NoInit : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = NoInit<U>;
+    };
+    NoInit() = default;
+    template <class U>
+    NoInit(const NoInit<U> &) {}
+    template <class U>
+    void construct(U *p) noexcept {
+        ::new ((void *)p) U;
+    }
+    template <class U, class... A>
+    void construct(U *p, A &&...a) {
+        ::new ((void *)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using big_vector = std::vector<T, NoInit<T>>;
 
 // body(begin, end) over [0, n) in chunks of `chunk`, handed out dynamically to
 // `nth` std::threads.
@@ -410,11 +434,11 @@ struct oracle_result {
     float bbox[9];
     std::vector<int64_t> level_counts;  // depthNumNodes + the top level
     std::vector<oracle_node> nodes;
-    std::vector<oracle_vertex> verts;
-    std::vector<oracle_edge> edges;
+    big_vector<oracle_vertex> verts;
+    big_vector<oracle_edge> edges;
     std::vector<uint64_t> keys;
     std::vector<uint64_t> codes;  // full-width Morton code per node
-    std::vector<uint64_t> dedup[3];
+    big_vector<uint64_t> dedup[3];
 };
 
 namespace {
@@ -646,57 +670,139 @@ inline uint32_t owner_of(const oracle_node &nd, const short *slots, int ns, uint
 
 inline bool veq(const float *a, const float *b) { return a[0] == b[0] && a[1] == b[1] && a[2] == b[2]; }
 
+// Vertex i of node t (src/SVO.cu:596-605): the corner offset without the origin.
+inline void make_vertex(const oracle_node &nd, uint32_t t, int i, bool min_owner, oracle_vertex &v) {
+    const float w = nd.width;
+    v.pos[0] = w * (float)(i & 1);
+    v.pos[1] = w * (float)((i >> 1) & 1);
+    v.pos[2] = w * (float)((i >> 2) & 1);
+    v.owner = owner_of(nd, kShared.vert[i], 8, t, min_owner);
+}
+
+// Edge e of node t (src/SVO.cu:638-674): origin plus 0 or width per component.
+inline void make_edge(const oracle_node &nd, uint32_t t, int e, bool min_owner, oracle_edge &ed) {
+    const float *o = nd.origin;
+    const float w = nd.width;
+    for (int s = 0; s < 2; ++s) {
+        const int c = kEdgeCorners[e][s];
+        float *dst = s ? ed.p1 : ed.p0;
+        if (c == 0) {  // `origin` itself, no add
+            dst[0] = o[0];
+            dst[1] = o[1];
+            dst[2] = o[2];
+        } else {
+            dst[0] = o[0] + ((c & 1) ? w : 0.0f);
+            dst[1] = o[1] + ((c & 2) ? w : 0.0f);
+            dst[2] = o[2] + ((c & 4) ? w : 0.0f);
+        }
+    }
+    ed.owner = owner_of(nd, kShared.edge[e], 4, t, min_owner);
+}
+
+inline bool same_edge(const oracle_edge &a, const oracle_edge &b) {  // uniqueEdge, src/SVO.cu:686-693
+    return (veq(a.p0, b.p0) && veq(a.p1, b.p1)) || (veq(a.p0, b.p1) && veq(a.p1, b.p0));
+}
+
+// The 8N vertices and 12N edges in node order, then thrust::unique's
+// consecutive-duplicate removal (src/SVO.cu:710-725): element k is kept unless
+// it equals element k - 1.  Element k - 1 is recomputed from its node, so the
+// work splits into independent node ranges: one pass counts what each range
+// keeps, a second writes it at the range's offset.
 void vert_edge(oracle_result &r, bool min_owner, int nth) {
     const auto &nodes = r.nodes;
-    const size_t N = nodes.size();
-    std::vector<oracle_vertex> V(N * 8);
-    std::vector<oracle_edge> E(N * 12);
-    parallel_for((int64_t)N, 4096, nth, [&](int64_t tb, int64_t te) {
-    for (int64_t t = tb; t < te; ++t) {
-        const oracle_node &nd = nodes[(size_t)t];
-        const float w = nd.width;
-        for (int i = 0; i < 8; ++i) {
-            oracle_vertex &v = V[(size_t)t * 8 + i];
-            v.pos[0] = w * (float)(i & 1);
-            v.pos[1] = w * (float)((i >> 1) & 1);
-            v.pos[2] = w * (float)((i >> 2) & 1);
-            v.owner = owner_of(nd, kShared.vert[i], 8, (uint32_t)t, min_owner);
-        }
-        const float *o = nd.origin;
-        for (int e = 0; e < 12; ++e) {
-            oracle_edge &ed = E[(size_t)t * 12 + e];
-            for (int s = 0; s < 2; ++s) {
-                const int c = kEdgeCorners[e][s];
-                float *dst = s ? ed.p1 : ed.p0;
-                if (c == 0) {  // `origin` itself, no add
-                    dst[0] = o[0];
-                    dst[1] = o[1];
-                    dst[2] = o[2];
-                } else {
-                    dst[0] = o[0] + ((c & 1) ? w : 0.0f);
-                    dst[1] = o[1] + ((c & 2) ? w : 0.0f);
-                    dst[2] = o[2] + ((c & 4) ? w : 0.0f);
-                }
+    const int64_t N = (int64_t)nodes.size();
+    constexpr int64_t kChunk = 1 << 14;
+    const int64_t nchunks = (N + kChunk - 1) / kChunk;
+    std::vector<int64_t> vcount(nchunks + 1, 0), ecount(nchunks + 1, 0);
+    auto vert_at = [&](int64_t k, oracle_vertex &v) {
+        make_vertex(nodes[(size_t)(k >> 3)], (uint32_t)(k >> 3), (int)(k & 7), min_owner, v);
+    };
+    auto edge_at = [&](int64_t k, oracle_edge &e) {
+        make_edge(nodes[(size_t)(k / 12)], (uint32_t)(k / 12), (int)(k % 12), min_owner, e);
+    };
+    // pass(c, write): walks chunk c's elements, counting (write = false) or
+    // storing (write = true) the kept ones.
+    auto pass = [&](int64_t c, bool write) {
+        const int64_t tb = c * kChunk, te = std::min(N, tb + kChunk);
+        int64_t nv = write ? vcount[c] : 0, ne = write ? ecount[c] : 0;
+        oracle_vertex pv{}, cv{};
+        if (tb > 0) vert_at(8 * tb - 1, pv);
+        for (int64_t k = 8 * tb; k < 8 * te; ++k) {
+            vert_at(k, cv);
+            if (k == 0 || !veq(pv.pos, cv.pos)) {
+                if (write) r.verts[(size_t)nv] = cv;
+                ++nv;
             }
-            ed.owner = owner_of(nd, kShared.edge[e], 4, (uint32_t)t, min_owner);
+            pv = cv;
         }
-    }
+        oracle_edge pe{}, ce{};
+        if (tb > 0) edge_at(12 * tb - 1, pe);
+        for (int64_t k = 12 * tb; k < 12 * te; ++k) {
+            edge_at(k, ce);
+            if (k == 0 || !same_edge(pe, ce)) {
+                if (write) r.edges[(size_t)ne] = ce;
+                ++ne;
+            }
+            pe = ce;
+        }
+        if (!write) {
+            vcount[c + 1] = nv;
+            ecount[c + 1] = ne;
+        }
+    };
+    parallel_for(nchunks, 1, nth, [&](int64_t cb, int64_t ce) {
+        for (int64_t c = cb; c < ce; ++c) pass(c, false);
     });
-    // thrust::unique: keep element i unless it equals element i-1
-    r.verts.clear();
-    r.verts.reserve(V.size());
-    for (size_t i = 0; i < V.size(); ++i)
-        if (i == 0 || !veq(V[i - 1].pos, V[i].pos)) r.verts.push_back(V[i]);
-    r.edges.clear();
-    r.edges.reserve(E.size());
-    for (size_t i = 0; i < E.size(); ++i) {
-        if (i > 0) {
-            const oracle_edge &a = E[i - 1], &b = E[i];
-            bool same = (veq(a.p0, b.p0) && veq(a.p1, b.p1)) || (veq(a.p0, b.p1) && veq(a.p1, b.p0));
-            if (same) continue;
-        }
-        r.edges.push_back(E[i]);
+    for (int64_t c = 0; c < nchunks; ++c) {
+        vcount[c + 1] += vcount[c];
+        ecount[c + 1] += ecount[c];
     }
+    r.verts.resize((size_t)vcount[nchunks]);
+    r.edges.resize((size_t)ecount[nchunks]);
+    parallel_for(nchunks, 1, nth, [&](int64_t cb, int64_t ce) {
+        for (int64_t c = cb; c < ce; ++c) pass(c, true);
+    });
+}
+
+// Sorts v and drops repeats (std::sort + std::unique), with the work split
+// over `nth` threads: contiguous slices are sorted and uniqued on their own,
+// then merged pairwise (uniqued again after each merge).
+void sort_unique(big_vector<uint64_t> &v, int nth) {
+    const size_t n = v.size();
+    size_t parts = 1;
+    while ((int)parts < nth && parts < 64 && n / (parts * 2) >= (1u << 16)) parts *= 2;
+    std::vector<size_t> lo(parts), hi(parts);
+    for (size_t p = 0; p < parts; ++p) {
+        lo[p] = n * p / parts;
+        hi[p] = n * (p + 1) / parts;
+    }
+    auto each = [&](size_t count, auto fn) {
+        std::vector<std::thread> pool;
+        for (size_t p = 1; p < count; ++p) pool.emplace_back(fn, p);
+        fn(0);
+        for (auto &t : pool) t.join();
+    };
+    each(parts, [&](size_t p) {
+        std::sort(v.begin() + lo[p], v.begin() + hi[p]);
+        hi[p] = (size_t)(std::unique(v.begin() + lo[p], v.begin() + hi[p]) - v.begin());
+    });
+    big_vector<uint64_t> tmp(n);
+    for (size_t width = 1; width < parts; width *= 2) {
+        // merge slice p with slice p + width into tmp at lo[p], then back
+        const size_t pairs = (parts + 2 * width - 1) / (2 * width);
+        each(pairs, [&](size_t q) {
+            const size_t p = q * 2 * width, o = p + width;
+            size_t end = lo[p];
+            if (o < parts) {
+                end = (size_t)(std::merge(v.begin() + lo[p], v.begin() + hi[p], v.begin() + lo[o],
+                                          v.begin() + hi[o], tmp.begin() + lo[p]) - tmp.begin());
+                end = (size_t)(std::unique(tmp.begin() + lo[p], tmp.begin() + end) - tmp.begin());
+                std::copy(tmp.begin() + lo[p], tmp.begin() + end, v.begin() + lo[p]);
+                hi[p] = end;
+            }
+        });
+    }
+    v.resize(hi[0]);
 }
 
 // Morton-keyed dedup of the nodes' vertices, edges and faces (no reference
@@ -705,39 +811,43 @@ void vert_edge(oracle_result &r, bool min_owner, int nth) {
 //   vertex key = morton(X, Y, Z)
 //   edge key   = morton(min corner) << 6 | (d-1) << 2 | axis
 //   face key   = morton(min corner) << 6 | (d-1) << 2 | normal axis
-void dedup(oracle_result &r) {
+void dedup(oracle_result &r, int nth) {
     std::vector<int64_t> off(1, 0);
     for (int64_t c : r.level_counts) off.push_back(off.back() + c);
-    for (auto &v : r.dedup) v.clear();
+    const int64_t N = off.back();
+    r.dedup[0].resize((size_t)N * 8);
+    r.dedup[1].resize((size_t)N * 12);
+    r.dedup[2].resize((size_t)N * 6);
     for (int lvl = 0; lvl < r.depth; ++lvl) {
         const uint32_t s = 1u << lvl;
-        for (int64_t t = off[lvl]; t < off[lvl + 1]; ++t) {
+        parallel_for(off[lvl + 1] - off[lvl], 1 << 14, nth, [&](int64_t tb, int64_t te) {
+        for (int64_t t = off[lvl] + tb; t < off[lvl] + te; ++t) {
             uint32_t x, y, z;
             demorton(r.codes[(size_t)t], x, y, z);
             uint32_t c[3] = {x << lvl, y << lvl, z << lvl};
+            uint64_t *vk = &r.dedup[0][(size_t)t * 8];
+            uint64_t *ek = &r.dedup[1][(size_t)t * 12];
+            uint64_t *fk = &r.dedup[2][(size_t)t * 6];
             for (int i = 0; i < 8; ++i)
-                r.dedup[0].push_back(morton(c[0] + ((i & 1) ? s : 0), c[1] + ((i & 2) ? s : 0),
-                                            c[2] + ((i & 4) ? s : 0)));
+                vk[i] = morton(c[0] + ((i & 1) ? s : 0), c[1] + ((i & 2) ? s : 0), c[2] + ((i & 4) ? s : 0));
             for (int a = 0; a < 3; ++a) {
                 const int b1 = (a + 1) % 3, b2 = (a + 2) % 3;
                 for (int k = 0; k < 4; ++k) {
                     uint32_t q[3] = {c[0], c[1], c[2]};
                     if (k & 1) q[b1] += s;
                     if (k & 2) q[b2] += s;
-                    r.dedup[1].push_back((morton(q[0], q[1], q[2]) << 6) | ((uint64_t)lvl << 2) | a);
+                    ek[4 * a + k] = (morton(q[0], q[1], q[2]) << 6) | ((uint64_t)lvl << 2) | a;
                 }
                 for (int k = 0; k < 2; ++k) {
                     uint32_t q[3] = {c[0], c[1], c[2]};
                     if (k) q[a] += s;
-                    r.dedup[2].push_back((morton(q[0], q[1], q[2]) << 6) | ((uint64_t)lvl << 2) | a);
+                    fk[2 * a + k] = (morton(q[0], q[1], q[2]) << 6) | ((uint64_t)lvl << 2) | a;
                 }
             }
         }
+        });
     }
-    for (auto &v : r.dedup) {
-        std::sort(v.begin(), v.end());
-        v.erase(std::unique(v.begin(), v.end()), v.end());
-    }
+    for (auto &v : r.dedup) sort_unique(v, nth);
 }
 
 }  // namespace
@@ -942,7 +1052,7 @@ int oracle_build(const float *points, int64_t n_points, const int32_t *tris, int
     }
     neighbors(*r, full);
     if (!(flags & ORACLE_FLAG_NO_VERT_EDGE)) vert_edge(*r, full, nth);
-    if (flags & ORACLE_FLAG_DEDUP) dedup(*r);
+    if (flags & ORACLE_FLAG_DEDUP) dedup(*r, nth);
     *out = r;
     return ORACLE_OK;
 }

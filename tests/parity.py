@@ -4,16 +4,24 @@ import numpy as np
 FIELDS = ["morton_code", "is_leaf", "origin", "width", "parent", "childs", "neighbors"]
 
 
-def first_diff(a: np.ndarray, b: np.ndarray, what: str) -> str:
+def first_diff(a: np.ndarray, b: np.ndarray, what: str, chunk: int = 1 << 22) -> str:
+    """'' if a and b are byte-identical, else a description of the first
+    differing record.  Compares `chunk` records at a time (multi-GB arrays)."""
     if a.shape != b.shape:
         return f"{what}: shape {a.shape} vs {b.shape}"
-    ab = a.view(np.uint8).reshape(a.shape[0], -1) if a.ndim == 1 else a
-    bb = b.view(np.uint8).reshape(b.shape[0], -1) if b.ndim == 1 else b
-    bad = np.nonzero((ab != bb).reshape(ab.shape[0], -1).any(1))[0]
-    if bad.size == 0:
+    n = a.shape[0] if a.ndim else 1
+    nbad, i = 0, -1
+    for s in range(0, n, chunk):
+        ab = a[s:s + chunk].view(np.uint8).reshape(-1, a.itemsize)
+        bb = b[s:s + chunk].view(np.uint8).reshape(-1, b.itemsize)
+        bad = np.nonzero((ab != bb).any(1))[0]
+        if bad.size:
+            nbad += bad.size
+            if i < 0:
+                i = s + int(bad[0])
+    if i < 0:
         return ""
-    i = int(bad[0])
-    msg = f"{what}: {bad.size} records differ, first at {i}"
+    msg = f"{what}: {nbad} records differ, first at {i}"
     if a.dtype.names:
         for f in a.dtype.names:
             if not np.array_equal(a[f][i], b[f][i]):

@@ -59,8 +59,9 @@ def test_no_samples():
 def test_args(monkeypatch):
     monkeypatch.setattr(sys, "argv", ["bench.py"])
     a = bench.parse_args()
-    assert (a.gpus, a.steps, a.warmup, a.impl, a.workload, a.tune, a.tuning) == (1, 10, 3, "ours", "torus_slivers", 1, "")
-    monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "heightfield", "--tuning", "128,256,0,64,0"])
+    assert (a.gpus, a.steps, a.warmup, a.impl, a.workload, a.tune, a.tuning) == (1, 10, 3, "ours", "heightfield", 1, "")
+    assert bench.CPU_STRIDE[a.workload] > 1  # the CPU legs build a bounded sample of the 5M-triangle mesh
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--workload", "torus_slivers", "--tuning", "128,256,0,64,0"])
     a = bench.parse_args()
     assert tuple(int(x) for x in a.tuning.split(",")) == (128, 256, 0, 64, 0)
     assert a.warmup >= 3

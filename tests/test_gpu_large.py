@@ -43,6 +43,49 @@ def test_heightfield_subsample_res2048(gpu_ctx, oracle_mod, svo_mod):
     assert_same(g, o, check_ve=False)
 
 
+def _assert_dedup(g, o):
+    for k in range(3):
+        d = g.dedup(k)
+        assert d.shape == o.dedup[k].shape, (k, d.shape, o.dedup[k].shape)
+        assert np.array_equal(d, o.dedup[k]), k
+
+
+def test_heightfield_subsample_res2048_full_dedup(gpu_ctx, oracle_mod, svo_mod):
+    """The heightfield workload's own flags -- full 27-neighbour tables and the
+    vertex/edge/face dedup lists -- at resolution 2048 (64-bit Morton codes) on
+    every 7th triangle: node records with all neighbours, the vertex/edge
+    arrays (owner = smallest sharing node), the voxel keys and the three dedup
+    lists, element for element against the oracle."""
+    v, f, res = _heightfield_sample(7)
+    g = gpu_ctx.build(v, f, res, svo_mod.FLAG_FULL_NEIGHBORS | svo_mod.FLAG_DEDUP)
+    o = oracle_mod.build_svo(v, f, res, flags=oracle_mod.FLAG_FULL_NEIGHBORS | oracle_mod.FLAG_DEDUP)
+    assert o.depth == 12 and (o.keys >= 1 << 32).any()
+    # neighbour tables are really populated (not just the root's self entry):
+    # every node below the root sees itself and its 7 siblings
+    nb = o.nodes["neighbors"][:-1]
+    assert (nb[:, 13] != NONE).all() and (nb != NONE).sum(1).min() >= 8
+    assert_same(g, o)
+    _assert_dedup(g, o)
+
+
+@pytest.mark.parametrize("mode", ["full", "dedup"])
+def test_icosphere_res1024(gpu_ctx, oracle_mod, svo_mod, mode):
+    """The icosphere (config 1's mesh) at resolution 1024, the largest grid of
+    32-bit Morton codes, with full neighbour tables or with dedup lists, in
+    full against the oracle."""
+    from svo_b200 import meshgen
+
+    v, f, _ = meshgen.icosphere_l5()
+    gf = svo_mod.FLAG_FULL_NEIGHBORS if mode == "full" else svo_mod.FLAG_DEDUP
+    of = oracle_mod.FLAG_FULL_NEIGHBORS if mode == "full" else oracle_mod.FLAG_DEDUP
+    g = gpu_ctx.build(v, f, 1024, gf)
+    o = oracle_mod.build_svo(v, f, 1024, flags=of)
+    assert o.depth == 11
+    assert_same(g, o)
+    if mode == "dedup":
+        _assert_dedup(g, o)
+
+
 def test_heightfield_full_properties(gpu_ctx, svo_mod):
     from svo_b200 import meshgen
 

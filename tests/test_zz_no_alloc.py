@@ -50,6 +50,35 @@ def test_noalloc_matches_build_two_calls(gpu_ctx, svo_mod, oracle_mod, bunny_pat
         assert got.shape == want.shape and np.array_equal(got, want)
 
 
+def _axis_mesh():
+    """Large axis-aligned triangles across the unit cube (planes normal to each
+    axis) plus a triangle from corner to corner that fixes the bounding cube."""
+    t = [[(0, 0, .5), (1, 0, .5), (0, 1, .5)], [(1, 1, .25), (0, 1, .25), (1, 0, .25)],
+         [(.3, 0, 0), (.3, 1, 0), (.3, 0, 1)], [(0, .7, 0), (0, .7, 1), (1, .7, 1)],
+         [(0, 0, 0), (1, 1, 1), (1, 0, 1)]]
+    v = np.array(t, dtype=np.float32).reshape(-1, 3)
+    return v, np.arange(v.shape[0], dtype=np.int32).reshape(-1, 3)
+
+
+@pytest.mark.parametrize("res", [128, 256])
+@pytest.mark.parametrize("kind", ["blob", "sliver", "axis"])
+def test_noalloc_large_triangles(gpu_ctx, svo_mod, oracle_mod, kind, res):
+    """Triangles whose grid boxes span many 4x4x4 bricks.  This entry point
+    has no queue for them (it allocates none), so the warp that set a
+    triangle up walks all of its bricks; the keys must still equal the
+    oracle's voxelization and svo_build's, at the largest resolution (256)
+    too, on two calls in a row."""
+    from conftest import random_mesh
+
+    v, f = _axis_mesh() if kind == "axis" else random_mesh(11, 40 if kind == "blob" else 300, kind)
+    want = oracle_mod.voxelize(v, f, res)
+    assert want.size > 0
+    for _ in range(2):
+        got = _noalloc_keys(svo_mod, v, f, res)
+        assert got.shape == want.shape and np.array_equal(got, want)
+    assert np.array_equal(gpu_ctx.build(v, f, res, svo_mod.FLAG_NO_VERT_EDGE).keys(), want)
+
+
 def test_noalloc_rejects_large_resolution_and_host_memory(gpu_ctx, svo_mod):
     import torch
 
