@@ -479,6 +479,16 @@ def run_ours(args, rank: int, world: int):
         cpu = {"value": stris.shape[0] / dt, "unit": "tris/s", "cores": threads, "kind": "port",
                "sample": cpu_sample_text(stride, wname, stris.shape[0], res, bflags) + "; best of 2 oracle builds"}
 
+    writer = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        import tempfile
+
+        r = ctx.build(d_pts, d_tris, res, bflags, sid)
+        nodes = r.nodes()[: 1 << 18]
+        r.close()
+        with tempfile.TemporaryDirectory() as td:
+            writer = time_writers(nodes, td)
+
     if rank == 0:
         line = {
             "metric": "tris/s", "value": value, "unit": "tris/s", "n_gpus": world, "steps": args.steps,
@@ -489,10 +499,69 @@ def run_ours(args, rank: int, world: int):
                        "tuning": dict(zip(TUNING_KEYS, tuning)), **info},
             "nodes_per_s": nodes_per_s,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
-            "gpu_launches": launches,
+            "gpu_launches": launches, "writer": writer,
         }
         print(json.dumps(line), flush=True)
     ctx.close()
+
+
+def result_digest(r) -> str:
+    """SHA-256 over a result's node, vertex, edge and key arrays (host copies)."""
+    import hashlib
+
+    h = hashlib.sha256()
+    for a in (r.nodes(), r.vertices(), r.edges(), r.keys()):
+        h.update(np.ascontiguousarray(a).view(np.uint8))
+    return h.hexdigest()
+
+
+def batch_equals_plain(ctx, pctx, d_meshes, flags: int, sid: int, stride: int = 32) -> dict:
+    """Every stride-th mesh of one (untimed) batch against its own plain build,
+    byte for byte over all output arrays; raises on a difference."""
+    idx = list(range(0, len(d_meshes), stride))
+    results, st, rc = ctx.build_batch([d_meshes[i] for i in idx], flags, sid)
+    if rc != 0:
+        raise RuntimeError(f"batch build failed: {st}")
+    for i, r in zip(idx, results):
+        p = pctx.build(*d_meshes[i], flags, sid)
+        if result_digest(r) != result_digest(p):
+            raise RuntimeError(f"mesh {i}: the batched result differs from its plain build")
+        p.close()
+        r.close()
+    return {"meshes": len(idx), "arrays": "nodes, vertices, edges, keys", "identical": True}
+
+
+def time_writers(nodes: np.ndarray, tmpdir: str) -> dict:
+    """The tree .obj writer (writeTree, src/SVO.cu:737-753) on the same nodes:
+    this library's multithreaded formatter against the oracle's std::ofstream
+    writer; both files must be byte-identical."""
+    import hashlib
+
+    import svo_b200 as S
+
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    a, b = os.path.join(tmpdir, "ours.obj"), os.path.join(tmpdir, "oracle.obj")
+    t = time.perf_counter()
+    S.write_tree_nodes(nodes, a)
+    ours = time.perf_counter() - t
+    t = time.perf_counter()
+    oracle.write_tree_nodes(nodes, b)
+    theirs = time.perf_counter() - t
+    digests = []
+    for path in (a, b):
+        with open(path, "rb") as fh:
+            digests.append(hashlib.sha256(fh.read()).hexdigest())
+    size = os.path.getsize(a)
+    os.remove(a)
+    os.remove(b)
+    if digests[0] != digests[1]:
+        raise RuntimeError("the tree writers disagree")
+    lines = 20 * nodes.shape[0]
+    return {"nodes": int(nodes.shape[0]), "lines": lines, "bytes": size, "threads": os.cpu_count() or 1,
+            "ours_s": ours, "ours_lines_per_s": lines / ours, "ours_mb_per_s": size / ours / 1e6,
+            "oracle_s": theirs, "oracle_lines_per_s": lines / theirs, "identical": True}
 
 
 def run_batch(args, rank: int, world: int):
@@ -583,6 +652,7 @@ def run_batch(args, rank: int, world: int):
         ms, pnodes = timed(plain_once)
         plain_ms.append(ms)
     assert pnodes == nodes
+    same = batch_equals_plain(ctx, pctx, d_meshes, flags, sid)
     dist_barrier()
     t_batch = dist_max(sum(batch_ms))
     t_plain = dist_max(sum(plain_ms))
@@ -617,6 +687,7 @@ def run_batch(args, rank: int, world: int):
             "plain": {"value": plain_value, "unit": "tris/s", "ms_per_step": t_plain / args.steps,
                       "path": "one svo_build per mesh, same stream, same flags, default work split"},
             "batch_over_plain": value / plain_value,
+            "batch_equals_plain": same,
             "e2e": None,
             "roofline": {"kernel": "k_emit (all waves)", "bound": "hbm", "achieved": achieved, "peak": peak,
                          "unit": "GB/s", "frac": (achieved / peak) if achieved else None, "traffic": None,

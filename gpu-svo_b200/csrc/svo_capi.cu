@@ -114,7 +114,7 @@ struct Scratch {
     T *get(size_t count) {
         void *p = nullptr;
         if (err != cudaSuccess) return nullptr;
-        err = cudaMallocFromPoolAsync(&p, std::max<size_t>(count * sizeof(T), 256), pool, st);
+        err = pool_malloc(&p, std::max<size_t>(count * sizeof(T), 256), pool, st);
         if (err != cudaSuccess) return nullptr;
         ptrs.push_back(p);
         return static_cast<T *>(p);
@@ -130,13 +130,13 @@ template <class T>
 T *pool_alloc(cudaMemPool_t pool, cudaStream_t st, size_t count, cudaError_t &err) {
     void *p = nullptr;
     if (err != cudaSuccess) return nullptr;
-    err = cudaMallocFromPoolAsync(&p, std::max<size_t>(count * sizeof(T), 256), pool, st);
+    err = pool_malloc(&p, std::max<size_t>(count * sizeof(T), 256), pool, st);
     return static_cast<T *>(p);
 }
 
 // CUDA events at stage boundaries (SVO_FLAG_TIMINGS).
 struct StageTimer {
-    enum { kStart, kBbox, kVox, kPyr, kScan, kCompact0, kCompact, kEmit, kUnique, kDedup, kN };
+    enum { kStart, kBbox, kVox, kPyr, kScan, kCompact0, kCompact, kEmit, kUnique, kDedup0, kDedup, kEnd, kN };
     bool on = false;
     cudaEvent_t ev[kN] = {};
     bool rec[kN] = {};
@@ -599,290 +599,332 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
     };
     Scratch S{ctx->pool, st};
     StageTimer tm((flags & SVO_FLAG_TIMINGS) != 0);
+    auto free_results = [&]() {
+        for (svo_result *&r : res) {
+            svo_result_free(r);
+            r = nullptr;
+        }
+    };
     if (n > 0) {
-        cudaError_t err = cudaSuccess;
-        // outputs, code lists, job tables
-        std::vector<CompactJob> jobs;
-        std::vector<uint64_t> word_off(1, 0);
-        std::vector<KeyJob> kjobs;
-        std::vector<uint64_t> blk_off(1, 0);
-        std::vector<EmitParams> ep(n);
-        std::vector<const uint64_t *> top_ptr(n);
-        uint64_t ktot = 0;
-        std::vector<uint64_t> kbase(n);
-        for (int j = 0; j < n; ++j) {
-            const MeshHost &mh = b->m[wave[j]];
-            kbase[j] = ktot;
-            for (int l = 1; l <= mh.T; ++l) ktot += mh.totals[l];
-        }
-        uint64_t *K = S.get<uint64_t>(ktot + 1);
-        // per-word ranks of levels >= 1 (k_compact writes them, rank lookups read them)
-        uint64_t wtot = 0;
-        std::vector<uint64_t> wbase(n);
-        for (int j = 0; j < n; ++j) {
-            const MeshHost &mh = b->m[wave[j]];
-            wbase[j] = wtot;
-            wtot += mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1];
-        }
-        uint32_t *WP = S.get<uint32_t>(wtot + 1);
-        unsigned long long *dups = S.get<unsigned long long>(2 * (size_t)n);
-        uint64_t *top = S.get<uint64_t>(n);
-        if (!K || !WP || !dups || !top) return cuda_fail(S.err, "wave scratch");
-        check(cudaMemsetAsync(dups, 0, 16 * (size_t)n, st), "memset");
-        // one block for the output arrays of the whole wave
-        size_t arena_bytes = 0;
-        for (int j = 0; j < n; ++j) {
-            const MeshHost &mh = b->m[wave[j]];
-            arena_bytes += arena_round(mh.N * sizeof(svo_node));
-            if (ve) arena_bytes += arena_round(mh.N * 8 * sizeof(svo_vertex)) + arena_round(mh.N * 12 * sizeof(svo_edge));
-            if (want_keys) arena_bytes += arena_round((size_t)mh.totals[0] * 8);
-        }
-        svo_arena *arena = new svo_arena();
-        arena->refs = 1;  // the wave's own reference, dropped below
-        if (cudaMallocFromPoolAsync(&arena->base, std::max<size_t>(arena_bytes, 256), ctx->out_pool, st) != cudaSuccess) {
-            delete arena;
-            cudaGetLastError();
-            return fail(SVO_ERR_OUT_OF_MEMORY, "wave outputs: %zu bytes", arena_bytes);
-        }
-        unsigned char *arena_at = static_cast<unsigned char *>(arena->base);
-        auto drop_arena = [&]() {
-            if (arena && arena->refs.fetch_sub(1) == 1) {
-                cudaFreeAsync(arena->base, st);
+        // The wave body: an error return from it still reaches the per-mesh
+        // status loop below, which marks every mesh of the wave as failed.
+        const int wave_rc = [&]() -> int {
+            cudaError_t err = cudaSuccess;
+            // outputs, code lists, job tables
+            std::vector<CompactJob> jobs;
+            std::vector<uint64_t> word_off(1, 0);
+            std::vector<KeyJob> kjobs;
+            std::vector<uint64_t> blk_off(1, 0);
+            std::vector<EmitParams> ep(n);
+            std::vector<const uint64_t *> top_ptr(n);
+            uint64_t ktot = 0;
+            std::vector<uint64_t> kbase(n);
+            for (int j = 0; j < n; ++j) {
+                const MeshHost &mh = b->m[wave[j]];
+                kbase[j] = ktot;
+                for (int l = 1; l <= mh.T; ++l) ktot += mh.totals[l];
+            }
+            uint64_t *K = S.get<uint64_t>(ktot + 1);
+            // per-word ranks of levels >= 1 (k_compact writes them, rank lookups read them)
+            uint64_t wtot = 0;
+            std::vector<uint64_t> wbase(n);
+            for (int j = 0; j < n; ++j) {
+                const MeshHost &mh = b->m[wave[j]];
+                wbase[j] = wtot;
+                wtot += mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1];
+            }
+            uint32_t *WP = S.get<uint32_t>(wtot + 1);
+            unsigned long long *dups = S.get<unsigned long long>(2 * (size_t)n);
+            uint64_t *top = S.get<uint64_t>(n);
+            if (!K || !WP || !dups || !top) return cuda_fail(S.err, "wave scratch");
+            check(cudaMemsetAsync(dups, 0, 16 * (size_t)n, st), "memset");
+            // one block for the output arrays of the whole wave
+            size_t arena_bytes = 0;
+            for (int j = 0; j < n; ++j) {
+                const MeshHost &mh = b->m[wave[j]];
+                arena_bytes += arena_round(mh.N * sizeof(svo_node));
+                if (ve) arena_bytes += arena_round(mh.N * 8 * sizeof(svo_vertex)) + arena_round(mh.N * 12 * sizeof(svo_edge));
+                if (want_keys) arena_bytes += arena_round((size_t)mh.totals[0] * 8);
+            }
+            svo_arena *arena = new svo_arena();
+            arena->refs = 1;  // the wave's own reference, dropped below
+            if (pool_malloc(&arena->base, std::max<size_t>(arena_bytes, 256), ctx->out_pool, st) != cudaSuccess) {
                 delete arena;
+                cudaGetLastError();
+                return fail(SVO_ERR_OUT_OF_MEMORY, "wave outputs: %zu bytes", arena_bytes);
             }
-            arena = nullptr;
-        };
-        for (int j = 0; j < n; ++j) {
-            const MeshHost &mh = b->m[wave[j]];
-            const MeshDev &md = b->h_mesh[dev_k[j]];
-            svo_result *r = new svo_result();
-            res[j] = r;
-            r->device = ctx->device;
-            r->stream = st;
-            r->pool = ctx->pool;
-            r->depth = mh.T + 1;
-            for (int l = 0; l <= mh.T; ++l) r->level_counts.push_back((int64_t)mh.n_l[l]);
-            for (int a = 0; a < 3; ++a) {
-                r->bbox.min[a] = mh.gp.bbox[a];
-                r->bbox.max[a] = mh.gp.bbox[3 + a];
-                r->bbox.width[a] = mh.gp.bbox[6 + a];
-                r->unit[a] = mh.gp.unit[a];
+            unsigned char *arena_at = static_cast<unsigned char *>(arena->base);
+            auto drop_arena = [&]() {
+                if (arena && arena->refs.fetch_sub(1) == 1) {
+                    cudaFreeAsync(arena->base, st);
+                    delete arena;
+                }
+                arena = nullptr;
+            };
+            for (int j = 0; j < n; ++j) {
+                const MeshHost &mh = b->m[wave[j]];
+                const MeshDev &md = b->h_mesh[dev_k[j]];
+                svo_result *r = new svo_result();
+                res[j] = r;
+                r->device = ctx->device;
+                r->stream = st;
+                r->pool = ctx->pool;
+                r->depth = mh.T + 1;
+                for (int l = 0; l <= mh.T; ++l) r->level_counts.push_back((int64_t)mh.n_l[l]);
+                for (int a = 0; a < 3; ++a) {
+                    r->bbox.min[a] = mh.gp.bbox[a];
+                    r->bbox.max[a] = mh.gp.bbox[3 + a];
+                    r->bbox.width[a] = mh.gp.bbox[6 + a];
+                    r->unit[a] = mh.gp.unit[a];
+                }
+                r->n_nodes = mh.N;
+                r->nodes = arena_take<svo_node>(arena_at, mh.N);
+                if (ve) {
+                    r->verts = arena_take<svo_vertex>(arena_at, mh.N * 8);
+                    r->edges = arena_take<svo_edge>(arena_at, mh.N * 12);
+                    r->n_verts = mh.N * 8;
+                    r->n_edges = mh.N * 12;
+                }
+                if (want_keys) {
+                    r->keys = arena_take<uint64_t>(arena_at, mh.totals[0]);
+                    r->n_keys = mh.totals[0];
+                }
+                r->arena = arena;
+                r->own = 0x70;
+                arena->refs.fetch_add(1);
+                // compaction jobs: levels 1..T into K, level 0 into the keys
+                CompactJob job{};
+                job.bits = md.bits;
+                job.pre = md.pre;
+                job.py = mh.py;
+                job.l0 = 1;
+                job.l1 = mh.T + 1;
+                job.out = K + kbase[j];
+                job.wpre = WP + wbase[j];
+                uint64_t ko = 0;
+                for (int l = 1; l <= mh.T; ++l) {
+                    job.koff[l] = ko;
+                    ko += mh.totals[l];
+                }
+                jobs.push_back(job);
+                word_off.push_back(word_off.back() + mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1]);
+                if (want_keys && mh.T >= 3) {
+                    // the level-3 code list is the list of non-empty level-0 blocks
+                    kjobs.push_back(KeyJob{md.bits, md.pre, job.out + job.koff[3], r->keys});
+                    blk_off.push_back(blk_off.back() + mh.totals[3]);
+                } else if (want_keys) {
+                    CompactJob k0 = job;
+                    k0.l0 = 0;
+                    k0.l1 = 1;
+                    k0.out = r->keys;
+                    k0.wpre = nullptr;
+                    std::memset(k0.koff, 0, sizeof(k0.koff));
+                    k0.rflag = mh.py.words[0] >= kRegionWords ? b->rflag + mh.cta0 : nullptr;
+                    jobs.push_back(k0);
+                    word_off.push_back(word_off.back() + mh.py.words[0]);
+                }
+                // emission parameters
+                EmitParams &P = ep[j];
+                P.T = mh.T;
+                P.N = (uint32_t)mh.N;
+                P.flags = flags;
+                const uint32_t R = 1u << (mh.py.grid_levels - 1);
+                float w = mh.gp.unit[0];  // unitVoxelSize.x doubled per level (src/SVO.cu:351,483)
+                for (int l = 0; l <= mh.T; ++l) {
+                    P.lv[l].off = (uint32_t)mh.off[l];
+                    P.lv[l].n = (uint32_t)mh.n_l[l];
+                    P.lv[l].K1 = job.out + (l < mh.T ? job.koff[l + 1] : job.koff[mh.T]);
+                    P.lv[l].bits = md.bits + mh.py.woff[l];
+                    P.lv[l].wpre = l >= 1 ? job.wpre + (mh.py.woff[l] - mh.py.woff[1]) : nullptr;
+                    P.lv[l].coff = mh.py.coff[l];
+                    P.lv[l].side = std::max<uint32_t>(1u, R >> l);
+                    P.lv[l].width = w;
+                    w = w * 2.0f;
+                }
+                P.pre = md.pre;
+                P.gp = md.gp;
+                P.nodes = r->nodes;
+                P.verts = ve ? r->verts : nullptr;
+                P.edges = ve ? r->edges : nullptr;
+                P.dups = dups + 2 * j;
+                top_ptr[j] = job.out + job.koff[mh.T];
             }
-            r->n_nodes = mh.N;
-            r->nodes = arena_take<svo_node>(arena_at, mh.N);
-            if (ve) {
-                r->verts = arena_take<svo_vertex>(arena_at, mh.N * 8);
-                r->edges = arena_take<svo_edge>(arena_at, mh.N * 12);
-                r->n_verts = mh.N * 8;
-                r->n_edges = mh.N * 12;
+            if (err != cudaSuccess) {
+                free_results();
+                drop_arena();
+                return cuda_fail(err, "output allocation");
             }
-            if (want_keys) {
-                r->keys = arena_take<uint64_t>(arena_at, mh.totals[0]);
-                r->n_keys = mh.totals[0];
-            }
-            r->arena = arena;
-            r->own = 0x70;
-            arena->refs.fetch_add(1);
-            // compaction jobs: levels 1..T into K, level 0 into the keys
-            CompactJob job{};
-            job.bits = md.bits;
-            job.pre = md.pre;
-            job.py = mh.py;
-            job.l0 = 1;
-            job.l1 = mh.T + 1;
-            job.out = K + kbase[j];
-            job.wpre = WP + wbase[j];
-            uint64_t ko = 0;
-            for (int l = 1; l <= mh.T; ++l) {
-                job.koff[l] = ko;
-                ko += mh.totals[l];
-            }
-            jobs.push_back(job);
-            word_off.push_back(word_off.back() + mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1]);
-            if (want_keys && mh.T >= 3) {
-                // the level-3 code list is the list of non-empty level-0 blocks
-                kjobs.push_back(KeyJob{md.bits, md.pre, job.out + job.koff[3], r->keys});
-                blk_off.push_back(blk_off.back() + mh.totals[3]);
-            } else if (want_keys) {
-                CompactJob k0 = job;
-                k0.l0 = 0;
-                k0.l1 = 1;
-                k0.out = r->keys;
-                k0.wpre = nullptr;
-                std::memset(k0.koff, 0, sizeof(k0.koff));
-                k0.rflag = mh.py.words[0] >= kRegionWords ? b->rflag + mh.cta0 : nullptr;
-                jobs.push_back(k0);
-                word_off.push_back(word_off.back() + mh.py.words[0]);
-            }
-            // emission parameters
-            EmitParams &P = ep[j];
-            P.T = mh.T;
-            P.N = (uint32_t)mh.N;
-            P.flags = flags;
-            const uint32_t R = 1u << (mh.py.grid_levels - 1);
-            float w = mh.gp.unit[0];  // unitVoxelSize.x doubled per level (src/SVO.cu:351,483)
-            for (int l = 0; l <= mh.T; ++l) {
-                P.lv[l].off = (uint32_t)mh.off[l];
-                P.lv[l].n = (uint32_t)mh.n_l[l];
-                P.lv[l].K1 = job.out + (l < mh.T ? job.koff[l + 1] : job.koff[mh.T]);
-                P.lv[l].bits = md.bits + mh.py.woff[l];
-                P.lv[l].wpre = l >= 1 ? job.wpre + (mh.py.woff[l] - mh.py.woff[1]) : nullptr;
-                P.lv[l].coff = mh.py.coff[l];
-                P.lv[l].side = std::max<uint32_t>(1u, R >> l);
-                P.lv[l].width = w;
-                w = w * 2.0f;
-            }
-            P.pre = md.pre;
-            P.gp = md.gp;
-            P.nodes = r->nodes;
-            P.verts = ve ? r->verts : nullptr;
-            P.edges = ve ? r->edges : nullptr;
-            P.dups = dups + 2 * j;
-            top_ptr[j] = job.out + job.koff[mh.T];
-        }
-        if (err != cudaSuccess) {
-            for (svo_result *r : res) svo_result_free(r);
-            drop_arena();
-            return cuda_fail(err, "output allocation");
-        }
-        CompactJob *d_jobs = S.get<CompactJob>(jobs.size());
-        uint64_t *d_word_off = S.get<uint64_t>(word_off.size());
-        KeyJob *d_kjobs = kjobs.empty() ? nullptr : S.get<KeyJob>(kjobs.size());
-        uint64_t *d_blk_off = kjobs.empty() ? nullptr : S.get<uint64_t>(blk_off.size());
-        const uint64_t **d_top_ptr = S.get<const uint64_t *>(n);
-        if (S.err != cudaSuccess) {
-            for (svo_result *r : res) svo_result_free(r);
-            drop_arena();
-            return cuda_fail(S.err, "wave tables");
-        }
-        check(upload(d_jobs, jobs, st), "upload");
-        check(upload(d_word_off, word_off, st), "upload");
-        if (!kjobs.empty()) {
-            check(upload(d_kjobs, kjobs, st), "upload");
-            check(upload(d_blk_off, blk_off, st), "upload");
-        }
-        check(upload(d_top_ptr, top_ptr, st), "upload");
-        tm.mark(StageTimer::kCompact0, st);
-        check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
-        if (!kjobs.empty())
-            check(launch_compact_keys(KeyBatch{d_kjobs, (int)kjobs.size(), d_blk_off}, blk_off.back(), st), "keys");
-        tm.mark(StageTimer::kCompact, st);
-        // Large meshes get launches of their own (parameters in the kernel's
-        // constant space); the rest share one launch over the mesh table.
-        // With two or more of them, they spread round-robin over the build
-        // stream and three more, so that one kernel's tail overlaps the next.
-        std::vector<EmitParams> ep_small;
-        std::vector<uint64_t> off_small(1, 0);
-        int n_own = 0;
-        for (int j = 0; j < n; ++j) n_own += (n == 1 || ep[j].N >= kOwnEmitNodes) ? 1 : 0;
-        AuxStreams *aux = n_own >= 2 ? aux_acquire(ctx) : nullptr;
-        if (aux) {
-            check(cudaEventRecord(aux->fork, st), "fork");
-            for (int i = 0; i < AuxStreams::kCount; ++i) check(cudaStreamWaitEvent(aux->s[i], aux->fork, 0), "fork");
-        }
-        int k_own = 0;
-        for (int j = 0; j < n; ++j) {
-            if (n == 1 || ep[j].N >= kOwnEmitNodes) {
-                const int lane = aux ? k_own % (AuxStreams::kCount + 1) : 0;
-                cudaStream_t es = lane == 0 ? st : aux->s[lane - 1];
-                ++k_own;
-                check(launch_emit(EmitBatch{nullptr, 1, nullptr}, &ep[j], ep[j].N, flags, ctx->num_sms, es), "emit");
-            } else {
-                ep_small.push_back(ep[j]);
-                off_small.push_back(off_small.back() + (ep[j].N + 31) / 32 * 32);
-            }
-        }
-        if (aux) {
-            for (int i = 0; i < AuxStreams::kCount; ++i) {
-                check(cudaEventRecord(aux->join[i], aux->s[i]), "join");
-                check(cudaStreamWaitEvent(st, aux->join[i], 0), "join");
-            }
-            aux_release(ctx, aux);
-        }
-        if (!ep_small.empty()) {
-            EmitParams *d_eps = S.get<EmitParams>(ep_small.size());
-            uint64_t *d_offs = S.get<uint64_t>(off_small.size());
+            CompactJob *d_jobs = S.get<CompactJob>(jobs.size());
+            uint64_t *d_word_off = S.get<uint64_t>(word_off.size());
+            KeyJob *d_kjobs = kjobs.empty() ? nullptr : S.get<KeyJob>(kjobs.size());
+            uint64_t *d_blk_off = kjobs.empty() ? nullptr : S.get<uint64_t>(blk_off.size());
+            const uint64_t **d_top_ptr = S.get<const uint64_t *>(n);
             if (S.err != cudaSuccess) {
-                for (svo_result *r : res) svo_result_free(r);
+                free_results();
                 drop_arena();
                 return cuda_fail(S.err, "wave tables");
             }
-            check(upload(d_eps, ep_small, st), "upload");
-            check(upload(d_offs, off_small, st), "upload");
-            check(launch_emit(EmitBatch{d_eps, (int)ep_small.size(), d_offs}, nullptr, off_small.back(), flags,
-                              ctx->num_sms, st),
-                  "emit");
-        }
-        tm.mark(StageTimer::kEmit, st);
-        k_gather_top<<<(n + 127) / 128, 128, 0, st>>>(d_top_ptr, n, top);
-        count_launches(1);
-        std::vector<uint64_t> h_top(n);
-        std::vector<unsigned long long> h_dups(2 * n);
-        check(cudaMemcpyAsync(h_top.data(), top, 8 * (size_t)n, cudaMemcpyDeviceToHost, st), "read top");
-        check(cudaMemcpyAsync(h_dups.data(), dups, 16 * (size_t)n, cudaMemcpyDeviceToHost, st), "read dups");
-        check(cudaStreamSynchronize(st), "emit phase");
-        for (int j = 0; j < n && rc == SVO_OK; ++j) {
-            MeshHost &mh = b->m[wave[j]];
-            svo_result *r = res[j];
-            if (mh.T == 0 || (h_top[j] & 7) != 0) {
-                mesh_error(mh, SVO_ERR_DEGENERATE,
-                           "single top-level node with a non-zero octant: undefined in the reference");
-                continue;
+            check(upload(d_jobs, jobs, st), "upload");
+            check(upload(d_word_off, word_off, st), "upload");
+            if (!kjobs.empty()) {
+                check(upload(d_kjobs, kjobs, st), "upload");
+                check(upload(d_blk_off, blk_off, st), "upload");
             }
-            if (ve && (h_dups[2 * j] || h_dups[2 * j + 1])) {
-                // consecutive duplicates (degenerate widths or absorbed
-                // coordinates): compact both arrays as thrust::unique does
-                const uint64_t nv = mh.N * 8, ne = mh.N * 12;
-                const uint64_t tiles = (std::max(nv, ne) + kUniqueTile - 1) / kUniqueTile;
-                Scratch U{ctx->pool, st};
-                uint32_t *tc = U.get<uint32_t>(tiles), *tp = U.get<uint32_t>(tiles + 1);
-                unsigned long long *ss = U.get<unsigned long long>(scan_scratch_words(tiles));
-                uint32_t *ustat = U.get<uint32_t>(1);
-                svo_vertex *v2 = h_dups[2 * j] ? pool_alloc<svo_vertex>(ctx->out_pool, st, nv, err) : nullptr;
-                svo_edge *e2 = h_dups[2 * j + 1] ? pool_alloc<svo_edge>(ctx->out_pool, st, ne, err) : nullptr;
-                if (U.err != cudaSuccess || err != cudaSuccess) {
-                    rc = cuda_fail(U.err != cudaSuccess ? U.err : err, "unique scratch");
-                    break;
-                }
-                check(cudaMemsetAsync(ustat, 0, 4, st), "memset");
-                uint32_t cv = 0, ce = 0;
-                if (v2) {
-                    check(launch_unique_vertices(r->verts, nv, v2, tc, tp, ss, ustat, st), "unique v");
-                    check(cudaMemcpyAsync(&cv, tp + (nv + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost,
-                                          st), "read");
-                    check(cudaStreamSynchronize(st), "unique v");
-                }
-                if (e2) {
-                    check(launch_unique_edges(r->edges, ne, e2, tc, tp, ss, ustat, st), "unique e");
-                    check(cudaMemcpyAsync(&ce, tp + (ne + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost,
-                                          st), "read");
-                    check(cudaStreamSynchronize(st), "unique e");
-                }
-                if (v2) {
-                    if (r->own & 2) cudaFreeAsync(r->verts, st);
-                    r->verts = v2;
-                    r->own |= 2;
-                    r->n_verts = cv;
-                }
-                if (e2) {
-                    if (r->own & 4) cudaFreeAsync(r->edges, st);
-                    r->edges = e2;
-                    r->own |= 4;
-                    r->n_edges = ce;
+            check(upload(d_top_ptr, top_ptr, st), "upload");
+            tm.mark(StageTimer::kCompact0, st);
+            check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
+            if (!kjobs.empty())
+                check(launch_compact_keys(KeyBatch{d_kjobs, (int)kjobs.size(), d_blk_off}, blk_off.back(), st), "keys");
+            tm.mark(StageTimer::kCompact, st);
+            // The dedup keys read only the bitmaps and code lists: they run on
+            // a stream of their own, forked here, while the emission writes.
+            const bool dd = (flags & SVO_FLAG_DEDUP) != 0;
+            AuxStreams *dset = dd ? aux_acquire(ctx) : nullptr;
+            const cudaStream_t ds = dset ? dset->s[0] : st;
+            if (dset) {
+                check(cudaEventRecord(dset->fork, st), "fork");
+                check(cudaStreamWaitEvent(ds, dset->fork, 0), "fork");
+            }
+            auto join_dedup = [&]() {
+                if (!dset) return;
+                check(cudaEventRecord(dset->join[0], ds), "join");
+                check(cudaStreamWaitEvent(st, dset->join[0], 0), "join");
+                aux_release(ctx, dset);
+                dset = nullptr;
+            };
+            // Large meshes get launches of their own (parameters in the kernel's
+            // constant space); the rest share one launch over the mesh table.
+            // With two or more of them, they spread round-robin over the build
+            // stream and three more, so that one kernel's tail overlaps the next.
+            std::vector<EmitParams> ep_small;
+            std::vector<uint64_t> off_small(1, 0);
+            int n_own = 0;
+            for (int j = 0; j < n; ++j) n_own += (n == 1 || ep[j].N >= kOwnEmitNodes) ? 1 : 0;
+            AuxStreams *aux = n_own >= 2 ? aux_acquire(ctx) : nullptr;
+            if (aux) {
+                check(cudaEventRecord(aux->fork, st), "fork");
+                for (int i = 0; i < AuxStreams::kCount; ++i) check(cudaStreamWaitEvent(aux->s[i], aux->fork, 0), "fork");
+            }
+            int k_own = 0;
+            for (int j = 0; j < n; ++j) {
+                if (n == 1 || ep[j].N >= kOwnEmitNodes) {
+                    const int lane = aux ? k_own % (AuxStreams::kCount + 1) : 0;
+                    cudaStream_t es = lane == 0 ? st : aux->s[lane - 1];
+                    ++k_own;
+                    check(launch_emit(EmitBatch{nullptr, 1, nullptr}, &ep[j], ep[j].N, flags, ctx->num_sms, es), "emit");
+                } else {
+                    ep_small.push_back(ep[j]);
+                    off_small.push_back(off_small.back() + (ep[j].N + 31) / 32 * 32);
                 }
             }
-        }
-        tm.mark(StageTimer::kUnique, st);
-        for (int j = 0; j < n && rc == SVO_OK; ++j) {
-            MeshHost &mh = b->m[wave[j]];
-            if (mh.status != SVO_OK || !(flags & SVO_FLAG_DEDUP)) continue;
-            const int drc = build_dedup(ctx->pool, ctx->out_pool, st, ep[j], res[j]->n_dedup, res[j]->dedup,
-                                        ctx->num_sms);
-            if (drc != SVO_OK) mesh_error(mh, drc, svo_last_error());
-        }
-        tm.mark(StageTimer::kDedup, st);
-        if (tm.on) cudaEventSynchronize(tm.ev[StageTimer::kDedup]);
-        drop_arena();
+            if (aux) {
+                for (int i = 0; i < AuxStreams::kCount; ++i) {
+                    check(cudaEventRecord(aux->join[i], aux->s[i]), "join");
+                    check(cudaStreamWaitEvent(st, aux->join[i], 0), "join");
+                }
+                aux_release(ctx, aux);
+            }
+            if (!ep_small.empty()) {
+                EmitParams *d_eps = S.get<EmitParams>(ep_small.size());
+                uint64_t *d_offs = S.get<uint64_t>(off_small.size());
+                if (S.err != cudaSuccess) {
+                    join_dedup();
+                    free_results();
+                    drop_arena();
+                    return cuda_fail(S.err, "wave tables");
+                }
+                check(upload(d_eps, ep_small, st), "upload");
+                check(upload(d_offs, off_small, st), "upload");
+                check(launch_emit(EmitBatch{d_eps, (int)ep_small.size(), d_offs}, nullptr, off_small.back(), flags,
+                                  ctx->num_sms, st),
+                      "emit");
+            }
+            tm.mark(StageTimer::kEmit, st);
+            // Dedup of every mesh on the forked stream (its host-side waits
+            // overlap the emission running on the GPU); statuses are applied
+            // after the emission's own checks.
+            std::vector<int> drc(n, SVO_OK);
+            std::vector<std::string> dmsg(n);
+            if (dd) {
+                tm.mark(StageTimer::kDedup0, ds);
+                for (int j = 0; j < n && rc == SVO_OK; ++j) {
+                    if (b->m[wave[j]].status != SVO_OK) continue;
+                    drc[j] = build_dedup(ctx->pool, ctx->out_pool, ds, ep[j], res[j]->n_dedup, res[j]->dedup,
+                                         ctx->num_sms);
+                    if (drc[j] != SVO_OK) dmsg[j] = svo_last_error();
+                }
+                tm.mark(StageTimer::kDedup, ds);
+            }
+            k_gather_top<<<(n + 127) / 128, 128, 0, st>>>(d_top_ptr, n, top);
+            count_launches(1);
+            std::vector<uint64_t> h_top(n);
+            std::vector<unsigned long long> h_dups(2 * n);
+            check(cudaMemcpyAsync(h_top.data(), top, 8 * (size_t)n, cudaMemcpyDeviceToHost, st), "read top");
+            check(cudaMemcpyAsync(h_dups.data(), dups, 16 * (size_t)n, cudaMemcpyDeviceToHost, st), "read dups");
+            check(cudaStreamSynchronize(st), "emit phase");
+            for (int j = 0; j < n && rc == SVO_OK; ++j) {
+                MeshHost &mh = b->m[wave[j]];
+                svo_result *r = res[j];
+                if (mh.T == 0 || (h_top[j] & 7) != 0) {
+                    mesh_error(mh, SVO_ERR_DEGENERATE,
+                               "single top-level node with a non-zero octant: undefined in the reference");
+                    continue;
+                }
+                if (ve && (h_dups[2 * j] || h_dups[2 * j + 1])) {
+                    // consecutive duplicates (degenerate widths or absorbed
+                    // coordinates): compact both arrays as thrust::unique does
+                    const uint64_t nv = mh.N * 8, ne = mh.N * 12;
+                    const uint64_t tiles = (std::max(nv, ne) + kUniqueTile - 1) / kUniqueTile;
+                    Scratch U{ctx->pool, st};
+                    uint32_t *tc = U.get<uint32_t>(tiles), *tp = U.get<uint32_t>(tiles + 1);
+                    unsigned long long *ss = U.get<unsigned long long>(scan_scratch_words(tiles));
+                    uint32_t *ustat = U.get<uint32_t>(1);
+                    svo_vertex *v2 = h_dups[2 * j] ? pool_alloc<svo_vertex>(ctx->out_pool, st, nv, err) : nullptr;
+                    svo_edge *e2 = h_dups[2 * j + 1] ? pool_alloc<svo_edge>(ctx->out_pool, st, ne, err) : nullptr;
+                    if (U.err != cudaSuccess || err != cudaSuccess) {
+                        rc = cuda_fail(U.err != cudaSuccess ? U.err : err, "unique scratch");
+                        break;
+                    }
+                    check(cudaMemsetAsync(ustat, 0, 4, st), "memset");
+                    uint32_t cv = 0, ce = 0;
+                    if (v2) {
+                        check(launch_unique_vertices(r->verts, nv, v2, tc, tp, ss, ustat, st), "unique v");
+                        check(cudaMemcpyAsync(&cv, tp + (nv + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost,
+                                              st), "read");
+                        check(cudaStreamSynchronize(st), "unique v");
+                    }
+                    if (e2) {
+                        check(launch_unique_edges(r->edges, ne, e2, tc, tp, ss, ustat, st), "unique e");
+                        check(cudaMemcpyAsync(&ce, tp + (ne + kUniqueTile - 1) / kUniqueTile, 4, cudaMemcpyDeviceToHost,
+                                              st), "read");
+                        check(cudaStreamSynchronize(st), "unique e");
+                    }
+                    if (v2) {
+                        if (r->own & 2) cudaFreeAsync(r->verts, st);
+                        r->verts = v2;
+                        r->own |= 2;
+                        r->n_verts = cv;
+                    }
+                    if (e2) {
+                        if (r->own & 4) cudaFreeAsync(r->edges, st);
+                        r->edges = e2;
+                        r->own |= 4;
+                        r->n_edges = ce;
+                    }
+                }
+            }
+            tm.mark(StageTimer::kUnique, st);
+            join_dedup();
+            for (int j = 0; j < n; ++j) {
+                MeshHost &mh = b->m[wave[j]];
+                if (mh.status == SVO_OK && drc[j] != SVO_OK) mesh_error(mh, drc[j], dmsg[j].c_str());
+            }
+            tm.mark(StageTimer::kEnd, st);
+            if (tm.on) cudaEventSynchronize(tm.ev[StageTimer::kEnd]);
+            drop_arena();
+            return SVO_OK;
+        }();
+        if (wave_rc != SVO_OK && rc == SVO_OK) rc = wave_rc;
     }
     int first_err = rc;
     for (int j = 0; j < n; ++j) {
@@ -900,8 +942,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 r->timings[5] = tm.span(StageTimer::kCompact0, StageTimer::kCompact);
                 r->timings[6] = tm.span(StageTimer::kCompact, StageTimer::kEmit);
                 r->timings[7] = tm.span(StageTimer::kEmit, StageTimer::kUnique);
-                r->timings[8] = tm.span(StageTimer::kUnique, StageTimer::kDedup);
-                r->timings[0] = b->timings_a[0] + tm.span(StageTimer::kCompact0, StageTimer::kDedup);
+                r->timings[8] = tm.span(StageTimer::kDedup0, StageTimer::kDedup);
+                r->timings[0] = b->timings_a[0] + tm.span(StageTimer::kCompact0, StageTimer::kEnd);
             }
             out[wave[j] - first] = r;
         } else {
@@ -1058,6 +1100,35 @@ int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t) {
     t->split = ctx->tune.split;
     t->inplace_max = ctx->tune.inplace_max;
     t->serial_packed = ctx->tune.serial_packed;
+    return SVO_OK;
+}
+
+int svo_ctx_memory(const svo_ctx *ctx, uint64_t *scratch_used, uint64_t *result_used) {
+    if (!ctx) return fail(SVO_ERR_INVALID_ARGUMENT, "null context");
+    uint64_t a = 0, b = 0;  // the attribute is a 64-bit unsigned count
+    SVO_TRY(cudaMemPoolGetAttribute(ctx->pool, cudaMemPoolAttrUsedMemCurrent, &a), "pool attribute");
+    SVO_TRY(cudaMemPoolGetAttribute(ctx->out_pool, cudaMemPoolAttrUsedMemCurrent, &b), "pool attribute");
+    if (scratch_used) *scratch_used = (uint64_t)a;
+    if (result_used) *result_used = (uint64_t)b;
+    return SVO_OK;
+}
+
+int svo_selftest_scan_timeout(svo_ctx *ctx, void *stream) {
+    if (!ctx) return fail(SVO_ERR_INVALID_ARGUMENT, "null context");
+    SVO_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint64_t n = 3 * 4096 + 17;  // four tiles of the single-pass scan
+    Scratch S{ctx->pool, st};
+    uint32_t *in = S.get<uint32_t>(n), *out = S.get<uint32_t>(n + 1), *status = S.get<uint32_t>(1);
+    unsigned long long *scratch = S.get<unsigned long long>(scan_stalled_scratch_words(n));
+    if (S.err != cudaSuccess) return cuda_fail(S.err, "self-test scratch");
+    SVO_TRY(cudaMemsetAsync(in, 0, n * sizeof(uint32_t), st), "memset");
+    SVO_TRY(cudaMemsetAsync(status, 0, sizeof(uint32_t), st), "memset");
+    SVO_TRY(launch_scan_stalled(in, out, n, scratch, status, 1 << 12, st), "stalled scan");
+    uint32_t h = 0;
+    SVO_TRY(cudaMemcpyAsync(&h, status, sizeof(h), cudaMemcpyDeviceToHost, st), "read status");
+    SVO_TRY(cudaStreamSynchronize(st), "stalled scan");
+    if (h & kStatusScanTimeout) return fail(SVO_ERR_DEVICE_TIMEOUT, "scan look-back timed out (self-test)");
     return SVO_OK;
 }
 
@@ -1319,6 +1390,25 @@ void set_error(const char *msg) { g_err = msg; }
 namespace svo {
 static std::atomic<int64_t> g_launches{0};
 void count_launches(int n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+
+// Countdown of svo_debug_fail_alloc: when it reaches the allocation it names,
+// that allocation reports cudaErrorMemoryAllocation without asking the pool.
+static std::atomic<int64_t> g_fail_alloc{0};
+
+cudaError_t pool_malloc(void **p, size_t bytes, cudaMemPool_t pool, cudaStream_t st) {
+    int64_t k = g_fail_alloc.load(std::memory_order_relaxed);
+    while (k > 0 && !g_fail_alloc.compare_exchange_weak(k, k - 1, std::memory_order_relaxed)) {
+    }
+    if (k == 1) {
+        *p = nullptr;
+        return cudaErrorMemoryAllocation;
+    }
+    return cudaMallocFromPoolAsync(p, bytes, pool, st);
+}
 }  // namespace svo
 
 extern "C" int64_t svo_kernel_launches(void) { return svo::g_launches.load(std::memory_order_relaxed); }
+
+extern "C" int64_t svo_debug_fail_alloc(int64_t n) {
+    return svo::g_fail_alloc.exchange(n > 0 ? n : 0, std::memory_order_relaxed);
+}

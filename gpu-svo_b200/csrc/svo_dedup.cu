@@ -520,7 +520,7 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
                           scan_scratch_words(std::max<uint64_t>(p.chunks, g_words)) * 8, 256};
     void *blk2[6] = {};  // sized once the counts are known: states per chunk, the states, keys per tile
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = cudaMallocFromPoolAsync(&blk[i], sz[i], pool, st);
+    for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = pool_malloc(&blk[i], sz[i], pool, st);
     auto release = [&]() {
         for (void *b : blk)
             if (b) cudaFreeAsync(b, st);
@@ -577,7 +577,7 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     const size_t sz2[6] = {std::max<uint64_t>(nt, 1) * 4, (nt + 1) * 4, std::max<uint64_t>(h_nq, 1) * 8,
                            3 * std::max<uint64_t>(ntiles, 1) * 4, 3 * (ntiles + 1) * 4,
                            scan_scratch_words(std::max<uint64_t>(std::max<uint64_t>(nt, ntiles), 1)) * 8};
-    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = cudaMallocFromPoolAsync(&blk2[i], sz2[i], pool, st);
+    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = pool_malloc(&blk2[i], sz2[i], pool, st);
     if (e != cudaSuccess) return fail(e, "scratch");
     p.qn = static_cast<uint32_t *>(blk2[0]);
     uint32_t *qpre = static_cast<uint32_t *>(blk2[1]);
@@ -613,7 +613,7 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     for (int k = 0; k < 3; ++k) {
         if (h[k] == 0) continue;
         void *o = nullptr;
-        if ((e = cudaMallocFromPoolAsync(&o, (size_t)h[k] * 8, out_pool, st)) != cudaSuccess) {
+        if ((e = pool_malloc(&o, (size_t)h[k] * 8, out_pool, st)) != cudaSuccess) {
             for (int j = 0; j < k; ++j)
                 if (out[j]) cudaFreeAsync(out[j], st);
             for (int j = 0; j < 3; ++j) out[j] = nullptr;

@@ -183,6 +183,19 @@ cudaError_t launch_regions(const BatchDev &b, int64_t total_tris, uint32_t total
 size_t scan_scratch_words(uint64_t n);
 cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned long long *scratch,
                         uint32_t *status, cudaStream_t st);
+// Self-test of the scan's bounded look-back wait: the single-pass scan with
+// its tile counter started at 1, so tile 0 never publishes and every
+// look-back that reaches it gives up after spin_limit polls and records
+// kStatusScanTimeout in *status.  n must span at least 2 tiles; scratch holds
+// scan_stalled_scratch_words(n) words (the CTA that draws index `tiles` has no
+// tile and publishes one slot past the last).  out (n + 1 entries) receives
+// partial sums.  Synchronises st before the launch.
+size_t scan_stalled_scratch_words(uint64_t n);
+cudaError_t launch_scan_stalled(const uint32_t *in, uint32_t *out, uint64_t n, unsigned long long *scratch,
+                                uint32_t *status, int spin_limit, cudaStream_t st);
+// Stream-ordered allocation from one of a context's pools: the one place a
+// build allocates device memory (svo_debug_fail_alloc injects failures here).
+cudaError_t pool_malloc(void **p, size_t bytes, cudaMemPool_t pool, cudaStream_t st);
 // totals of every (mesh, level).
 cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st);
 cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st);

@@ -200,7 +200,7 @@ __device__ __forceinline__ void st_relaxed(unsigned long long *p, unsigned long 
 __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restrict__ in,
                                                        uint32_t *__restrict__ out, uint64_t n,
                                                        unsigned long long *__restrict__ scratch,
-                                                       uint32_t *__restrict__ status) {
+                                                       uint32_t *__restrict__ status, int spin_limit) {
     __shared__ uint32_t s_tile, s_prefix;
     __shared__ uint32_t s_warp[kScanThreads / 32];
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
@@ -248,7 +248,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan(const uint32_t *__restric
                 const unsigned long long s = q >= 0 ? ld_relaxed(st + q) : (2ull << 32);
                 const uint32_t flag = (uint32_t)(s >> 32);
                 if (__any_sync(0xFFFFFFFFu, flag == 0)) {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > spin_limit) {
                         if (lane == 0) atomicOr(status, kStatusScanTimeout);
                         break;
                     }
@@ -926,7 +926,24 @@ cudaError_t launch_scan(const uint32_t *in, uint32_t *out, uint64_t n, unsigned 
     cudaError_t e = cudaMemsetAsync(scratch, 0, scan_scratch_words(n) * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     if (tiles == 0) return cudaMemsetAsync(out, 0, sizeof(uint32_t), st);
-    k_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, scratch, status);
+    k_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, scratch, status, kSpinLimit);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+size_t scan_stalled_scratch_words(uint64_t n) { return scan_scratch_words(n) + 1; }
+
+cudaError_t launch_scan_stalled(const uint32_t *in, uint32_t *out, uint64_t n, unsigned long long *scratch,
+                                uint32_t *status, int spin_limit, cudaStream_t st) {
+    const uint64_t tiles = (n + kScanTile - 1) / kScanTile;
+    if (tiles < 2 || tiles > 0x7FFFFFFFull || spin_limit < 1) return cudaErrorInvalidValue;
+    cudaError_t e = cudaMemsetAsync(scratch, 0, scan_stalled_scratch_words(n) * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    // the tile counter starts at 1: tile 0 is never run and never publishes
+    const unsigned long long one = 1;
+    if ((e = cudaMemcpyAsync(scratch, &one, sizeof(one), cudaMemcpyHostToDevice, st)) != cudaSuccess) return e;
+    if ((e = cudaStreamSynchronize(st)) != cudaSuccess) return e;
+    k_scan<<<(unsigned)tiles, kScanThreads, 0, st>>>(in, out, n, scratch, status, spin_limit);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -8,10 +8,14 @@
 // svo_batch_emit for all of it) and publishes the results.  While one
 // worker's batch is on the GPU the others admit what arrived meanwhile and
 // launch on their own streams, so batches of different sizes overlap on the
-// device.  Admission reserves svo_estimate_bytes() per request; once a batch
-// is built the reservation becomes the exact bytes of the result, held until
-// the client releases it.
+// device.  Admission reserves svo_estimate_bytes() per request.  Once the
+// batch's counting phase knows each result's exact size, the batch keeps the
+// longest prefix whose exact needs fit the budget beside what other batches
+// hold and sends the rest back to the front of the queue with their exact
+// sizes; after emission a request holds the exact bytes of its result until
+// the client releases it.  Queued requests can be cancelled.
 #include <chrono>
+#include <algorithm>
 #include <condition_variable>
 #include <deque>
 #include <mutex>
@@ -29,6 +33,7 @@ struct svo_server {
         uint64_t ticket = 0;
         svo_mesh_desc desc{};
         uint64_t est = 0;   // bytes reserved at admission
+        uint64_t base = 0;  // the inputs + scratch part of est
         uint64_t held = 0;  // bytes reserved now
         std::chrono::steady_clock::time_point t_submit, t_start, t_done;
         bool done = false;
@@ -44,6 +49,7 @@ struct svo_server {
     std::unordered_map<uint64_t, Req *> reqs;
     uint64_t next_ticket = 1;
     uint64_t reserved = 0;
+    uint64_t peak_reserved = 0;
     int busy = 0;  // workers with a batch on the device
     bool stop = false;
     std::vector<std::thread> workers;
@@ -63,12 +69,44 @@ int server_fail(int code, const char *msg) {
 
 int max_res(const int r[3]) { return std::max(r[0], std::max(r[1], r[2])); }
 
+// Admission estimate: inputs + scratch of a res^3 grid (`base`) and the
+// outputs of 16*res^2 nodes (a closed surface spanning the grid).
+uint64_t estimate_parts(int64_t n_points, int64_t n_tris, const int res[3], uint32_t flags, uint64_t *base) {
+    uint64_t side = 1;
+    while (side < (uint64_t)max_res(res)) side *= 2;
+    const uint64_t nt = n_tris > 0 ? (uint64_t)n_tris : (uint64_t)std::max<int64_t>(n_points, 0) / 3;
+    const uint64_t inputs = 12 * (uint64_t)std::max<int64_t>(n_points, 0) + 12 * nt;
+    const uint64_t scratch = side * side * side / 7 + 32 * nt + (1u << 20);
+    const uint64_t nodes = 16 * side * side;
+    uint64_t per_node = sizeof(svo_node);
+    if (!(flags & SVO_FLAG_NO_VERT_EDGE)) per_node += 8 * sizeof(svo_vertex) + 12 * sizeof(svo_edge);
+    if (flags & SVO_FLAG_DEDUP) per_node += 8 * 4;
+    *base = inputs + scratch;
+    return inputs + scratch + nodes * per_node;
+}
+
+void reserve(svo_server *s, uint64_t add, uint64_t remove) {
+    s->reserved = s->reserved + add - remove;
+    s->peak_reserved = std::max(s->peak_reserved, s->reserved);
+}
+
 // The longest FIFO prefix that fits the budget; a request larger than the
 // whole budget runs alone when nothing else is reserved.
 bool admissible(const svo_server *s) {
     if (s->queue.empty()) return false;
     const uint64_t e = s->queue.front()->est;
     return s->reserved + e <= s->cfg.mem_budget || s->reserved == 0;
+}
+
+void publish(svo_server *s, svo_server::Req *r, svo_result *res, int status, uint64_t bytes,
+             Clock::time_point now) {
+    reserve(s, bytes, r->held);
+    r->held = bytes;
+    r->result = res;
+    r->status = status;
+    r->t_done = now;
+    r->done = true;
+    s->finished.push_back(r->ticket);
 }
 
 void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &take) {
@@ -80,11 +118,42 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
     std::vector<int> status(n, SVO_OK);
     std::vector<uint64_t> bytes(n, 0);
     svo_batch *b = nullptr;
+    int keep = n;  // take[0, keep) is built by this batch; the rest is requeued
     int rc = svo_batch_create(s->ctx, d.data(), n, s->cfg.flags, st, &b);
     if (rc == SVO_OK) {
-        rc = svo_batch_emit(b, 0, n, out.data(), status.data());
-        for (int i = 0; i < n; ++i)
-            if (status[i] == SVO_OK) bytes[i] = (uint64_t)svo_batch_mesh_output_bytes(b, i);
+        // Exact output sizes are known now.  Hold them instead of the
+        // estimates for the prefix that fits beside what others hold; send
+        // the rest back to the front of the queue with their exact sizes.
+        {
+            std::lock_guard<std::mutex> lk(s->mu);
+            uint64_t mine = 0;
+            for (svo_server::Req *r : take) mine += r->held;
+            const uint64_t others = s->reserved - mine;
+            uint64_t acc = 0, drop = 0;
+            keep = 0;
+            for (int i = 0; i < n; ++i) {
+                const int64_t ob = svo_batch_mesh_output_bytes(b, i);  // -1: this mesh failed counting
+                const uint64_t need = take[i]->base + (ob > 0 ? (uint64_t)ob : 0);
+                const bool fits = others + acc + need <= s->cfg.mem_budget || (others == 0 && i == 0);
+                drop += take[i]->held;
+                if (keep == i && fits) {
+                    acc += need;
+                    take[i]->held = need;
+                    ++keep;
+                } else {
+                    take[i]->est = need;
+                    take[i]->held = 0;
+                }
+            }
+            reserve(s, acc, drop);
+            for (int i = n - 1; i >= keep; --i) s->queue.push_front(take[i]);
+        }
+        if (keep < n) s->cv_work.notify_all();
+        if (keep > 0) {
+            rc = svo_batch_emit(b, 0, keep, out.data(), status.data());
+            for (int i = 0; i < keep; ++i)
+                if (status[i] == SVO_OK) bytes[i] = (uint64_t)svo_batch_mesh_output_bytes(b, i);
+        }
         svo_batch_free(b);
     } else {
         for (int i = 0; i < n; ++i) status[i] = rc;
@@ -92,21 +161,12 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
     {
         std::lock_guard<std::mutex> lk(s->mu);
         const auto now = Clock::now();
-        for (int i = 0; i < n; ++i) {
-            svo_server::Req *r = take[i];
-            s->reserved -= r->held;
-            r->held = bytes[i];
-            s->reserved += r->held;
-            r->result = out[i];
-            r->status = status[i];
-            r->t_done = now;
-            r->done = true;
-            s->finished.push_back(r->ticket);
-        }
-        s->batches += 1;
-        s->built += (uint64_t)n;
+        for (int i = 0; i < keep; ++i) publish(s, take[i], out[i], status[i], bytes[i], now);
+        if (keep > 0) s->batches += 1;
+        s->built += (uint64_t)keep;
         s->build_s += std::chrono::duration<double>(now - t0).count();
-        for (int i = 0; i < n; ++i) s->queue_s += std::chrono::duration<double>(take[i]->t_start - take[i]->t_submit).count();
+        for (int i = 0; i < keep; ++i)
+            s->queue_s += std::chrono::duration<double>(take[i]->t_start - take[i]->t_submit).count();
         --s->busy;
     }
     s->cv_done.notify_all();
@@ -128,7 +188,7 @@ void worker(svo_server *s, int w) {
             while (!s->queue.empty() && (int)take.size() < s->cfg.max_batch) {
                 svo_server::Req *r = s->queue.front();
                 if (s->reserved + r->est > s->cfg.mem_budget && !(s->reserved == 0 && take.empty())) break;
-                s->reserved += r->est;
+                reserve(s, r->est, 0);
                 r->held = r->est;
                 r->t_start = now;
                 take.push_back(r);
@@ -146,16 +206,8 @@ extern "C" {
 
 uint64_t svo_estimate_bytes(int64_t n_points, int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags) {
     const int r[3] = {res_x, res_y, res_z};
-    uint64_t side = 1;
-    while (side < (uint64_t)max_res(r)) side *= 2;
-    const uint64_t nt = n_tris > 0 ? (uint64_t)n_tris : (uint64_t)std::max<int64_t>(n_points, 0) / 3;
-    const uint64_t inputs = 12 * (uint64_t)std::max<int64_t>(n_points, 0) + 12 * nt;
-    const uint64_t scratch = side * side * side / 7 + 32 * nt + (1u << 20);
-    const uint64_t nodes = 16 * side * side;  // a closed surface spanning the grid
-    uint64_t per_node = sizeof(svo_node);
-    if (!(flags & SVO_FLAG_NO_VERT_EDGE)) per_node += 8 * sizeof(svo_vertex) + 12 * sizeof(svo_edge);
-    if (flags & SVO_FLAG_DEDUP) per_node += 8 * 4;
-    return inputs + scratch + nodes * per_node;
+    uint64_t base = 0;
+    return estimate_parts(n_points, n_tris, r, flags, &base);
 }
 
 int svo_server_create(svo_ctx *ctx, const svo_server_config *cfg, svo_server **out) {
@@ -190,8 +242,7 @@ int svo_server_submit(svo_server *s, const svo_mesh_desc *desc, uint64_t *ticket
     if (!s || !desc || !ticket) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
     auto *r = new svo_server::Req();
     r->desc = *desc;
-    r->est = svo_estimate_bytes(desc->n_points, desc->n_tris, desc->res[0], desc->res[1], desc->res[2],
-                                s->cfg.flags);
+    r->est = estimate_parts(desc->n_points, desc->n_tris, desc->res, s->cfg.flags, &r->base);
     r->t_submit = Clock::now();
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -260,12 +311,31 @@ int svo_server_release(svo_server *s, uint64_t ticket) {
                 s->finished.erase(f);
                 break;
             }
-        s->reserved -= r->held;
+        reserve(s, 0, r->held);
         res = r->result;
         s->reqs.erase(it);
         delete r;
     }
     svo_result_free(res);
+    s->cv_work.notify_all();
+    return SVO_OK;
+}
+
+int svo_server_cancel(svo_server *s, uint64_t ticket) {
+    if (!s) return server_fail(SVO_ERR_INVALID_ARGUMENT, "null server");
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        auto it = s->reqs.find(ticket);
+        if (it == s->reqs.end()) return server_fail(SVO_ERR_INVALID_ARGUMENT, "unknown ticket");
+        svo_server::Req *r = it->second;
+        auto q = std::find(s->queue.begin(), s->queue.end(), r);
+        if (q == s->queue.end())
+            return server_fail(SVO_ERR_INVALID_ARGUMENT, r->done ? "request already finished"
+                                                               : "request already building");
+        s->queue.erase(q);
+        publish(s, r, nullptr, SVO_ERR_CANCELLED, 0, Clock::now());
+    }
+    s->cv_done.notify_all();
     s->cv_work.notify_all();
     return SVO_OK;
 }
@@ -281,6 +351,7 @@ int svo_server_stats(const svo_server *s, svo_server_stats_t *out) {
     out->built = s->built;
     out->build_seconds = s->build_s;
     out->queue_seconds = s->queue_s;
+    out->peak_reserved_bytes = s->peak_reserved;
     return SVO_OK;
 }
 

@@ -26,6 +26,7 @@ ERR_PARSE = 7
 ERR_UNSUPPORTED = 8
 ERR_DEVICE_TIMEOUT = 9
 ERR_TIMEOUT = 10
+ERR_CANCELLED = 11
 
 FLAG_FULL_NEIGHBORS = 0x1
 FLAG_DEDUP = 0x2
@@ -85,7 +86,7 @@ class ServerConfig(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("queued", C.c_int64), ("busy_workers", C.c_int), ("reserved_bytes", C.c_uint64),
                 ("batches", C.c_uint64), ("built", C.c_uint64), ("build_seconds", C.c_double),
-                ("queue_seconds", C.c_double)]
+                ("queue_seconds", C.c_double), ("peak_reserved_bytes", C.c_uint64)]
 
 
 _lib = None
@@ -148,6 +149,11 @@ def lib() -> C.CDLL:
         L.svo_server_next.argtypes = [vp, i64, C.POINTER(C.c_uint64), C.POINTER(vp), C.POINTER(C.c_int),
                                       C.POINTER(C.c_double)]
         L.svo_server_stats.argtypes = [vp, C.POINTER(ServerStats)]
+        L.svo_server_cancel.argtypes = [vp, C.c_uint64]
+        L.svo_ctx_memory.argtypes = [vp, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]
+        L.svo_selftest_scan_timeout.argtypes = [vp, vp]
+        L.svo_debug_fail_alloc.argtypes = [i64]
+        L.svo_debug_fail_alloc.restype = i64
         L.svo_server_destroy.argtypes = [vp]
         L.svo_server_destroy.restype = None
         L.svo_ctx_device.argtypes = [vp, C.POINTER(C.c_int)]
@@ -237,6 +243,16 @@ class Context:
         except Exception:
             pass
 
+    def memory(self) -> tuple:
+        """(scratch bytes, result bytes) allocated from the context's pools now."""
+        a, b = C.c_uint64(), C.c_uint64()
+        _check(lib().svo_ctx_memory(self.handle, C.byref(a), C.byref(b)))
+        return a.value, b.value
+
+    def selftest_scan_timeout(self, stream: int = 0) -> int:
+        """Status of the scan self-test (ERR_DEVICE_TIMEOUT when the bounded wait works)."""
+        return int(lib().svo_selftest_scan_timeout(self.handle, stream or None))
+
     @property
     def tuning(self) -> tuple:
         """(serial_max, warp_max, split, inplace_max, serial_packed) of the voxelizer work split."""
@@ -291,6 +307,12 @@ class Context:
         return results, list(st), rc
 
 
+def debug_fail_alloc(n: int) -> int:
+    """svo_debug_fail_alloc: the n-th device allocation of a build from now on
+    fails (0 disarms); returns the countdown it replaces (> 0: not fired)."""
+    return int(lib().svo_debug_fail_alloc(int(n)))
+
+
 def estimate_bytes(n_points: int, n_tris: int, res, flags: int = 0) -> int:
     """svo_estimate_bytes: the server's admission estimate for one mesh."""
     return int(lib().svo_estimate_bytes(n_points, n_tris, *_res3(res), flags))
@@ -342,6 +364,10 @@ class Server:
     def release(self, ticket: int) -> None:
         _check(lib().svo_server_release(self._h, ticket))
         self._keep.pop(ticket, None)
+
+    def cancel(self, ticket: int) -> None:
+        """Withdraws a queued request (it finishes with ERR_CANCELLED)."""
+        _check(lib().svo_server_cancel(self._h, ticket))
 
     def stats(self) -> dict:
         s = ServerStats()

@@ -35,6 +35,7 @@ extern "C" {
 #define SVO_ERR_UNSUPPORTED 8
 #define SVO_ERR_DEVICE_TIMEOUT 9 /* a bounded device-side wait gave up */
 #define SVO_ERR_TIMEOUT 10       /* a host-side wait ran out (svo_server_wait) */
+#define SVO_ERR_CANCELLED 11     /* the request was cancelled before it was built (svo_server_cancel) */
 
 /* ---- build flags ---------------------------------------------------------- */
 /* Default (0): the reference's effective behaviour bit for bit, including its
@@ -95,6 +96,11 @@ int svo_ctx_device(const svo_ctx *ctx, int *device);
  * per-build scratch); builds then carve it without growing the pools.  The
  * memory stays with the context until svo_ctx_destroy. */
 int svo_ctx_reserve(svo_ctx *ctx, uint64_t result_bytes, uint64_t scratch_bytes, void *stream);
+/* Device bytes currently allocated from the context's two pools: per-build
+ * scratch and result arrays (0 and the size of the live results once every
+ * build has finished and its stream is idle).  No counterpart in the
+ * reference. */
+int svo_ctx_memory(const svo_ctx *ctx, uint64_t *scratch_used, uint64_t *result_used);
 
 /* Voxelizer work split: triangles whose grid bbox has at most serial_max
  * (<= 65536) voxels are tested row by row without culling, the rows of a
@@ -203,9 +209,13 @@ void svo_batch_free(svo_batch *b);
  * each, take the longest FIFO prefix of queued requests that fits mem_budget
  * (at most max_batch) and build it as one batch, while the other workers
  * admit later arrivals and overlap their batches on the device.  Admission
- * reserves svo_estimate_bytes() per request; once built, the reservation is
- * the exact size of the result until svo_server_release.  Mesh pointers
- * (host or device) must stay valid until the request is finished. */
+ * reserves svo_estimate_bytes() per request.  When a batch's counting phase
+ * has the exact result sizes, the batch builds the longest prefix of its
+ * requests that fits the budget beside the other reservations and puts the
+ * rest back at the front of the queue with their exact sizes (a request larger
+ * than the whole budget is built alone).  A built request holds the exact size
+ * of its result until svo_server_release.  Mesh pointers (host or device)
+ * must stay valid until the request is finished. */
 typedef struct svo_server svo_server;
 typedef struct svo_server_config {
     uint64_t mem_budget; /* device bytes for admitted requests and live results */
@@ -221,6 +231,7 @@ typedef struct svo_server_stats_t {
     uint64_t built;   /* requests built so far */
     double build_seconds; /* wall time of all batches (summed over workers) */
     double queue_seconds; /* time requests waited for admission (summed) */
+    uint64_t peak_reserved_bytes; /* most device bytes reserved at any time */
 } svo_server_stats_t;
 /* Device bytes admission reserves for a mesh: inputs, scratch of a res^3
  * grid and the outputs of 16*res^2 nodes (a closed surface spanning it). */
@@ -237,6 +248,11 @@ int svo_server_wait(svo_server *s, uint64_t ticket, int64_t timeout_us, svo_resu
 int svo_server_next(svo_server *s, int64_t timeout_us, uint64_t *ticket, svo_result **result, int *status,
                     double *latency_s);
 int svo_server_release(svo_server *s, uint64_t ticket);
+/* Withdraws a request that is still queued: it finishes at once with status
+ * SVO_ERR_CANCELLED and no result (reported by svo_server_wait/next, then
+ * released as usual).  A request already building or finished cannot be
+ * cancelled (SVO_ERR_INVALID_ARGUMENT). */
+int svo_server_cancel(svo_server *s, uint64_t ticket);
 int svo_server_stats(const svo_server *s, svo_server_stats_t *out);
 /* Finishes every queued request, then frees all results not yet released. */
 void svo_server_destroy(svo_server *s);
@@ -286,9 +302,10 @@ int svo_result_copy_keys(const svo_result *r, uint64_t *dst, int64_t cap);
  * CUDA events on the build stream: [0] first to last event (includes the
  * host round trip that sizes the outputs), [1] bounding cube, [2] voxelize,
  * [3] bitmap pyramid, [4] block-count scan, [5] level code lists,
- * [6] node/vertex/edge emission, [7] duplicate removal, [8] dedup keys.
- * Returns the number of entries (9), or 0 without timings.  No counterpart in
- * the reference (it has no instrumentation). */
+ * [6] node/vertex/edge emission, [7] duplicate removal, [8] dedup keys (on a
+ * stream of its own, concurrent with [6] and [7], so the stages need not add
+ * up to [0]).  Returns the number of entries (9), or 0 without timings.  No
+ * counterpart in the reference (it has no instrumentation). */
 int svo_result_timings(const svo_result *r, float *ms, int cap);
 
 /* Morton-keyed unique primitives (SVO_FLAG_DEDUP): kind 0 vertices, 1 edges,
@@ -310,6 +327,23 @@ int svo_write_voxels(const svo_result *r, const char *path);
  * keys[i], computed on the host (src/SVO.cu:766-775). */
 int svo_write_voxel_keys(const uint64_t *keys, int64_t n, const float origin[3], float width,
                          const char *path);
+
+/* ---- diagnostics and fault injection (no counterpart in the reference) ------
+ * The reference stops the process on any CUDA error (CUDA_CHECK and
+ * getLastCudaError call exit(), src/CUDAUtil.h:21-48); this library returns a
+ * status instead and keeps the context usable.  These two calls let a test
+ * provoke the two failures a build can meet without faulting a GPU. */
+/* Runs the single-pass scan that every build uses, over a small array, with
+ * its first tile never run: every look-back wait that reaches that tile gives
+ * up after its poll limit.  Returns SVO_ERR_DEVICE_TIMEOUT when the bounded
+ * wait ended the kernel as designed (any other status is a failure of the
+ * self-test); the context stays usable afterwards.  Synchronises `stream`. */
+int svo_selftest_scan_timeout(svo_ctx *ctx, void *stream);
+/* Process-wide: the n-th device allocation that a build makes from now on
+ * (1 = the next one) fails as out of memory; n <= 0 disarms.  Returns the
+ * countdown it replaces (> 0: the previous injection has not fired yet).  For
+ * tests of the SVO_ERR_OUT_OF_MEMORY paths. */
+int64_t svo_debug_fail_alloc(int64_t n);
 
 #ifdef __cplusplus
 }

@@ -88,6 +88,8 @@ def lib() -> C.CDLL:
         L.oracle_set_fp_sites.argtypes = [C.c_void_p, C.c_int]
         L.oracle_result_free.argtypes = [C.c_void_p]
         L.oracle_write_tree.argtypes = [C.c_void_p, C.c_char_p]
+        L.oracle_write_voxels.argtypes = [C.c_void_p, C.c_char_p]
+        L.oracle_write_tree_nodes.argtypes = [C.c_void_p, C.c_int64, C.c_char_p]
         _lib = L
     return _lib
 
@@ -230,6 +232,10 @@ class Result:
     def write_tree(self, path: str) -> None:
         _check(lib().oracle_write_tree(self._handle, path.encode()))
 
+    def write_voxels(self, path: str) -> None:
+        """writeVoxel as create() calls it: one cube per surface voxel."""
+        _check(lib().oracle_write_voxels(self._handle, path.encode()))
+
     def close(self) -> None:
         if self._handle:
             lib().oracle_result_free(self._handle)
@@ -240,6 +246,13 @@ class Result:
             self.close()
         except Exception:
             pass
+
+
+def write_tree_nodes(nodes: np.ndarray, path: str) -> None:
+    """writeTree's std::ofstream writer over a node array (168-byte records)."""
+    n = np.ascontiguousarray(nodes)
+    assert n.dtype.itemsize == NODE_DTYPE.itemsize
+    _check(lib().oracle_write_tree_nodes(n.ctypes.data, n.shape[0], path.encode()))
 
 
 def build_svo(points, tris, res, flags: int = 0, threads: int = 0) -> Result:

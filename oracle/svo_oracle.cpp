@@ -431,6 +431,7 @@ int voxelize(const float *points, const int32_t *tris, int64_t nt, const Grid &g
 
 struct oracle_result {
     int depth = 0;
+    int res[3] = {0, 0, 0};
     float bbox[9];
     std::vector<int64_t> level_counts;  // depthNumNodes + the top level
     std::vector<oracle_node> nodes;
@@ -1043,6 +1044,7 @@ int oracle_build(const float *points, int64_t n_points, const int32_t *tris, int
     oracle_result *r = new (std::nothrow) oracle_result();
     if (!r) return fail(ORACLE_ERR_OUT_OF_MEMORY, "alloc");
     std::memcpy(r->bbox, g.bbox, sizeof(g.bbox));
+    for (int a = 0; a < 3; ++a) r->res[a] = res[a];
     const int nth = nthreads_of(n_threads);
     rc = voxelize(points, tris, n_tris, g, strict, nth, r->keys);
     if (!rc) rc = build_levels(r->keys, g, strict, *r);
@@ -1080,10 +1082,15 @@ const uint64_t *oracle_result_dedup(const oracle_result *r, int kind) {
     return (kind >= 0 && kind < 3) ? r->dedup[kind].data() : nullptr;
 }
 
-// writeTree + write_cube (src/SVO.cu:737-753, src/IO.h:8-90): the same
+}  // extern "C"
+
+namespace {
+
+// write_cube (src/IO.h:23-90) over a list of cubes, with the same
 // std::ofstream insertions (default float format = "%.6g" of the value
 // widened to double; indices through Eigen::Vector2i, i.e. int).
-int oracle_write_tree(const oracle_result *r, const char *path) {
+template <class Cube>
+int write_cubes(const char *path, size_t n, Cube cube) {
     std::ofstream output(path, std::ios::out);
     if (!output) return fail(ORACLE_ERR_IO, std::string("cannot open ") + path);
     size_t faceBegIdx = 0;
@@ -1093,9 +1100,9 @@ int oracle_write_tree(const oracle_result *r, const char *path) {
     auto line = [&](size_t a, size_t b) {
         output << "l " << (int)a << " " << (int)b << std::endl;
     };
-    for (const oracle_node &n : r->nodes) {
-        const float *o = n.origin;
-        const float w = n.width;
+    for (size_t i = 0; i < n; ++i) {
+        float o[3], w;
+        cube(i, o, w);
         vtx(o[0] + 0.0f, o[1] + w, o[2] + w);        // v1
         vtx(o[0] + 0.0f, o[1] + 0.0f, o[2] + w);     // v2
         vtx(o[0] + 0.0f, o[1] + w, o[2] + 0.0f);     // v3
@@ -1121,6 +1128,41 @@ int oracle_write_tree(const oracle_result *r, const char *path) {
     }
     output.close();
     return output.fail() ? fail(ORACLE_ERR_IO, "write failed") : ORACLE_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+// writeTree (src/SVO.cu:737-753): one cube per node, at its origin and width.
+int oracle_write_tree(const oracle_result *r, const char *path) {
+    return write_cubes(path, r->nodes.size(), [&](size_t i, float o[3], float &w) {
+        for (int a = 0; a < 3; ++a) o[a] = r->nodes[i].origin[a];
+        w = r->nodes[i].width;
+    });
+}
+
+// writeTree's loop over any node array (the bench times it against the
+// product's writer on the same nodes).
+int oracle_write_tree_nodes(const oracle_node *nodes, int64_t n, const char *path) {
+    return write_cubes(path, (size_t)n, [&](size_t i, float o[3], float &w) {
+        for (int a = 0; a < 3; ++a) o[a] = nodes[i].origin[a];
+        w = nodes[i].width;
+    });
+}
+
+// writeVoxel (src/SVO.cu:755-777), as create() calls it on the surface voxels
+// (src/SVO.cu:411-419): width = unitNodeWidth = the voxel size along x, and
+// cube i at modelBBox.min + width * (x, y, z) of voxel i, host arithmetic
+// (each product and sum rounded; x86-64 code without FMA).
+int oracle_write_voxels(const oracle_result *r, const char *path) {
+    const float width = r->bbox[6] / (float)r->res[0];
+    return write_cubes(path, r->keys.size(), [&](size_t i, float o[3], float &w) {
+        uint32_t c[3];
+        demorton(r->keys[i], c[0], c[1], c[2]);
+        for (int a = 0; a < 3; ++a) o[a] = r->bbox[a] + width * (float)c[a];
+        w = width;
+    });
 }
 
 }  // extern "C"

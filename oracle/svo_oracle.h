@@ -14,6 +14,7 @@
  *                     meshVoxelize/surfaceVoxelize  src/SVO.cu:37-206
  *                     constructNodeAtrributes       src/SVO.cu:522-735
  *   oracle_write_tree SparseVoxelOctree::writeTree  src/SVO.cu:737-753
+ *   oracle_write_voxels SparseVoxelOctree::writeVoxel src/SVO.cu:755-777 (as called at :411-419)
  *                     write_cube                    src/IO.h:8-90
  *
  * Parity pinning: the Morton encoder/decoder and the neighbour/shared-corner
@@ -128,6 +129,8 @@ const uint64_t *oracle_result_dedup(const oracle_result *r, int kind);
 
 /* writeTree: writes <path> exactly as the reference's std::ofstream writer. */
 int oracle_write_tree(const oracle_result *r, const char *path);
+int oracle_write_voxels(const oracle_result *r, const char *path);
+int oracle_write_tree_nodes(const oracle_node *nodes, int64_t n, const char *path);
 
 const char *oracle_last_error(void);
 

@@ -109,3 +109,76 @@ def test_completion_order(gpu_ctx, svo_mod):
         srv.release(t)
     assert srv.next(timeout_us=1000) is None
     srv.close()
+
+
+def test_cancel_queued(gpu_ctx, svo_mod):
+    """A request still in the queue can be withdrawn: it finishes at once with
+    ERR_CANCELLED and no result; the others are built as if it never came; a
+    request already finished cannot be cancelled."""
+    from svo_b200 import meshgen
+
+    soup, _, _ = meshgen.torus_slivers(200_000)
+    small = _requests(2, seed=12, res_choices=(64,))
+    srv = svo_mod.Server(gpu_ctx, 40 << 30, workers=1, max_batch=1)
+    big = srv.submit(soup, None, 512)  # keeps the one worker busy while the rest queue up
+    t1 = srv.submit(*small[0])
+    t2 = srv.submit(*small[1])
+    srv.cancel(t2)
+    r, st, _ = srv.wait(t2)
+    assert st == svo_mod.ERR_CANCELLED and r is None
+    for t, m in ((big, (soup, None, 512)), (t1, small[0])):
+        r, st, _ = srv.wait(t)
+        assert st == 0
+        _same(r, gpu_ctx.build(*m))
+    with pytest.raises(svo_mod.SvoError) as e:
+        srv.cancel(t1)
+    assert e.value.code == svo_mod.ERR_INVALID_ARGUMENT
+    for t in (big, t1, t2):
+        srv.release(t)
+    s = srv.stats()
+    assert s["built"] == 2 and s["reserved_bytes"] == 0 and s["queued"] == 0
+    srv.close()
+
+
+def test_budget_holds_when_results_outgrow_estimates(gpu_ctx, svo_mod):
+    """A soup of 100k scattered slivers, whose octree is several times the
+    admission estimate, with a budget that holds one such result: the
+    estimates admit three requests into one batch, but once their exact sizes
+    are known only one is built at a time and the rest wait for memory; every
+    result is still correct and the reservations never exceed the budget."""
+    from svo_b200 import meshgen
+
+    soup = meshgen.slivers(100_000, np.random.default_rng(5)).reshape(-1, 3)
+    flags = svo_mod.FLAG_NO_VERT_EDGE
+    alone = gpu_ctx.build(soup, None, 256, flags)
+    exact = alone.num_nodes * 168 + alone.num_keys * 8
+    est = svo_mod.estimate_bytes(soup.shape[0], 0, 256, flags)
+    assert exact > 3 * est  # the estimate really is far too small
+    budget = int(1.5 * (exact + est))
+    srv = svo_mod.Server(gpu_ctx, budget, workers=2, max_batch=8, flags=flags)
+    tickets = [srv.submit(soup, None, 256) for _ in range(3)]
+    for t in tickets:
+        r, st, _ = srv.wait(t)
+        assert st == 0
+        assert r.nodes().tobytes() == alone.nodes().tobytes() and r.keys().tobytes() == alone.keys().tobytes()
+        srv.release(t)
+    s = srv.stats()
+    assert s["built"] == 3 and s["batches"] == 3 and s["reserved_bytes"] == 0
+    assert 0 < s["peak_reserved_bytes"] <= budget
+    srv.close()
+
+
+def test_served_results_match_oracle(gpu_ctx, svo_mod, oracle_mod):
+    """Served results against the oracle directly (not only against builds of
+    the same library): nodes, vertex/edge arrays and keys, bit for bit."""
+    from parity import assert_same
+
+    reqs = _requests(6, seed=13, res_choices=(32, 64, 128))
+    srv = svo_mod.Server(gpu_ctx, 8 << 30, workers=2, max_batch=4)
+    tickets = [srv.submit(*m) for m in reqs]
+    for t, (p, f, res) in zip(tickets, reqs):
+        r, st, _ = srv.wait(t)
+        assert st == 0
+        assert_same(r, oracle_mod.build_svo(p, f, res))
+        srv.release(t)
+    srv.close()
