@@ -34,7 +34,8 @@ struct svo_ctx {
     int num_sms = 148;
     cudaMemPool_t pool = nullptr;      // per-build scratch
     cudaMemPool_t out_pool = nullptr;  // result arrays, kept apart so scratch never splits their blocks
-    VoxTuning tune;
+    VoxTuning tune;                    // read and written under tune_mu
+    std::mutex tune_mu;
     std::mutex aux_mu;                 // builds on other threads take sets of their own
     std::vector<AuxStreams *> aux_free, aux_all;
 };
@@ -227,6 +228,7 @@ struct svo_batch {
     svo_ctx *ctx = nullptr;
     cudaStream_t st = nullptr;
     uint32_t flags = 0;
+    VoxTuning tune;                         // the voxelizer split this batch runs with
     std::vector<MeshHost> m;
     std::vector<int> live;                  // meshes with device work
     std::vector<void *> allocs;             // phase A buffers (pool)
@@ -447,7 +449,7 @@ int batch_phase_a(svo_batch *b) {
         SVO_TRY(cudaMemsetAsync(rflag, 0, std::max<uint32_t>(ctas, 1), st), "memset regions");
         SVO_TRY(cudaMemsetAsync(b->cnt, 0, blocks * 4, st), "memset counts");
         SVO_TRY(launch_regions(bd, (int64_t)tris, ctas, ctx->num_sms, st), "zero bitmaps");
-        SVO_TRY(launch_voxelize(bd, (int64_t)tris, strict, ctx->tune, big, big_cap, counters, ctx->num_sms, st,
+        SVO_TRY(launch_voxelize(bd, (int64_t)tris, strict, b->tune, big, big_cap, counters, ctx->num_sms, st,
                                 small),
                 "voxelize");
         tm.mark(StageTimer::kVox, st);
@@ -964,12 +966,19 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
     return first_err;
 }
 
+// tune: the voxelizer split to use (null: the context's, read once here).
 int batch_create(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, cudaStream_t st,
-                 svo_batch **out) {
+                 svo_batch **out, const VoxTuning *tune = nullptr) {
     svo_batch *b = new svo_batch();
     b->ctx = ctx;
     b->st = st;
     b->flags = flags;
+    if (tune) {
+        b->tune = *tune;
+    } else {
+        std::lock_guard<std::mutex> lk(ctx->tune_mu);
+        b->tune = ctx->tune;
+    }
     b->m.resize(n);
     for (int i = 0; i < n; ++i) {
         MeshHost &mh = b->m[i];
@@ -1085,6 +1094,7 @@ int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t) {
     if (t->warp_max == 0) return fail(SVO_ERR_INVALID_ARGUMENT, "warp_max must be positive");
     if (t->serial_max > (1u << 16)) return fail(SVO_ERR_INVALID_ARGUMENT, "serial_max must be <= 65536");
     if (t->serial_packed > 1) return fail(SVO_ERR_INVALID_ARGUMENT, "serial_packed must be 0 or 1");
+    std::lock_guard<std::mutex> lk(ctx->tune_mu);
     ctx->tune.serial_max = t->serial_max;
     ctx->tune.warp_max = t->warp_max;
     ctx->tune.split = t->split;
@@ -1095,6 +1105,7 @@ int svo_ctx_set_tuning(svo_ctx *ctx, const svo_tuning *t) {
 
 int svo_ctx_get_tuning(const svo_ctx *ctx, svo_tuning *t) {
     if (!ctx || !t) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
+    std::lock_guard<std::mutex> lk(const_cast<svo_ctx *>(ctx)->tune_mu);
     t->serial_max = ctx->tune.serial_max;
     t->warp_max = ctx->tune.warp_max;
     t->split = ctx->tune.split;
@@ -1223,15 +1234,20 @@ void svo_batch_free(svo_batch *b) { batch_destroy(b); }
 int svo_ctx_autotune(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, void *stream,
                      svo_tuning *best) {
     if (!ctx || !descs || n <= 0) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument or empty sample");
-    const VoxTuning saved = ctx->tune;
+    VoxTuning saved;
+    {
+        std::lock_guard<std::mutex> lk(ctx->tune_mu);
+        saved = ctx->tune;
+    }
     cudaStream_t st = static_cast<cudaStream_t>(stream);
-    // device ms of the voxelizer stage of the counting phase, best of 2 (after one untimed run)
+    // device ms of the voxelizer stage of the counting phase, best of 2 (after
+    // one untimed run); the candidate goes to the measured batches only, so
+    // builds on other threads keep the context's split meanwhile
     auto measure = [&](const VoxTuning &t, float &ms) -> int {
-        ctx->tune = t;
         ms = 1e30f;
         for (int rep = 0; rep < 3; ++rep) {
             svo_batch *b = nullptr;
-            const int rc = batch_create(ctx, descs, n, flags | SVO_FLAG_TIMINGS, st, &b);
+            const int rc = batch_create(ctx, descs, n, flags | SVO_FLAG_TIMINGS, st, &b, &t);
             if (rc != SVO_OK) {
                 batch_destroy(b);
                 return rc;
@@ -1274,11 +1290,11 @@ int svo_ctx_autotune(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t f
             win = t;
         }
     }
-    if (rc != SVO_OK) {
-        ctx->tune = saved;
-        return rc;
+    if (rc != SVO_OK) return rc;
+    {
+        std::lock_guard<std::mutex> lk(ctx->tune_mu);
+        ctx->tune = win;
     }
-    ctx->tune = win;
     if (best) {
         best->serial_max = win.serial_max;
         best->warp_max = win.warp_max;

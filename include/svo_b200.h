@@ -154,7 +154,9 @@ int svo_bbox_cube(const float *points, int64_t n_points, svo_aabb *out);
  * svo_node.morton_code then holds the low 32 bits, svo_result_copy_keys the
  * full codes).
  * `stream` is a cudaStream_t (NULL = the legacy default stream).  On success
- * *out owns the device arrays of the octree. */
+ * *out owns the device arrays of the octree.  The result remembers `stream`:
+ * svo_result_free releases its arrays there (stream-ordered) and the copy
+ * functions copy there, so the stream must outlive the result. */
 int svo_build(svo_ctx *ctx, const float *points, int64_t n_points, const int32_t *tris,
               int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags, void *stream,
               svo_result **out);
@@ -180,7 +182,9 @@ int svo_build_batch(svo_ctx *ctx, const svo_mesh_desc *descs, int n, void *strea
  * (a batch, as svo_batch_create) for a grid of candidate splits, times the
  * voxelizer stage on the device, installs the fastest split in the context
  * and returns it in *best (may be null).  Results do not depend on the split.
- * No counterpart in the reference. */
+ * Builds that other threads run on the context meanwhile keep its previous
+ * split (each build reads the split once, when it starts).  No counterpart in
+ * the reference. */
 int svo_ctx_autotune(svo_ctx *ctx, const svo_mesh_desc *descs, int n, uint32_t flags, void *stream,
                      svo_tuning *best);
 
