@@ -277,7 +277,6 @@ int batch_phase_a(svo_batch *b) {
     SVO_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
     cudaError_t err = cudaSuccess;
     // ---- validation and mesh data on the device ----
-    std::vector<int> idx_check;  // meshes whose device-side indices need a range check
     for (int i = 0; i < (int)b->m.size(); ++i) {
         MeshHost &mh = b->m[i];
         if (!mh.h_pts || mh.n_pts <= 0) {
@@ -301,18 +300,9 @@ int batch_phase_a(svo_batch *b) {
             mesh_error(mh, SVO_ERR_UNSUPPORTED, msg);
             continue;
         }
-        if (mh.h_tris && mh.n_tris > 0) {
-            mh.tris_on_device = is_device_ptr(mh.h_tris);
-            if (!mh.tris_on_device) {
-                bool ok = true;
-                for (int64_t k = 0; k < 3 * mh.n_tris && ok; ++k)
-                    ok = mh.h_tris[k] >= 0 && mh.h_tris[k] < mh.n_pts;
-                if (!ok) {
-                    mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "triangle index out of range");
-                    continue;
-                }
-            }
-        }
+        // face indices are checked on the device by the kernels that read them
+        // (kStatusBadIndex, reported with the level totals)
+        if (mh.h_tris && mh.n_tris > 0) mh.tris_on_device = is_device_ptr(mh.h_tris);
         if (is_device_ptr(mh.h_pts)) {
             mh.d_pts = mh.h_pts;
         } else {
@@ -324,7 +314,6 @@ int batch_phase_a(svo_batch *b) {
         if (mh.h_tris && mh.n_tris > 0) {
             if (mh.tris_on_device) {
                 mh.d_tris = mh.h_tris;
-                idx_check.push_back(i);
             } else {
                 int32_t *p = batch_alloc<int32_t>(b, (size_t)mh.n_tris * 3, err);
                 if (!p) return cuda_fail(err, "alloc tris");
@@ -340,37 +329,6 @@ int batch_phase_a(svo_batch *b) {
     const MetaLayout ml(n);
     b->meta = batch_alloc<unsigned char>(b, ml.bytes, err);
     if (!b->meta) return cuda_fail(err, "alloc meta");
-    if (!idx_check.empty()) {  // device-side index ranges, one read for all meshes
-        int32_t *imm = reinterpret_cast<int32_t *>(b->meta + ml.imm);
-        const int nj = (int)idx_check.size();
-        std::vector<IndexJob> jobs(nj);
-        std::vector<uint32_t> boff(nj + 1, 0);
-        for (int k = 0; k < nj; ++k) {
-            const MeshHost &mh = b->m[idx_check[k]];
-            jobs[k] = IndexJob{mh.d_tris, mh.n_tris * 3};
-            boff[k + 1] = boff[k] + index_blocks(jobs[k].n);
-        }
-        IndexJob *d_jobs = batch_alloc<IndexJob>(b, nj, err);
-        uint32_t *d_boff = d_jobs ? batch_alloc<uint32_t>(b, nj + 1, err) : nullptr;
-        if (!d_boff) return cuda_fail(err, "alloc index jobs");
-        SVO_TRY(upload(d_jobs, jobs, st), "upload");
-        SVO_TRY(upload(d_boff, boff, st), "upload");
-        SVO_TRY(launch_index_ranges(d_jobs, nj, d_boff, boff[nj], imm, st), "index range");
-        std::vector<int32_t> h(2 * idx_check.size());
-        SVO_TRY(cudaMemcpyAsync(h.data(), imm, h.size() * 4, cudaMemcpyDeviceToHost, st), "read");
-        SVO_TRY(cudaStreamSynchronize(st), "index check");
-        std::vector<int> keep;
-        for (size_t k = 0; k < idx_check.size(); ++k) {
-            MeshHost &mh = b->m[idx_check[k]];
-            if (h[2 * k] < 0 || h[2 * k + 1] >= mh.n_pts) mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "triangle index out of range");
-        }
-        for (int i : b->live)
-            if (b->m[i].status == SVO_OK) keep.push_back(i);
-        if ((int)keep.size() != n) {
-            b->live = keep;
-            return batch_phase_a(b);  // rebuild the tables without the rejected meshes
-        }
-    }
     // ---- layout ----
     uint64_t words = 0, blocks = 0, tris = 0;
     uint32_t ctas = 0, bblocks = 0;
@@ -487,6 +445,10 @@ int batch_phase_a(svo_batch *b) {
     // ---- level structure per mesh (src/SVO.cu:383-495) ----
     for (int k = 0; k < n; ++k) {
         MeshHost &mh = b->m[b->live[k]];
+        if (mh.gp.status & kStatusBadIndex) {
+            mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "triangle index out of range");
+            continue;
+        }
         if (mh.gp.status & kStatusNonFinite) {
             mesh_error(mh, SVO_ERR_INVALID_ARGUMENT, "non-finite vertex coordinate");
             continue;

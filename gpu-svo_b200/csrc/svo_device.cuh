@@ -109,7 +109,7 @@ struct GridParams {
     float origin[3];  // modelBBox.min
     float unit[3];    // unitVoxelSize
     float bbox[9];    // min, max, width
-    uint32_t status;  // bit 0: non-finite vertex
+    uint32_t status;  // kStatus* bits of this mesh
     uint32_t pad_;
 };
 
@@ -118,6 +118,7 @@ enum : uint32_t {
     kStatusNonFinite = 1u,
     kStatusBigOverflow = 2u,
     kStatusScanTimeout = 4u,
+    kStatusBadIndex = 8u,  // a triangle names a vertex outside the mesh (that triangle is skipped)
 };
 
 }  // namespace svo

@@ -497,6 +497,32 @@ __device__ __forceinline__ uint32_t brick_count(const Tri &t) {
            (uint32_t)((t.hi[2] >> 2) - (t.lo[2] >> 2) + 1);
 }
 
+// The vertices of an indexed triangle after checking its indices against the
+// mesh's n_pts vertices; false (nothing read) when one is outside.  Soups are
+// always in range.
+__device__ __forceinline__ bool load_tri_checked(const float *__restrict__ pts, const int32_t *__restrict__ tris,
+                                                 int64_t n_pts, int64_t t, float p[3][3]) {
+    if (tris) {
+        int64_t vi[3];
+#pragma unroll
+        for (int k = 0; k < 3; ++k) vi[k] = __ldg(tris + 3 * t + k);
+        if ((uint64_t)vi[0] >= (uint64_t)n_pts || (uint64_t)vi[1] >= (uint64_t)n_pts ||
+            (uint64_t)vi[2] >= (uint64_t)n_pts)
+            return false;
+#pragma unroll
+        for (int k = 0; k < 3; ++k)
+#pragma unroll
+            for (int a = 0; a < 3; ++a) p[k][a] = __ldg(pts + 3 * vi[k] + a);
+        return true;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k)
+#pragma unroll
+        for (int a = 0; a < 3; ++a) p[k][a] = __ldg(pts + 9 * t + 3 * k + a);
+    return true;
+}
+
+// The same for a triangle that k_voxelize has already checked.
 __device__ __forceinline__ void load_tri(const float *__restrict__ pts, const int32_t *__restrict__ tris,
                                          int64_t t, float p[3][3]) {
     if (tris) {
@@ -646,14 +672,16 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3)
             const MeshDev &md = bd.mesh[m];
             const GridParams g = *md.gp;
             float p[3][3];
-            load_tri(md.pts, md.tris, gid - (int64_t)bd.tri_off[m], p);
-            tri_setup<S>(g, md.res, p[0], p[1], p[2], t);
-            const uint64_t vol = (uint64_t)(t.hi[0] - t.lo[0] + 1) * (uint64_t)(t.hi[1] - t.lo[1] + 1) *
-                                 (uint64_t)(t.hi[2] - t.lo[2] + 1);
-            nb = brick_count(t);
-            tier = vol <= (uint64_t)tune.serial_max ? 0 : (INPLACE || nb <= tune.inplace_max) ? 1 : 2;
-            if (tier == 1 || tier == 0) {
+            if (load_tri_checked(md.pts, md.tris, md.n_pts, gid - (int64_t)bd.tri_off[m], p)) {
+                tri_setup<S>(g, md.res, p[0], p[1], p[2], t);
+                const uint64_t vol = (uint64_t)(t.hi[0] - t.lo[0] + 1) * (uint64_t)(t.hi[1] - t.lo[1] + 1) *
+                                     (uint64_t)(t.hi[2] - t.lo[2] + 1);
+                nb = brick_count(t);
+                tier = vol <= (uint64_t)tune.serial_max ? 0 : (INPLACE || nb <= tune.inplace_max) ? 1 : 2;
             } else {
+                atomicOr(&md.gp->status, kStatusBadIndex);  // tier stays -1: the triangle is skipped
+            }
+            if (tier == 2) {
                 const uint32_t eb = tune.warp_max;
                 const uint32_t ne = (nb + eb - 1) / eb;
                 const uint32_t at = atomicAdd(big_count, ne);
@@ -859,7 +887,7 @@ __global__ void __launch_bounds__(256) k_region_mark(BatchDev bd, int64_t total)
         if (!md.regions) continue;
         const GridParams g = *md.gp;
         float p[3][3];
-        load_tri(md.pts, md.tris, gid - (int64_t)bd.tri_off[m], p);
+        if (!load_tri_checked(md.pts, md.tris, md.n_pts, gid - (int64_t)bd.tri_off[m], p)) continue;  // k_voxelize reports it
         int lo[3], hi[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
