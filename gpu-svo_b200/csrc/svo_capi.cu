@@ -272,6 +272,7 @@ cudaError_t upload(T *dst, const std::vector<T> &src, cudaStream_t st) {
 // Phase A.  Returns SVO_OK when the batch itself works (individual meshes
 // may still carry an error status).
 int batch_phase_a(svo_batch *b) {
+    svo::host::TraceRange trace("svo: counting phase (voxelize, pyramid, scan)");
     svo_ctx *ctx = b->ctx;
     cudaStream_t st = b->st;
     SVO_TRY(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -539,6 +540,7 @@ constexpr uint64_t kOwnEmitNodes = SVO_OWN_EMIT_NODES;
 
 // Phase B for meshes [first, first + count).
 int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *status_out) {
+    svo::host::TraceRange trace("svo: emission wave (codes, nodes, vertices, edges, dedup)");
     svo_ctx *ctx = b->ctx;
     cudaStream_t st = b->st;
     const uint32_t flags = b->flags;
@@ -1344,6 +1346,7 @@ int svo_result_copy_dedup(const svo_result *r, int kind, uint64_t *dst, int64_t 
 }
 
 int svo_write_tree(const svo_result *r, const char *path) {
+    svo::host::TraceRange trace("svo: write tree .obj");
     if (!r || !path) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
     std::vector<svo_node> h(r->n_nodes);
     int rc = svo_result_copy_nodes(r, h.data(), (int64_t)h.size());

@@ -523,6 +523,7 @@ int dedup_fail(int code, const char *msg) {
 
 int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, const EmitParams &ep,
                 uint64_t n_out[3], uint64_t *out[3], int num_sms) {
+    svo::host::TraceRange trace("svo: dedup keys");
     for (int k = 0; k < 3; ++k) {
         n_out[k] = 0;
         out[k] = nullptr;

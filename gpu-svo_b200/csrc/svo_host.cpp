@@ -144,6 +144,7 @@ void svo_free_host(void *p) { std::free(p); }
 // separate threads and joined in file order; face indices are absolute, so
 // the result does not depend on the cut.
 int svo_load_obj(const char *path, float **points, int64_t *n_points, int32_t **tris, int64_t *n_tris) {
+    svo::host::TraceRange trace("svo: load OBJ");
     if (!path || !points || !n_points || !tris || !n_tris) return fail(SVO_ERR_INVALID_ARGUMENT, "null argument");
     FILE *f = std::fopen(path, "rb");
     if (!f) return fail(SVO_ERR_IO, std::string("cannot open ") + path);

@@ -2,11 +2,22 @@
 #pragma once
 #include <cstdint>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "svo_b200.h"
 
 namespace svo::host {
 
 void set_error(const char *msg);
+
+// An NVTX range over a scope: the library's stages appear by name in Nsight
+// Systems timelines (a no-op when no tool is attached).
+struct TraceRange {
+    explicit TraceRange(const char *name) { nvtxRangePushA(name); }
+    ~TraceRange() { nvtxRangePop(); }
+    TraceRange(const TraceRange &) = delete;
+    TraceRange &operator=(const TraceRange &) = delete;
+};
 
 // writeVoxel body (src/SVO.cu:755-777): one cube per surface voxel, origin =
 // min + width * (x, y, z) computed on the host (separately rounded).

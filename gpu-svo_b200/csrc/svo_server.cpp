@@ -110,6 +110,7 @@ void publish(svo_server *s, svo_server::Req *r, svo_result *res, int status, uin
 }
 
 void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &take) {
+    svo::host::TraceRange trace("svo_server: batch");
     const int n = (int)take.size();
     const auto t0 = Clock::now();
     std::vector<svo_mesh_desc> d(n);

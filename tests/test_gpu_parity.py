@@ -125,3 +125,49 @@ def test_errors(gpu_ctx, svo_mod):
     # the context stays usable after errors
     r = gpu_ctx.build(pts, np.array([[0, 1, 2]], np.int32), 8)
     assert r.depth == 4
+
+
+def _tiny_meshes(count: int):
+    """Meshes of 1 to 8 triangles on small grids (2 to 16 per axis): random,
+    lattice-aligned and zero-area triangles, and triangles clustered in one
+    corner of a bounding cube stretched by an unused vertex -- tiny ones give a
+    single surface voxel, larger ones a single top node in a non-zero octant,
+    the two inputs the reference has no defined build for."""
+    out = []
+    for seed in range(count):
+        rng = np.random.default_rng(1000 + seed)
+        n = 1 + seed % 8
+        kind = seed % 5
+        tris = np.arange(n * 3, dtype=np.int32).reshape(-1, 3)
+        if kind == 0:
+            v = rng.normal(size=(n * 3, 3))
+        elif kind == 1:
+            v = rng.integers(0, 5, size=(n * 3, 3)) / 4.0
+        elif kind == 2:  # repeated vertices: zero-area triangles
+            v = np.repeat(rng.normal(size=(n, 3)), 3, axis=0)
+        else:  # clustered near (1, 1, 1); the last vertex, at the origin, is used by no triangle
+            spread = 0.3 if kind == 3 else 1e-4
+            v = np.concatenate([1.0 - rng.uniform(0.0, spread, size=(n * 3, 3)), [[0.0, 0.0, 0.0]]])
+        res = (2, 3, 4, 5, 8, 16, 7)[seed % 7]
+        out.append((v.astype(np.float32), tris, res))
+    return out
+
+
+def test_tiny_meshes_exhaustive(gpu_ctx, oracle_mod, svo_mod):
+    """Every tiny mesh, built in one batch, against the oracle: the same
+    status, and where the build is defined, the same octree bit for bit."""
+    meshes = _tiny_meshes(336)
+    results, st, _ = gpu_ctx.build_batch(meshes)
+    seen = set()
+    for (v, f, res), r, s in zip(meshes, results, st):
+        try:
+            o = oracle_mod.build_svo(v, f, res)
+        except oracle_mod.OracleError as e:
+            assert s == e.code and r is None, (res, s, e.code)
+            seen.add(e.code)
+            continue
+        assert s == svo_mod.OK, (res, s)
+        assert_same(r, o)
+        seen.add(0)
+        r.close()
+    assert {0, svo_mod.ERR_DEGENERATE} <= seen
