@@ -20,6 +20,11 @@ value = triangles of all ranks / max over ranks of the device time.
 
 --impl reference times the CPU restatement of the reference's build
 (oracle/, all host threads) on a bounded sample of the same workload.
+
+On one GPU the default line also carries `batch256` and `serve`: short runs of
+the 256-mesh batch (against one plain build per mesh) and of the served
+Poisson stream (p50/p99 latency against the plain per-request path), measured
+after the headline's timed region.
 """
 from __future__ import annotations
 
@@ -65,6 +70,8 @@ def parse_args():
     ap.add_argument("--res", type=int, default=0, help="override the workload's resolution")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="heightfield: skip the short batched and served runs reported beside the headline")
     ap.add_argument("--tune", type=int, default=1, help="single-mesh workloads: autotune the voxelizer split first")
     ap.add_argument("--tuning", default="", help="single-mesh workloads: use this split instead "
                     "(serial_max,warp_max,split,inplace_max,serial_packed)")
@@ -501,8 +508,8 @@ def run_ours(args, rank: int, world: int):
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
             "gpu_launches": launches, "writer": writer,
         }
-        print(json.dumps(line), flush=True)
     ctx.close()
+    return line if rank == 0 else None
 
 
 def result_digest(r) -> str:
@@ -695,8 +702,8 @@ def run_batch(args, rank: int, world: int):
                          "launch_ms": emit_ms},
             "cpu_baseline": cpu, "clocks": clocks.summary(), "gpu_launches": launches,
         }
-        print(json.dumps(line), flush=True)
     ctx.close()
+    return line if rank == 0 else None
 
 
 def run_serve(args, rank: int, world: int):
@@ -783,7 +790,25 @@ def run_serve(args, rank: int, world: int):
             "rates": out, "e2e": None, "roofline": None, "cpu_baseline": None, "clocks": clocks.summary(),
             "gpu_launches": launches,
         }
-        print(json.dumps(line), flush=True)
+        return line
+    return None
+
+
+def extras(args, rank: int, world: int) -> dict:
+    """Short runs of the batched (256 meshes) and served (Poisson stream)
+    workloads beside the headline build, outside its timed region: each with
+    its own warm-up, CUDA-event or server-clock timing and clock samples."""
+    import copy
+
+    b = copy.copy(args)
+    b.steps, b.warmup, b.no_cpu, b.flags = 3, 2, True, -1
+    batch = run_batch(b, rank, world)
+    sv = copy.copy(args)
+    sv.rates, sv.window, sv.flags = "500,2000", 0.5, -1
+    serve = run_serve(sv, rank, world)
+    keep_b = ("value", "unit", "ms_per_step", "plain", "batch_over_plain", "batch_equals_plain", "config", "clocks")
+    return {"batch256": {k: batch[k] for k in keep_b} if batch else None,
+            "serve": {k: serve[k] for k in ("rates", "config", "clocks")} if serve else None}
 
 
 def main():
@@ -792,12 +817,17 @@ def main():
     try:
         if args.impl == "reference":
             run_reference(args, rank)
-        elif args.workload == "batch256":
-            run_batch(args, rank, world)
+            return
+        if args.workload == "batch256":
+            line = run_batch(args, rank, world)
         elif args.workload == "serve":
-            run_serve(args, rank, world)
+            line = run_serve(args, rank, world)
         else:
-            run_ours(args, rank, world)
+            line = run_ours(args, rank, world)
+            if line is not None and world == 1 and args.workload == "heightfield" and not args.no_extras:
+                line.update(extras(args, rank, world))
+        if line is not None:
+            print(json.dumps(line), flush=True)
     finally:
         dist_done()
 
