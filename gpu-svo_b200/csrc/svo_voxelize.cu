@@ -236,7 +236,6 @@ struct Row {
     float inner;      // tail of n.dot(p)
     float xyb[3];     // XY: b * p.y
     float zxp[3];     // ZX: a * p.z
-    float pz;
     uint64_t syz;     // Morton bits of y and z
 };
 
@@ -253,7 +252,6 @@ __device__ __forceinline__ bool row_prep(const Tri &t, const GridParams &g, int 
         r.xyb[k] = __fmul_rn(t.eb[k], py);
         r.zxp[k] = __fmul_rn(t.ea[6 + k], pz);
     }
-    r.pz = pz;
     r.syz = (spread3((uint32_t)y) << 1) | (spread3((uint32_t)z) << 2);
     return true;
 }
@@ -267,10 +265,8 @@ __device__ __forceinline__ bool voxel_test(const Tri &t, const GridParams &g, co
     for (int k = 0; k < 3; ++k) {
         const float f = S ? __fadd_rn(__fmul_rn(t.ea[k], px), r.xyb[k]) : __fmaf_rn(t.ea[k], px, r.xyb[k]);
         ok &= !(__fadd_rn(f, t.ed[k]) < 0.0f);
-        // ZX tests 0 and 1 fuse b*p.x (a*p.z is loop-invariant), test 2 fuses a*p.z
-        const float h = S ? __fadd_rn(r.zxp[k], __fmul_rn(t.eb[6 + k], px))
-                          : (k < 2 ? __fmaf_rn(t.eb[6 + k], px, r.zxp[k])
-                                   : __fmaf_rn(t.ea[6 + k], r.pz, __fmul_rn(t.eb[6 + k], px)));
+        // the ZX tests fuse b*p.x (a*p.z is loop-invariant, hoisted out of the x loop)
+        const float h = S ? __fadd_rn(r.zxp[k], __fmul_rn(t.eb[6 + k], px)) : __fmaf_rn(t.eb[6 + k], px, r.zxp[k]);
         ok &= !(__fadd_rn(h, t.ed[6 + k]) < 0.0f);
     }
     return ok;
@@ -320,8 +316,7 @@ __device__ __forceinline__ bool voxel_pass(const Tri &t, const GridParams &g, in
     for (int k = 0; k < 3; ++k) {
         ok &= !(__fadd_rn(Fp<S>::dot2(t.ea[k], t.eb[k], px, py), t.ed[k]) < 0.0f);
         ok &= !(__fadd_rn(Fp<S>::dot2(t.ea[3 + k], t.eb[3 + k], py, pz), t.ed[3 + k]) < 0.0f);
-        const float zx = k < 2 ? Fp<S>::dot2_late(t.ea[6 + k], t.eb[6 + k], pz, px)
-                               : Fp<S>::dot2(t.ea[6 + k], t.eb[6 + k], pz, px);
+        const float zx = Fp<S>::dot2_late(t.ea[6 + k], t.eb[6 + k], pz, px);
         ok &= !(__fadd_rn(zx, t.ed[6 + k]) < 0.0f);
     }
     return ok;
@@ -346,7 +341,7 @@ __device__ __forceinline__ bool brick_reject(const Tri &t, const GridParams &g, 
             const float a = t.ea[3 * p + k], b = t.eb[3 * p + k];
             const float pi = a >= 0.0f ? ph[i] : pl[i];
             const float pj = b >= 0.0f ? ph[j] : pl[j];
-            const float f = (p == 2 && k < 2) ? Fp<S>::dot2_late(a, b, pi, pj) : Fp<S>::dot2(a, b, pi, pj);
+            const float f = p == 2 ? Fp<S>::dot2_late(a, b, pi, pj) : Fp<S>::dot2(a, b, pi, pj);
             if (__fadd_rn(f, t.ed[3 * p + k]) < 0.0f) return true;
         }
     }

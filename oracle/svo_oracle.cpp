@@ -128,25 +128,28 @@ inline void demorton(uint64_t c, uint32_t &x, uint32_t &y, uint32_t &z) {
 // "reference" mode below states which product becomes the FMA: the left
 // operand of the add, the minuend of the sub -- except inside the voxel loop,
 // where a product that does not depend on the loop's x is hoisted first and
-// the other one is fused (dot2_late).  A GPU probe test checks this against
-// nvcc's own contraction of the same expressions in the same loop structure.  "strict" mode
-// rounds every operation (what a non-contracting compiler would produce).
+// the other one is fused.  The reference's own build pins the pattern (its
+// recorded voxels, nodes and arrays, tests/test_ref_pins.py); a GPU probe test
+// checks the same machinery against nvcc on restated expressions.  "strict"
+// mode rounds every operation (what a non-contracting compiler would produce).
 // ---------------------------------------------------------------------------
 namespace fp {
 // Contraction sites of the reference's arithmetic.  Choice per site: 0 fuse
 // the first product of the sum, 1 fuse the second, 2 no fusion.  Strict mode
-// never fuses.  The defaults are the pattern nvcc 12.9 produces for the
-// reference's expressions in their loop structure (tests/fp_probe.cu):
-// everything fuses its first product except the inner sum of the squared
-// norm (c1*c1 + c2*c2 fuses c2*c2) and the first two ZX edge tests in the
-// voxel loop (a*p.z is hoisted out of the x loop, b*p.x is fused); the third
-// ZX test fuses a*p.z.  oracle_set_fp_sites changes them (used only to search
-// for the pattern).
+// never fuses.  The defaults are the pattern of the reference's own build
+// (src/SVO.cu compiled by nvcc 12.9 for sm_100a; its surface voxels are
+// recorded in tests/golden/ref_pins.json and ref_voxels.npz): everything
+// fuses its first product except the inner sum of the squared norm
+// (c1*c1 + c2*c2 fuses c2*c2) and the three ZX edge tests in the voxel loop
+// (a*p.z does not vary with x and is hoisted out of the x loop; b*p.x is
+// fused).  oracle_set_fp_sites changes them (used to search for the pattern,
+// and by the probe test, whose restated loop nvcc fuses differently in the
+// third ZX test).
 enum Site {
     kCross, kSqInner, kSqOuter, kD12Inner, kD12Outer, kDEdge, kPlaneInner, kPlaneOuter,
     kLoopXY, kLoopYZ = kLoopXY + 3, kLoopZX = kLoopYZ + 3, kNumSites = kLoopZX + 3
 };
-int g_site[kNumSites] = {0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 0};
+int g_site[kNumSites] = {0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1};
 
 inline float dot2s(int site, bool strict, float a0, float a1, float b0, float b1) {
     const int c = strict ? 2 : g_site[site];

@@ -7,7 +7,7 @@ tests/refcases.py (needs a CUDA GPU) and writes
   <out>/ref_pins.json   per case: depth, counts, depthNumNodes, bounding cube,
                         SHA-256 of the node / vertex / edge / voxel arrays and
                         of the tree .obj, and the reference's own timings
-  <out>/ref_voxels.npz  the voxel code lists of the cases of at most 2^20 voxels
+  <out>/ref_voxels.npz  the voxel code lists of the cases of at most 2^17 voxels
 and checks the reference's CLI (oracle/_ref/ref_main, main.cpp) on the bunny at
 its default resolution against the harness's tree file; its NDEBUG build
 (oracle/_ref/ref_main_ndebug) records the surface-voxel file writeVoxel writes.
@@ -111,7 +111,7 @@ def main():
                 with open(path, "rb") as fh:
                     entry["sha256"]["tree_obj"] = hashlib.sha256(fh.read()).hexdigest()
                 entry["tree_obj_bytes"] = os.path.getsize(path)
-            if voxels.size <= (1 << 20):
+            if voxels.size <= (1 << 17):
                 vox[name] = voxels
             pins[name] = entry
             print(f"{name}: depth {meta['depth']}, {meta['num_nodes']} nodes, {meta['num_voxels']} voxels, "

@@ -1,15 +1,19 @@
-"""Pins the floating-point model behind the voxel test and node origins.
+"""Checks the oracle's floating-point machinery against nvcc.
 
 The reference's arithmetic is Eigen 3.4 compiled by nvcc with its default
 --fmad=true; which products nvcc fuses into FMAs is not visible in the source
 and depends on context (loop-invariant products are hoisted before fusion).
-tests/fp_probe.cu restates the reference's triangle setup and voxel loop in
-plain float code with Eigen's evaluation order and the reference's statement
-and loop structure; built with default contraction it must agree bit for bit
-with the oracle's default model, and built with --fmad=false with the
-oracle's strict model -- on small shapes, on the setup values and on the
-complete voxel test, including lattice-aligned triangles where many tests are
-decided by the last bit.
+The pattern itself is pinned by the reference's own build
+(tests/test_ref_pins.py).  Here tests/fp_probe.cu restates the triangle setup
+and voxel loop in plain float code with Eigen's evaluation order; built with
+default contraction it must agree bit for bit with the oracle's contraction
+model, and built with --fmad=false with the oracle's strict model -- on small
+shapes, on the setup values and on the complete voxel test, including
+lattice-aligned triangles where many tests are decided by the last bit.  In
+the probe's restated loop nvcc fuses the third ZX edge test's z product
+(a*p.z) where the reference's own loop fuses its x product; the voxel test is
+compared under the probe's pattern (PROBE_SITES), everything else under the
+reference's.
 """
 import ctypes as C
 import os
@@ -21,6 +25,11 @@ import pytest
 from conftest import ROOT
 
 pytestmark = pytest.mark.gpu
+
+# the oracle's contraction sites as nvcc fuses them in the probe's loop: the
+# reference's pattern with the third ZX test fusing its first product
+PROBE_SITES = [0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 0]
+REFERENCE_SITES = [0, 1, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 0, 1, 1, 1]
 
 
 @pytest.fixture(scope="module")
@@ -85,7 +94,11 @@ def test_voxel_predicate(probes, oracle_mod, aligned, seed):
     x = _voxel_cases(np.random.default_rng(seed), 300_000, aligned)
     fused = _run(probes["fmad"], 5, x, 14, 1)
     plain = _run(probes["nofmad"], 5, x, 14, 1)
-    ref = oracle_mod.fp_eval(5, False, x)
+    oracle_mod.set_fp_sites(PROBE_SITES)
+    try:
+        ref = oracle_mod.fp_eval(5, False, x)
+    finally:
+        oracle_mod.set_fp_sites(REFERENCE_SITES)
     strict = oracle_mod.fp_eval(5, True, x)
     assert 0.05 < ref.mean() < 0.95
     assert np.array_equal(fused, ref), int((fused != ref).sum())
