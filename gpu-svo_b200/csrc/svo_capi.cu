@@ -498,10 +498,15 @@ AuxStreams *aux_acquire(svo_ctx *ctx) {
         ctx->aux_free.pop_back();
         return a;
     }
+    // The highest stream priority: when a wave's dedup runs beside its
+    // emission, the block scheduler places the dedup kernels' CTAs ahead of
+    // the emission grid's pending ones instead of after all of them.
+    int least = 0, greatest = 0;
+    cudaDeviceGetStreamPriorityRange(&least, &greatest);
     auto *a = new AuxStreams();
     bool ok = cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming) == cudaSuccess;
     for (int i = 0; i < AuxStreams::kCount && ok; ++i)
-        ok = cudaStreamCreateWithFlags(&a->s[i], cudaStreamNonBlocking) == cudaSuccess &&
+        ok = cudaStreamCreateWithPriority(&a->s[i], cudaStreamNonBlocking, greatest) == cudaSuccess &&
              cudaEventCreateWithFlags(&a->join[i], cudaEventDisableTiming) == cudaSuccess;
     if (!ok) {
         cudaGetLastError();
@@ -806,6 +811,9 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                       "emit");
             }
             tm.mark(StageTimer::kEmit, st);
+            // the top codes, gathered after the emission
+            k_gather_top<<<(n + 127) / 128, 128, 0, st>>>(d_top_ptr, n, top);
+            count_launches(1);
             // Dedup of every mesh on the forked stream (its host-side waits
             // overlap the emission running on the GPU); statuses are applied
             // after the emission's own checks.
@@ -821,8 +829,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 }
                 tm.mark(StageTimer::kDedup, ds);
             }
-            k_gather_top<<<(n + 127) / 128, 128, 0, st>>>(d_top_ptr, n, top);
-            count_launches(1);
+            // read back the top codes and duplicate counts (pageable copies:
+            // these wait for the emission, so they come after the dedup launches)
             std::vector<uint64_t> h_top(n);
             std::vector<unsigned long long> h_dups(2 * n);
             check(cudaMemcpyAsync(h_top.data(), top, 8 * (size_t)n, cudaMemcpyDeviceToHost, st), "read top");
