@@ -329,10 +329,52 @@ def run_reference(args, rank: int):
         "config": {"workload": wname, "triangles": nt, "resolution": res},
         "cpu_baseline": {"value": value, "unit": "tris/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "tris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": "the reference has no CPU build path and cannot be built here (Eigen 3.4 is fetched at "
-                "configure time); this times the CPU restatement of its algorithm (oracle/)",
+        "note": "the reference has no CPU build path (its build is CUDA); this times the CPU restatement "
+                "of its algorithm (oracle/) on the host cores",
+        "reference_cuda": reference_cuda_build(),
     }
     print(json.dumps(line), flush=True)
+
+
+# The input on which the reference's own CUDA build is timed beside ours: every
+# 16th triangle of the torus + sliver soup at resolution 512 (within the
+# reference's 32-bit Morton codes), as an OBJ file both programs read.
+REF_CUDA_INPUT = ("torus_slivers_every16_res512", 16, 512)
+
+
+def write_ref_cuda_input(directory: str) -> str:
+    from svo_b200 import meshgen
+
+    soup, _, _ = meshgen.torus_slivers()
+    path = os.path.join(directory, "torus_slivers_every16.obj")
+    meshgen.write_obj(path, soup.reshape(-1, 3, 3)[:: REF_CUDA_INPUT[1]].reshape(-1, 3), None)
+    return path
+
+
+def reference_cuda_build():
+    """GPU-SVO's own CUDA build (its unmodified src/SVO.cu, compiled for
+    sm_100a into oracle/_ref/ref_dump where the reference tree was present) on
+    REF_CUDA_INPUT, on this GPU: the wall time of SparseVoxelOctree::create()
+    -- host triangle gather, device build, copies of the octree back to the
+    host -- best of 2.  None when the binary is absent."""
+    import tempfile
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_dump")
+    if not os.path.exists(exe):
+        return None
+    with tempfile.TemporaryDirectory() as td:
+        obj = write_ref_cuda_input(td)
+        runs = []
+        for _ in range(2):
+            r = subprocess.run([exe, obj, str(REF_CUDA_INPUT[2]), td, "ref"], stdout=subprocess.DEVNULL,
+                               stderr=subprocess.PIPE, text=True)
+            if r.returncode != 0:
+                return {"error": r.stderr[-300:]}
+            runs.append(json.load(open(os.path.join(td, "meta.json"))))
+    best = min(runs, key=lambda m: m["create_ms"])
+    return {"workload": REF_CUDA_INPUT[0], "create_ms": best["create_ms"], "load_ms": best["load_ms"],
+            "voxelize_ms": best["voxelize_ms"], "nodes": best["num_nodes"],
+            "what": "SparseVoxelOctree::create() wall time of the reference's own build on this GPU"}
 
 
 # ---------------------------------------------------------------------------
@@ -486,6 +528,10 @@ def run_ours(args, rank: int, world: int):
         cpu = {"value": stris.shape[0] / dt, "unit": "tris/s", "cores": threads, "kind": "port",
                "sample": cpu_sample_text(stride, wname, stris.shape[0], res, bflags) + "; best of 2 oracle builds"}
 
+    same_input = None
+    if rank == 0 and world == 1 and not args.no_extras:
+        same_input = ours_on_ref_cuda_input(ctx, sid)
+
     writer = None
     if rank == 0 and world == 1 and not args.no_cpu:
         import tempfile
@@ -506,10 +552,45 @@ def run_ours(args, rank: int, world: int):
                        "tuning": dict(zip(TUNING_KEYS, tuning)), **info},
             "nodes_per_s": nodes_per_s,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
-            "gpu_launches": launches, "writer": writer,
+            "gpu_launches": launches, "writer": writer, "ref_cuda_input": same_input,
         }
     ctx.close()
     return line if rank == 0 else None
+
+
+def ours_on_ref_cuda_input(ctx, sid: int) -> dict:
+    """This library on the input the reference arm times the reference's own
+    CUDA build on: from the host arrays of the loaded OBJ to the octree (nodes,
+    vertex/edge arrays) back in host memory, like create(); best of 5 after a
+    warm-up, host wall clock."""
+    import tempfile
+
+    import torch
+
+    import svo_b200 as S
+
+    with tempfile.TemporaryDirectory() as td:
+        pts, tris = S.load_obj(write_ref_cuda_input(td))
+    res = REF_CUDA_INPUT[2]
+    lib = S.lib()
+
+    def once():
+        torch.cuda.synchronize()
+        t = time.perf_counter()
+        r = ctx.build(pts, tris, res, 0, sid)
+        bufs = (np.empty(r.num_nodes, S.NODE_DTYPE), np.empty(r.num_vertices, S.VERTEX_DTYPE),
+                np.empty(r.num_edges, S.EDGE_DTYPE))
+        for fn, b in zip((lib.svo_result_copy_nodes, lib.svo_result_copy_vertices, lib.svo_result_copy_edges), bufs):
+            S._check(fn(r.handle, b.ctypes.data, b.shape[0]))
+        dt = time.perf_counter() - t
+        n = r.num_nodes
+        r.close()
+        return dt, n
+
+    once()
+    best = min(once() for _ in range(5))
+    return {"workload": REF_CUDA_INPUT[0], "e2e_ms": 1e3 * best[0], "nodes": best[1],
+            "what": "svo_build from host arrays + node/vertex/edge copies to host, wall time"}
 
 
 def result_digest(r) -> str:
