@@ -826,7 +826,10 @@ def run_serve(args, rank: int, world: int):
         th.start()
         lat = []
         for _ in range(len(reqs)):  # completion order: each result released as soon as it is built
-            t, r, st, l = srv.next()
+            got = srv.next(timeout_us=300_000_000)
+            if got is None:
+                raise RuntimeError("a served request was not built within 300 s")
+            t, r, st, l = got
             if st != 0:
                 raise RuntimeError(f"request {t} failed: {st}")
             lat.append(l)

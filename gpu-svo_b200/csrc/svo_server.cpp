@@ -43,7 +43,9 @@ struct svo_server {
     svo_ctx *ctx = nullptr;
     svo_server_config cfg{};
     std::mutex mu;
-    std::condition_variable cv_work, cv_done;
+    std::condition_variable cv_work, cv_done, cv_decide;
+    uint64_t admitted_batches = 0;  // sequence number of the next batch admitted
+    uint64_t decided_batches = 0;   // batches whose keep/requeue decision is made
     std::deque<Req *> queue;
     std::deque<uint64_t> finished;  // tickets in completion order, not yet taken by svo_server_next
     std::unordered_map<uint64_t, Req *> reqs;
@@ -109,7 +111,13 @@ void publish(svo_server *s, svo_server::Req *r, svo_result *res, int status, uin
     s->finished.push_back(r->ticket);
 }
 
-void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &take) {
+// seq: the batch's admission sequence number.  Batches count concurrently but
+// make their keep/requeue decisions in admission order, so memory goes to
+// requests first come, first served: a younger request is never kept while
+// an older one, still counting, is sent back for lack of room (a client
+// waiting for the older one while holding the younger result would wait
+// forever).
+void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &take, uint64_t seq) {
     svo::host::TraceRange trace("svo_server: batch");
     const int n = (int)take.size();
     const auto t0 = Clock::now();
@@ -121,12 +129,17 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
     svo_batch *b = nullptr;
     int keep = n;  // take[0, keep) is built by this batch; the rest is requeued
     int rc = svo_batch_create(s->ctx, d.data(), n, s->cfg.flags, st, &b);
+    auto decided = [&]() {  // under s->mu
+        ++s->decided_batches;
+        s->cv_decide.notify_all();
+    };
     if (rc == SVO_OK) {
         // Exact output sizes are known now.  Hold them instead of the
         // estimates for the prefix that fits beside what others hold; send
         // the rest back to the front of the queue with their exact sizes.
         {
-            std::lock_guard<std::mutex> lk(s->mu);
+            std::unique_lock<std::mutex> lk(s->mu);
+            s->cv_decide.wait(lk, [&] { return s->decided_batches == seq; });
             uint64_t mine = 0;
             for (svo_server::Req *r : take) mine += r->held;
             const uint64_t others = s->reserved - mine;
@@ -148,6 +161,7 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
             }
             reserve(s, acc, drop);
             for (int i = n - 1; i >= keep; --i) s->queue.push_front(take[i]);
+            decided();
         }
         if (keep < n) s->cv_work.notify_all();
         if (keep > 0) {
@@ -158,6 +172,9 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
         svo_batch_free(b);
     } else {
         for (int i = 0; i < n; ++i) status[i] = rc;
+        std::unique_lock<std::mutex> lk(s->mu);
+        s->cv_decide.wait(lk, [&] { return s->decided_batches == seq; });
+        decided();
     }
     {
         std::lock_guard<std::mutex> lk(s->mu);
@@ -181,6 +198,7 @@ void worker(svo_server *s, int w) {
     cudaStream_t st = s->streams[w];
     for (;;) {
         std::vector<svo_server::Req *> take;
+        uint64_t seq = 0;
         {
             std::unique_lock<std::mutex> lk(s->mu);
             s->cv_work.wait(lk, [&] { return admissible(s) || (s->stop && s->queue.empty()); });
@@ -196,8 +214,9 @@ void worker(svo_server *s, int w) {
                 s->queue.pop_front();
             }
             ++s->busy;
+            seq = s->admitted_batches++;
         }
-        run_batch(s, st, take);
+        run_batch(s, st, take, seq);
     }
 }
 
@@ -361,6 +380,16 @@ void svo_server_destroy(svo_server *s) {
     {
         std::lock_guard<std::mutex> lk(s->mu);
         s->stop = true;
+        // finished results nobody can take any more: freed now, so that their
+        // bytes admit what is still queued (the queue is built to the end)
+        for (auto &kv : s->reqs) {
+            svo_server::Req *r = kv.second;
+            if (!r->done) continue;
+            svo_result_free(r->result);
+            r->result = nullptr;
+            reserve(s, 0, r->held);
+            r->held = 0;
+        }
     }
     s->cv_work.notify_all();
     for (auto &t : s->workers) t.join();

@@ -258,7 +258,10 @@ int svo_server_release(svo_server *s, uint64_t ticket);
  * cancelled (SVO_ERR_INVALID_ARGUMENT). */
 int svo_server_cancel(svo_server *s, uint64_t ticket);
 int svo_server_stats(const svo_server *s, svo_server_stats_t *out);
-/* Finishes every queued request, then frees all results not yet released. */
+/* Frees the results not yet released, finishes every queued request and frees
+ * its result too.  A finished result holds its bytes of the budget until it is
+ * released: a client that waits for a request while holding results can keep
+ * that request from being admitted. */
 void svo_server_destroy(svo_server *s);
 
 /* Sorted surface-voxel Morton keys of a mesh (the first stage of svo_build:

@@ -7,6 +7,7 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
+WAIT_US = 120_000_000  # a request not built within two minutes fails the test instead of hanging it
 
 
 def _same(a, b):
@@ -34,7 +35,7 @@ def test_mix_equals_alone(gpu_ctx, svo_mod, workers, max_batch, budget):
     srv = svo_mod.Server(gpu_ctx, budget, workers=workers, max_batch=max_batch)
     tickets = [srv.submit(*r) for r in reqs]
     for t, (p, f, res) in zip(tickets, reqs):
-        r, st, lat = srv.wait(t)
+        r, st, lat = srv.wait(t, timeout_us=WAIT_US)
         assert st == 0 and lat > 0
         _same(r, gpu_ctx.build(p, f, res))
         srv.release(t)
@@ -61,7 +62,7 @@ def test_arrivals_while_busy(gpu_ctx, svo_mod):
     th.start()
     th.join()
     for t, m in zip(tickets, dev):
-        r, st, _ = srv.wait(t)
+        r, st, _ = srv.wait(t, timeout_us=WAIT_US)
         assert st == 0
         _same(r, gpu_ctx.build(*m))
         srv.release(t)
@@ -77,7 +78,7 @@ def test_failures_in_the_mix(gpu_ctx, svo_mod):
     srv = svo_mod.Server(gpu_ctx, 40 << 30, workers=2, max_batch=8)
     tickets = [srv.submit(*m) for m in mix]
     for t, m in zip(tickets, mix):
-        r, st, _ = srv.wait(t)
+        r, st, _ = srv.wait(t, timeout_us=WAIT_US)
         if m is bad:
             assert st == svo_mod.ERR_EMPTY and r is None
         else:
@@ -102,7 +103,7 @@ def test_completion_order(gpu_ctx, svo_mod):
     tickets = {srv.submit(*m): m for m in reqs}
     seen = set()
     for _ in range(len(reqs)):
-        t, r, st, lat = srv.next()
+        t, r, st, lat = srv.next(timeout_us=WAIT_US)
         assert st == 0 and t in tickets and t not in seen
         seen.add(t)
         _same(r, gpu_ctx.build(*tickets[t]))
@@ -124,10 +125,12 @@ def test_cancel_queued(gpu_ctx, svo_mod):
     t1 = srv.submit(*small[0])
     t2 = srv.submit(*small[1])
     srv.cancel(t2)
-    r, st, _ = srv.wait(t2)
+    r, st, _ = srv.wait(t2, timeout_us=WAIT_US)
     assert st == svo_mod.ERR_CANCELLED and r is None
     for t, m in ((big, (soup, None, 512)), (t1, small[0])):
-        r, st, _ = srv.wait(t)
+        got = srv.wait(t, timeout_us=WAIT_US)
+        assert got is not None, "request not built in time"
+        r, st, _ = got
         assert st == 0
         _same(r, gpu_ctx.build(*m))
     with pytest.raises(svo_mod.SvoError) as e:
@@ -157,8 +160,10 @@ def test_budget_holds_when_results_outgrow_estimates(gpu_ctx, svo_mod):
     budget = int(1.5 * (exact + est))
     srv = svo_mod.Server(gpu_ctx, budget, workers=2, max_batch=8, flags=flags)
     tickets = [srv.submit(soup, None, 256) for _ in range(3)]
-    for t in tickets:
-        r, st, _ = srv.wait(t)
+    for t in tickets:  # each result is released before the next request is awaited
+        got = srv.wait(t, timeout_us=WAIT_US)
+        assert got is not None, "request not built in time"
+        r, st, _ = got
         assert st == 0
         assert r.nodes().tobytes() == alone.nodes().tobytes() and r.keys().tobytes() == alone.keys().tobytes()
         srv.release(t)
@@ -177,7 +182,7 @@ def test_served_results_match_oracle(gpu_ctx, svo_mod, oracle_mod):
     srv = svo_mod.Server(gpu_ctx, 8 << 30, workers=2, max_batch=4)
     tickets = [srv.submit(*m) for m in reqs]
     for t, (p, f, res) in zip(tickets, reqs):
-        r, st, _ = srv.wait(t)
+        r, st, _ = srv.wait(t, timeout_us=WAIT_US)
         assert st == 0
         assert_same(r, oracle_mod.build_svo(p, f, res))
         srv.release(t)
