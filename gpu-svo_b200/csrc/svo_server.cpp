@@ -56,7 +56,7 @@ struct svo_server {
     bool stop = false;
     std::vector<std::thread> workers;
     std::vector<cudaStream_t> streams;
-    uint64_t batches = 0, built = 0;
+    uint64_t batches = 0, built = 0, requeued = 0;
     double build_s = 0.0, queue_s = 0.0;  // summed over batches / requests
 };
 
@@ -161,6 +161,7 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
             }
             reserve(s, acc, drop);
             for (int i = n - 1; i >= keep; --i) s->queue.push_front(take[i]);
+            s->requeued += (uint64_t)(n - keep);
             decided();
         }
         if (keep < n) s->cv_work.notify_all();
@@ -372,6 +373,9 @@ int svo_server_stats(const svo_server *s, svo_server_stats_t *out) {
     out->build_seconds = s->build_s;
     out->queue_seconds = s->queue_s;
     out->peak_reserved_bytes = s->peak_reserved;
+    out->requeued = s->requeued;
+    out->admitted_batches = s->admitted_batches;
+    out->decided_batches = s->decided_batches;
     return SVO_OK;
 }
 

@@ -86,7 +86,8 @@ class ServerConfig(C.Structure):
 class ServerStats(C.Structure):
     _fields_ = [("queued", C.c_int64), ("busy_workers", C.c_int), ("reserved_bytes", C.c_uint64),
                 ("batches", C.c_uint64), ("built", C.c_uint64), ("build_seconds", C.c_double),
-                ("queue_seconds", C.c_double), ("peak_reserved_bytes", C.c_uint64)]
+                ("queue_seconds", C.c_double), ("peak_reserved_bytes", C.c_uint64), ("requeued", C.c_uint64),
+                ("admitted_batches", C.c_uint64), ("decided_batches", C.c_uint64)]
 
 
 _lib = None

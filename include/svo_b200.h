@@ -236,6 +236,9 @@ typedef struct svo_server_stats_t {
     double build_seconds; /* wall time of all batches (summed over workers) */
     double queue_seconds; /* time requests waited for admission (summed) */
     uint64_t peak_reserved_bytes; /* most device bytes reserved at any time */
+    uint64_t requeued;            /* requests sent back to the queue once their exact size was known */
+    uint64_t admitted_batches;    /* batches taken from the queue so far */
+    uint64_t decided_batches;     /* of those, batches that have made their keep/requeue decision */
 } svo_server_stats_t;
 /* Device bytes admission reserves for a mesh: inputs, scratch of a res^3
  * grid and the outputs of 16*res^2 nodes (a closed surface spanning it). */

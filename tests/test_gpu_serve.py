@@ -7,7 +7,7 @@ import numpy as np
 import pytest
 
 pytestmark = pytest.mark.gpu
-WAIT_US = 120_000_000  # a request not built within two minutes fails the test instead of hanging it
+WAIT_US = 60_000_000  # a request not built within a minute fails the test instead of hanging it
 
 
 def _same(a, b):
@@ -162,7 +162,8 @@ def test_budget_holds_when_results_outgrow_estimates(gpu_ctx, svo_mod):
     tickets = [srv.submit(soup, None, 256) for _ in range(3)]
     for t in tickets:  # each result is released before the next request is awaited
         got = srv.wait(t, timeout_us=WAIT_US)
-        assert got is not None, "request not built in time"
+        assert got is not None, f"request {t} not built in time; server {srv.stats()}, budget {budget}, " \
+                                f"exact {exact}, estimate {est}"
         r, st, _ = got
         assert st == 0
         assert r.nodes().tobytes() == alone.nodes().tobytes() and r.keys().tobytes() == alone.keys().tobytes()
