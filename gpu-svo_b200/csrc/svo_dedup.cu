@@ -36,13 +36,13 @@ namespace {
 
 constexpr int kDedupWarps = 8;
 constexpr uint64_t kChunkWords = 32;  // u64 words of D per chunk (2048 bits)
+constexpr uint32_t kStageKeys = 512;  // keys of one kind a warp stages in shared memory
 
 struct DedupLevel {
     const uint64_t *bits;  // occupancy bitmap of this level
     const uint64_t *K1;    // sorted codes of level l+1 (this level's sibling groups)
     uint32_t groups;       // number of those codes
     uint32_t side;         // grid side at this level
-    uint64_t words;        // u64 words of the bitmap that may be read (side^3 bits)
 };
 
 struct DedupParams {
@@ -146,29 +146,6 @@ __device__ __forceinline__ uint32_t cell_mask(const uint64_t *bits, uint64_t vc,
     return m;
 }
 
-// cell_mask with a range of the bitmap held in the warp's registers: lane k
-// holds word base + k for k < nw (zero past the bitmap's end), and a cell
-// whose word lies in that range is read from there by a shuffle instead of a
-// load.  All 32 lanes execute it together.
-__device__ __forceinline__ uint32_t cell_mask_held(const uint64_t *bits, uint64_t vc, uint64_t sx, uint64_t held,
-                                                   uint64_t base, uint64_t nw) {
-    const uint64_t xm = vc & kDilX, ym = vc & kDilY, zm = vc & kDilZ;
-    const uint64_t xd = dil_dec(xm, kDilX), yd = dil_dec(ym, kDilY), zd = dil_dec(zm, kDilZ);
-    const bool vx0 = xm < sx, vy0 = ym < (sx << 1), vz0 = zm < (sx << 2);
-    const bool vx1 = xm != 0, vy1 = ym != 0, vz1 = zm != 0;
-    uint32_t m = 0;
-#pragma unroll
-    for (int e = 0; e < 8; ++e) {
-        const bool ok = ((e & 1) ? vx1 : vx0) && ((e & 2) ? vy1 : vy0) && ((e & 4) ? vz1 : vz0);
-        const uint64_t c = ((e & 1) ? xd : xm) | ((e & 2) ? yd : ym) | ((e & 4) ? zd : zm);
-        const uint64_t k = (c >> 6) - base;
-        const uint64_t w = __shfl_sync(0xFFFFFFFFu, held, (int)(k & 31));
-        const uint64_t word = k < nw ? w : (ok ? bits[c >> 6] : 0ull);
-        m |= (ok ? (uint32_t)((word >> (c & 63)) & 1ull) : 0u) << e;
-    }
-    return m;
-}
-
 // Shared tables.
 //   around[E * 8 + s]: existence of the 8 cells u - d around a point of
 //     parity s (bit d), given the parent mask E: cell u - d has parent
@@ -210,21 +187,16 @@ __device__ void init_tables(DedupTables &t) {
     __syncthreads();
 }
 
-// Cell existence around the point u (Morton code uc) at the top level, which
-// holds the root alone: cell u - d exists iff d = u - root.
-__device__ __forceinline__ uint32_t top_ex(uint64_t root, uint64_t uc) {
+// Cell existence around P = 2Q at level l >= 1 (u = P >> l has Morton code
+// uc): from the level l+1 bitmap, or at the top level, which holds the root
+// alone, cell u - d exists iff d = u - root.
+__device__ __forceinline__ uint32_t coarse_ex(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                              uint64_t root, int l, uint64_t uc) {
+    if (l < p.T) return tb.around[cell_mask(p.lv[l + 1].bits, uc >> 3, sx[l + 1]) * 8 + (uint32_t)(uc & 7)];
     const int dx = (int)compact3(uc) - (int)compact3(root);
     const int dy = (int)compact3(uc >> 1) - (int)compact3(root >> 1);
     const int dz = (int)compact3(uc >> 2) - (int)compact3(root >> 2);
     return (dx >= 0 && dx <= 1 && dy >= 0 && dy <= 1 && dz >= 0 && dz <= 1) ? 1u << (dx | dy << 1 | dz << 2) : 0u;
-}
-
-// Cell existence around P = 2Q at level l >= 1 (u = P >> l has Morton code
-// uc): from the level l+1 bitmap, or from the root at the top level.
-__device__ __forceinline__ uint32_t coarse_ex(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                              uint64_t root, int l, uint64_t uc) {
-    if (l < p.T) return tb.around[cell_mask(p.lv[l + 1].bits, uc >> 3, sx[l + 1]) * 8 + (uint32_t)(uc & 7)];
-    return top_ex(root, uc);
 }
 
 // What one Q needs for all its keys, packed into 64 bits:
@@ -238,28 +210,13 @@ __device__ __forceinline__ uint32_t coarse_ex(const DedupParams &p, const DedupT
 //              derived where needed, from the coarser bitmaps
 constexpr uint64_t kQcMask = (1ull << 36) - 1;
 
-// The state of a Q (code qc) of chunk ch: the level-1 parent mask E0 and the
-// cell existence around 2Q at levels 1 and 2 (coarse_ex), with the chunk's own
-// words of the level 1-3 bitmaps held by the warp (h1: level-1 words
-// ch * 32 + lane; h2: level-2 words ch * 4 + lane, lanes 0-3; h3: level-3 word
-// ch / 2, lane 0) -- most lookups of a chunk fall in them.  Every lane
-// executes it (inactive lanes on any code of the chunk).
-__device__ __forceinline__ uint64_t q_state_held(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                                 uint64_t root, uint64_t qc, uint64_t ch, uint64_t h1, uint64_t h2,
-                                                 uint64_t h3) {
-    const uint32_t E0 = cell_mask_held(p.lv[1].bits, qc, sx[1], h1, ch * 32, 32);
-    const uint32_t ex1 = p.T > 1 ? tb.around[cell_mask_held(p.lv[2].bits, qc >> 3, sx[2], h2, ch * 4, 4) * 8 +
-                                             (uint32_t)(qc & 7)]
-                                 : top_ex(root, qc);
-    uint64_t s = qc | (uint64_t)E0 << 36 | (uint64_t)tb.kinds[ex1] << 44;
-    if (p.T >= 2) {
-        const uint32_t ex2 = p.T > 2 ? tb.around[cell_mask_held(p.lv[3].bits, qc >> 6, sx[3], h3, ch >> 1, 1) * 8 +
-                                                 (uint32_t)((qc >> 3) & 7)]
-                                     : top_ex(root, qc >> 3);
-        if ((qc & 7) == 0) {
-            s |= (uint64_t)tb.kinds[ex2] << 51;
-            if (p.T >= 3 && (qc & 63) == 0) s |= 1ull << 58;
-        }
+__device__ __forceinline__ uint64_t q_state(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                            uint64_t root, uint64_t qc) {
+    const uint32_t E0 = cell_mask(p.lv[1].bits, qc, sx[1]);
+    uint64_t s = qc | (uint64_t)E0 << 36 | (uint64_t)tb.kinds[coarse_ex(p, tb, sx, root, 1, qc)] << 44;
+    if (p.T >= 2 && (qc & 7) == 0) {
+        s |= (uint64_t)tb.kinds[coarse_ex(p, tb, sx, root, 2, qc >> 3)] << 51;
+        if (p.T >= 3 && (qc & 63) == 0) s |= 1ull << 58;
     }
     return s;
 }
@@ -330,7 +287,7 @@ __device__ __forceinline__ void q_count(const DedupParams &p, const DedupTables 
 // in shared memory, then taken 32 at a time (lane i the i-th): each Q's
 // state is stored at its rank (the chunk's first state + its index) and its
 // keys are counted per kind into the rank's tile of 32 states.
-__global__ void __launch_bounds__(kDedupWarps * 32, 4) k_dedup_state(const __grid_constant__ DedupParams p) {
+__global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_state(const __grid_constant__ DedupParams p) {
     __shared__ DedupTables tb;
     __shared__ uint16_t list[kDedupWarps][2048];
     __shared__ uint64_t sx[kMaxLevels];  // dilated side of each level
@@ -343,11 +300,6 @@ __global__ void __launch_bounds__(kDedupWarps * 32, 4) k_dedup_state(const __gri
     uint16_t *lst = list[warp];
     for (uint64_t i = (uint64_t)blockIdx.x * kDedupWarps + warp; i < p.ntouched; i += nwarps) {
         const uint64_t ch = p.list[i];
-        // the chunk's own words of the level 1-3 bitmaps, read once
-        const uint64_t i1 = ch * 32 + lane, i2 = ch * 4 + lane, i3 = ch >> 1;
-        const uint64_t h1 = i1 < p.lv[1].words ? p.lv[1].bits[i1] : 0ull;
-        const uint64_t h2 = (p.T > 1 && lane < 4 && i2 < p.lv[2].words) ? p.lv[2].bits[i2] : 0ull;
-        const uint64_t h3 = (p.T > 2 && lane == 0 && i3 < p.lv[3].words) ? p.lv[3].bits[i3] : 0ull;
         // list the chunk's set bits in order
         uint64_t word = D64[ch * kChunkWords + lane];
         const uint32_t n = __popcll(word);
@@ -366,8 +318,8 @@ __global__ void __launch_bounds__(kDedupWarps * 32, 4) k_dedup_state(const __gri
             const uint32_t j = j0 + lane;
             const bool act = j < total;
             uint32_t c[3] = {0, 0, 0};
-            const uint64_t s = q_state_held(p, tb, sx, root, ch * 2048 + (act ? lst[j] : 0u), ch, h1, h2, h3);
             if (act) {
+                const uint64_t s = q_state(p, tb, sx, root, ch * 2048 + lst[j]);
                 p.qs[q0 + j] = s;
                 q_count(p, tb, sx, root, s, c);
             }
@@ -386,26 +338,58 @@ __global__ void __launch_bounds__(kDedupWarps * 32, 4) k_dedup_state(const __gri
     }
 }
 
-// Key offset of slot s of el/fl: s < 9 -- the point 2Q at level s / 3, axis
-// s % 3: (level << 2) | axis; 9 <= s < 30 -- the point 2Q + r at level 0,
-// r = 1 + (s - 9) / 3: (r << 6) | axis.
-__device__ __forceinline__ uint32_t slot_offset(uint32_t s) {
-    return s < 9 ? ((s / 3) << 2 | (s % 3)) : ((1 + (s - 9) / 3) << 6 | ((s - 9) % 3));
+// Stage position of key i: XOR-swizzled within rows of 16 keys, so that
+// lanes writing runs that start 16 keys apart hit different banks.
+__device__ __forceinline__ uint32_t stage_at(uint32_t i) { return i ^ ((i >> 4) & 15u); }
+
+// Key offsets of the edge/face slots of el/fl: (r << 6) | (l << 2) | axis.
+struct KeyOffsets {
+    uint16_t lo[32];
+};
+
+__device__ void init_offsets(KeyOffsets &t) {
+    if (threadIdx.x < 32) {
+        const uint32_t s = threadIdx.x;
+        uint32_t off = 0;
+        if (s < 9) off = (s / 3) << 2 | (s % 3);
+        else if (s < 30) off = (1 + (s - 9) / 3) << 6 | ((s - 9) % 3);
+        t.lo[s] = (uint16_t)off;
+    }
 }
 
-// One kind's keys of the warp's 32 Qs (lane i holds Q i's masks, in output
-// order: vertices v's bits; edges/faces lo's bits 0-8, then hi's, then lo's
-// bits 9-29).  Q i's keys go to base + x_i, ... with x the warp's exclusive
-// scan of the counts.  The warp walks the Qs with one output slot per lane, so
-// a Q's keys are stored by consecutive lanes at consecutive addresses and no
-// lane loops over its own keys:
-//   vertices: four Qs per round, lane 8k + r holding slot r of the k-th;
-//   edges/faces: one Q per round, lane s holding slot s of lo; hi's keys
-//   (levels >= 3 of the point 2Q, only for Q a multiple of 64 in Morton code)
-//   are written by the Q's own lane afterwards.
+// Writes the keys of one Q (code qc) for one kind at positions at, at + 1, ...
+// of o (through stage_at when STAGED).  Vertices: v's bits; edges/faces:
+// lo's bits 0-8, then hi's, then lo's bits 9-29.
+template <int KIND, bool STAGED>
+__device__ __forceinline__ void put_keys(uint64_t *o, uint32_t at, uint32_t lo, uint32_t hi, uint64_t qc,
+                                         const KeyOffsets &ko) {
+    if (KIND == 0) {
+        const uint64_t b = qc << 3;
+        for (uint32_t m = lo; m; m &= m - 1, ++at) o[STAGED ? stage_at(at) : at] = b | (uint64_t)(__ffs(m) - 1);
+        return;
+    }
+    const uint64_t b = qc << 9;
+    const uint32_t nh = __popc(hi);
+    uint32_t k = at;
+    for (uint32_t m = lo; m; m &= m - 1, ++k) {
+        const int s = __ffs(m) - 1;
+        const uint32_t pos = k + (s >= 9 ? nh : 0u);
+        o[STAGED ? stage_at(pos) : pos] = b | ko.lo[s];
+    }
+    if (hi) {  // levels >= 3 of the point 2Q
+        uint32_t pos = at + __popc(lo & 0x1FFu);
+        for (uint32_t m = hi; m; m &= m - 1, ++pos) {
+            const int s = __ffs(m) - 1, l = 3 + s / 3;
+            o[STAGED ? stage_at(pos) : pos] = b | (uint64_t)((l << 2) | (s % 3));
+        }
+    }
+}
+
+// One kind's keys of the warp's 32 Qs: lane offsets by a warp scan; staged
+// in shared memory and stored coalesced when they fit, else stored directly.
 template <int KIND>
-__device__ __forceinline__ void emit_kind(uint64_t *__restrict__ out, uint64_t base, uint32_t lo, uint32_t hi,
-                                          uint64_t qc, int lane) {
+__device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t lo, uint32_t hi, uint64_t qc,
+                                          uint64_t *stage, const KeyOffsets &ko, int lane) {
     const uint32_t c = __popc(lo) + __popc(hi);
     uint32_t x = c;
 #pragma unroll
@@ -413,37 +397,14 @@ __device__ __forceinline__ void emit_kind(uint64_t *__restrict__ out, uint64_t b
         const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
         if (lane >= d) x += y;
     }
-    const uint32_t excl = x - c;
-    if (KIND == 0) {
-        const uint32_t r = lane & 7;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int src = 4 * k + (lane >> 3);
-            const uint32_t m = __shfl_sync(0xFFFFFFFFu, lo, src);
-            const uint32_t at = __shfl_sync(0xFFFFFFFFu, excl, src);
-            const uint64_t q = __shfl_sync(0xFFFFFFFFu, qc, src);
-            if ((m >> r) & 1u) out[base + at + __popc(m & ((1u << r) - 1u))] = q << 3 | r;
-        }
-        return;
-    }
-    const uint32_t off = slot_offset((uint32_t)lane);
-    const uint32_t below = (1u << lane) - 1u;
-    const uint32_t nh_mine = __popc(hi);
-    for (int i = 0; i < 32; ++i) {
-        const uint32_t m = __shfl_sync(0xFFFFFFFFu, lo, i);
-        if (m == 0) continue;  // the same for every lane
-        const uint32_t at = __shfl_sync(0xFFFFFFFFu, excl, i);
-        const uint32_t nh = __shfl_sync(0xFFFFFFFFu, nh_mine, i);
-        const uint64_t q = __shfl_sync(0xFFFFFFFFu, qc, i);
-        if (lane < 30 && ((m >> lane) & 1u))
-            out[base + at + __popc(m & below) + (lane >= 9 ? nh : 0u)] = q << 9 | off;
-    }
-    if (hi) {
-        uint32_t pos = excl + __popc(lo & 0x1FFu);
-        for (uint32_t m = hi; m; m &= m - 1, ++pos) {
-            const int sl = __ffs(m) - 1, l = 3 + sl / 3;
-            out[base + pos] = qc << 9 | (uint64_t)((l << 2) | (sl % 3));
-        }
+    const uint32_t tot = __shfl_sync(0xFFFFFFFFu, x, 31);
+    if (tot <= kStageKeys) {
+        put_keys<KIND, true>(stage, x - c, lo, hi, qc, ko);
+        __syncwarp();
+        for (uint32_t i = lane; i < tot; i += 32) out[base + i] = stage[stage_at(i)];
+        __syncwarp();
+    } else {
+        put_keys<KIND, false>(out + base, x - c, lo, hi, qc, ko);
     }
 }
 
@@ -452,21 +413,25 @@ __device__ __forceinline__ void emit_kind(uint64_t *__restrict__ out, uint64_t b
 __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_write(const __grid_constant__ DedupParams p,
                                                                  uint64_t nq) {
     __shared__ DedupTables tb;
+    __shared__ KeyOffsets ko;
+    __shared__ uint64_t stage[kDedupWarps][kStageKeys];
     __shared__ uint64_t sx[kMaxLevels];
     if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
+    init_offsets(ko);
     init_tables(tb);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
     const uint64_t root = *p.root;
+    uint64_t *stg = stage[warp];
     for (uint64_t t = (uint64_t)blockIdx.x * kDedupWarps + warp; t < p.ntiles; t += nwarps) {
         const uint64_t r = t * 32 + lane;
         const bool act = r < nq;
         const uint64_t s = act ? p.qs[r] : 0;
         const QMasks m = act ? q_masks(p, tb, sx, root, s) : QMasks{0, 0, 0, 0, 0};
         const uint64_t qc = s & kQcMask;
-        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, lane);
-        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, lane);
-        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, lane);
+        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, ko, lane);
+        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, ko, lane);
+        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, ko, lane);
     }
 }
 
@@ -535,10 +500,7 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     DedupParams p{};
     p.T = T;
     p.root = ep.lv[T].K1;
-    for (int l = 0; l <= T; ++l) {
-        const uint64_t side = ep.lv[l].side;  // the pyramid holds at least the Morton cube of this side
-        p.lv[l] = DedupLevel{ep.lv[l].bits, ep.lv[l].K1, ep.lv[l].n / 8, ep.lv[l].side, (side * side * side + 63) / 64};
-    }
+    for (int l = 0; l <= T; ++l) p.lv[l] = DedupLevel{ep.lv[l].bits, ep.lv[l].K1, ep.lv[l].n / 8, ep.lv[l].side};
     uint32_t g = 0;
     for (int l = 1; l < T; ++l) {
         p.gstart[l] = g;

@@ -16,9 +16,12 @@
 // the client releases it.  Queued requests can be cancelled.
 #include <chrono>
 #include <algorithm>
+#include <cstdio>
+#include <cstdlib>
 #include <condition_variable>
 #include <deque>
 #include <mutex>
+#include <set>
 #include <thread>
 #include <unordered_map>
 #include <vector>
@@ -46,7 +49,8 @@ struct svo_server {
     std::condition_variable cv_work, cv_done, cv_decide;
     uint64_t admitted_batches = 0;  // sequence number of the next batch admitted
     uint64_t decided_batches = 0;   // batches whose keep/requeue decision is made
-    std::deque<Req *> queue;
+    std::deque<Req *> queue;         // pending requests in ticket (arrival) order
+    std::set<uint64_t> unkept;       // tickets neither kept by a batch nor finished nor cancelled
     std::deque<uint64_t> finished;  // tickets in completion order, not yet taken by svo_server_next
     std::unordered_map<uint64_t, Req *> reqs;
     uint64_t next_ticket = 1;
@@ -63,6 +67,24 @@ struct svo_server {
 namespace {
 
 using Clock = std::chrono::steady_clock;
+
+// SVO_SERVER_TRACE=1 in the environment: admissions, keep/requeue decisions,
+// publications and releases on stderr (for diagnosing admission under a tight
+// budget).
+bool trace_on() {
+    static const bool on = [] {
+        const char *v = std::getenv("SVO_SERVER_TRACE");
+        return v && *v && *v != '0';
+    }();
+    return on;
+}
+#define SVO_TRACE(...)                          \
+    do {                                        \
+        if (trace_on()) {                       \
+            std::fprintf(stderr, "[svo_server] " __VA_ARGS__); \
+            std::fputc('\n', stderr);           \
+        }                                       \
+    } while (0)
 
 int server_fail(int code, const char *msg) {
     svo::host::set_error(msg);
@@ -112,11 +134,12 @@ void publish(svo_server *s, svo_server::Req *r, svo_result *res, int status, uin
 }
 
 // seq: the batch's admission sequence number.  Batches count concurrently but
-// make their keep/requeue decisions in admission order, so memory goes to
-// requests first come, first served: a younger request is never kept while
-// an older one, still counting, is sent back for lack of room (a client
-// waiting for the older one while holding the younger result would wait
-// forever).
+// make their keep/requeue decisions in admission order, and a request is kept
+// only when every older request is kept, finished or cancelled; requests sent
+// back return to their arrival position.  Memory thus goes to requests first
+// come, first served: a younger result never holds the memory an older
+// request waits for (a client waiting for requests in arrival order, holding
+// the younger result, would wait forever).
 void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &take, uint64_t seq) {
     svo::host::TraceRange trace("svo_server: batch");
     const int n = (int)take.size();
@@ -149,10 +172,14 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
                 const int64_t ob = svo_batch_mesh_output_bytes(b, i);  // -1: this mesh failed counting
                 const uint64_t need = take[i]->base + (ob > 0 ? (uint64_t)ob : 0);
                 const bool fits = others + acc + need <= s->cfg.mem_budget || (others == 0 && i == 0);
+                // memory goes to requests in arrival order: a request is kept only
+                // when every older one is kept, finished or cancelled
+                const bool oldest = !s->unkept.empty() && *s->unkept.begin() == take[i]->ticket;
                 drop += take[i]->held;
-                if (keep == i && fits) {
+                if (keep == i && fits && oldest) {
                     acc += need;
                     take[i]->held = need;
+                    s->unkept.erase(take[i]->ticket);
                     ++keep;
                 } else {
                     take[i]->est = need;
@@ -160,8 +187,15 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
                 }
             }
             reserve(s, acc, drop);
-            for (int i = n - 1; i >= keep; --i) s->queue.push_front(take[i]);
+            for (int i = keep; i < n; ++i) {  // back into the queue at their arrival position
+                auto at = std::lower_bound(s->queue.begin(), s->queue.end(), take[i]->ticket,
+                                           [](const svo_server::Req *q, uint64_t t) { return q->ticket < t; });
+                s->queue.insert(at, take[i]);
+            }
             s->requeued += (uint64_t)(n - keep);
+            SVO_TRACE("decide seq %llu: %d of %d kept (first ticket %llu), others %llu, reserved %llu",
+                      (unsigned long long)seq, keep, n, (unsigned long long)take[0]->ticket,
+                      (unsigned long long)others, (unsigned long long)s->reserved);
             decided();
         }
         if (keep < n) s->cv_work.notify_all();
@@ -175,12 +209,15 @@ void run_batch(svo_server *s, cudaStream_t st, std::vector<svo_server::Req *> &t
         for (int i = 0; i < n; ++i) status[i] = rc;
         std::unique_lock<std::mutex> lk(s->mu);
         s->cv_decide.wait(lk, [&] { return s->decided_batches == seq; });
+        for (svo_server::Req *r : take) s->unkept.erase(r->ticket);  // finished, with the error
         decided();
     }
     {
         std::lock_guard<std::mutex> lk(s->mu);
         const auto now = Clock::now();
         for (int i = 0; i < keep; ++i) publish(s, take[i], out[i], status[i], bytes[i], now);
+        SVO_TRACE("seq %llu publishes %d (rc %d), reserved %llu, queued %zu", (unsigned long long)seq, keep, rc,
+                  (unsigned long long)s->reserved, s->queue.size());
         if (keep > 0) s->batches += 1;
         s->built += (uint64_t)keep;
         s->build_s += std::chrono::duration<double>(now - t0).count();
@@ -216,6 +253,9 @@ void worker(svo_server *s, int w) {
             }
             ++s->busy;
             seq = s->admitted_batches++;
+            SVO_TRACE("worker %d admits seq %llu: %zu requests from ticket %llu, reserved %llu, queued %zu", w,
+                      (unsigned long long)seq, take.size(), (unsigned long long)take[0]->ticket,
+                      (unsigned long long)s->reserved, s->queue.size());
         }
         run_batch(s, st, take, seq);
     }
@@ -274,6 +314,7 @@ int svo_server_submit(svo_server *s, const svo_mesh_desc *desc, uint64_t *ticket
         r->ticket = s->next_ticket++;
         s->reqs[r->ticket] = r;
         s->queue.push_back(r);
+        s->unkept.insert(r->ticket);
         *ticket = r->ticket;
     }
     s->cv_work.notify_one();
@@ -333,6 +374,8 @@ int svo_server_release(svo_server *s, uint64_t ticket) {
                 break;
             }
         reserve(s, 0, r->held);
+        SVO_TRACE("release ticket %llu, reserved %llu, queued %zu", (unsigned long long)ticket,
+                  (unsigned long long)s->reserved, s->queue.size());
         res = r->result;
         s->reqs.erase(it);
         delete r;
@@ -354,6 +397,7 @@ int svo_server_cancel(svo_server *s, uint64_t ticket) {
             return server_fail(SVO_ERR_INVALID_ARGUMENT, r->done ? "request already finished"
                                                                : "request already building");
         s->queue.erase(q);
+        s->unkept.erase(ticket);
         publish(s, r, nullptr, SVO_ERR_CANCELLED, 0, Clock::now());
     }
     s->cv_done.notify_all();
