@@ -49,6 +49,7 @@ L2_FLUSH_BYTES = 256 << 20
 # 8 vertices x 16 B, 12 edges x 28 B written; one 8-byte group code read per
 # 8 sibling nodes.
 EMIT_BYTES_PER_NODE = 168 + 8 * 16 + 12 * 28 + 1
+EMIT_BYTES_PER_NODE_NODES_ONLY = 168 + 1  # SVO_FLAG_NO_VERT_EDGE: the node records alone
 # Every stride-th triangle of a single-mesh workload is the bounded sample the
 # CPU legs (the oracle) build, with the workload's own flags.
 CPU_STRIDE = {"torus_slivers": 16, "heightfield": 128, "icosphere_l5": 1}
@@ -452,12 +453,12 @@ def run_ours(args, rank: int, world: int):
     emit_ms = stage.get("emit", 0.0)
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
     peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
-    emit_bytes = EMIT_BYTES_PER_NODE * info["nodes"]
+    emit_bytes = (EMIT_BYTES_PER_NODE_NODES_ONLY if bflags & S.FLAG_NO_VERT_EDGE else EMIT_BYTES_PER_NODE) * info["nodes"]
     achieved = emit_bytes / (emit_ms / 1e3) / 1e9 if emit_ms > 0 else None
     traffic = None
     tpath = os.path.join(ROOT, "profiles", "emit_traffic_per_node.json")
     tsrc = None
-    if os.path.exists(tpath):
+    if os.path.exists(tpath) and not bflags & S.FLAG_NO_VERT_EDGE:
         # DRAM bytes per node of the k_emit variant this build runs, from an
         # ncu capture of a smaller case, scaled by this build's node count
         ent = json.load(open(tpath)).get("full_neighbors" if bflags & S.FLAG_FULL_NEIGHBORS else "default")

@@ -16,14 +16,15 @@
 //   1. mark a candidate bitmap D over Q = P >> 1 (each bit stands for the 8
 //      lattice points 2Q + r) from the node groups of levels >= 1 -- every
 //      level-0 corner is also a corner of a level-1 node;
-//   2. walk D's set bits in order and derive, per Q, what its 8 points need
-//      from 8 parent-bitmap lookups per level (coarser levels only for
-//      r = 0), packed into one 64-bit state per Q (q_state below), counting
-//      keys per 2048-bit chunk of D;
+//   2. walk D's words in order and derive, per Q, what its 8 points need
+//      from the parent bitmaps (coarser levels only for r = 0), for the 64 Q
+//      of a word at once by shifts of whole bitmap words; pack it into one
+//      64-bit state per Q (layout at kQcMask) and count keys per tile of 32
+//      states;
 //   3. scan the counts and expand the states into keys: the keys come out in
 //      Morton order because D is in Morton order and each point's keys are
-//      produced in (level, axis) order.  Each warp stages its keys in shared
-//      memory and stores them coalesced.
+//      produced in (level, axis) order.  Each warp stages 16-bit key
+//      entries in shared memory and stores the keys coalesced.
 // D has R^3 bits (1 GiB at R = 2048); a 1-bit-per-chunk summary lets the walk
 // skip untouched chunks without reading them.
 #include <cstdio>
@@ -36,7 +37,7 @@ namespace {
 
 constexpr int kDedupWarps = 8;
 constexpr uint64_t kChunkWords = 32;  // u64 words of D per chunk (2048 bits)
-constexpr uint32_t kStageKeys = 512;  // keys of one kind a warp stages in shared memory
+constexpr uint32_t kStageKeys = 2048;  // key entries of one kind a warp stages in shared memory
 
 struct DedupLevel {
     const uint64_t *bits;  // occupancy bitmap of this level
@@ -210,17 +211,6 @@ __device__ __forceinline__ uint32_t coarse_ex(const DedupParams &p, const DedupT
 //              derived where needed, from the coarser bitmaps
 constexpr uint64_t kQcMask = (1ull << 36) - 1;
 
-__device__ __forceinline__ uint64_t q_state(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                            uint64_t root, uint64_t qc) {
-    const uint32_t E0 = cell_mask(p.lv[1].bits, qc, sx[1]);
-    uint64_t s = qc | (uint64_t)E0 << 36 | (uint64_t)tb.kinds[coarse_ex(p, tb, sx, root, 1, qc)] << 44;
-    if (p.T >= 2 && (qc & 7) == 0) {
-        s |= (uint64_t)tb.kinds[coarse_ex(p, tb, sx, root, 2, qc >> 3)] << 51;
-        if (p.T >= 3 && (qc & 63) == 0) s |= 1ull << 58;
-    }
-    return s;
-}
-
 // Key kinds of the point 2Q at levels >= 3 (state bit 58): vertex flag into
 // v, edges/faces of level l at bits 3(l - 3)..3(l - 3) + 2 of eh/fh.
 __device__ __forceinline__ void q_deep(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
@@ -268,28 +258,132 @@ __device__ __forceinline__ QMasks q_masks(const DedupParams &p, const DedupTable
     return m;
 }
 
-// Keys per kind of one Q from its state (cnt0 covers the 8 points at level 0).
-__device__ __forceinline__ void q_count(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                        uint64_t root, uint64_t s, uint32_t c[3]) {
-    const uint32_t E0 = (uint32_t)(s >> 36) & 0xFFu, k1 = (uint32_t)(s >> 44) & 0x7Fu, k2 = (uint32_t)(s >> 51) & 0x7Fu;
-    const uint32_t k0 = tb.cnt0[E0];
-    uint32_t v = k1 | k2;
-    uint32_t e = ((k1 >> 1) & 7) | ((k2 >> 1) & 7) << 3, f = ((k1 >> 4) & 7) | ((k2 >> 4) & 7) << 3;
-    uint32_t eh = 0, fh = 0;
-    if ((s >> 58) & 1) q_deep(p, tb, sx, root, s & kQcMask, v, eh, fh);
-    const bool v0 = tb.kinds[tb.around[E0 * 8]] & 1;
-    c[0] += (k0 & 0xFF) + ((!v0 && (v & 1)) ? 1u : 0u);
-    c[1] += ((k0 >> 8) & 0xFF) + __popc(e) + __popc(eh);
-    c[2] += (k0 >> 16) + __popc(f) + __popc(fh);
+// ---------------------------------------------------------------------------
+// The state pass works on whole words of D.  A word holds the 64 Q of an
+// aligned 4 x 4 x 4 block b (its index is b's Morton code), and the bitmaps'
+// words are such blocks too, so what the Qs of a word need comes from a few
+// bitmap words by shifts, for all 64 at once:
+//   M_e (e in {0,1}^3): bit i = the level-1 cell Q_i - e is occupied
+//       (the level-0 parents around the points 2Q + r: E0 of every Q);
+//   X_d: bit i = the level-1 cell Q_i - d exists, i.e. its level-2 parent
+//       (Q_i - d) >> 1 is occupied (the cells around the point Q at level 1).
+// Bit i of a block is its cell with x = i & 1 | (i >> 2) & 2, y = (i >> 1) &
+// 1 | (i >> 3) & 2, z = (i >> 2) & 1 | (i >> 4) & 2.
+// ---------------------------------------------------------------------------
+
+// The bits of a block whose coordinate along axis a equals v.
+__host__ __device__ constexpr uint64_t block_plane(int a, int v) {
+    uint64_t m = 0;
+    for (int i = 0; i < 64; ++i)
+        if ((((i >> a) & 1) | (((i >> (a + 3)) & 1) << 1)) == v) m |= 1ull << i;
+    return m;
 }
 
-// One warp per touched chunk of D.  The chunk's set bits are listed in order
-// in shared memory, then taken 32 at a time (lane i the i-th): each Q's
-// state is stored at its rank (the chunk's first state + its index) and its
-// keys are counted per kind into the rank's tile of 32 states.
+// A block's field moved one cell up along axis A: bit i of the result is the
+// field at cell(i) - e_A, taken from `cur` (the block) or, for coordinate 0,
+// from `low` (the block below along A).
+template <int A>
+__device__ __forceinline__ uint64_t shift_up(uint64_t cur, uint64_t low) {
+    constexpr int s0 = 1 << A, s1 = 8 << A;
+    constexpr uint64_t P0 = block_plane(A, 0), P13 = block_plane(A, 1) | block_plane(A, 3), P2 = block_plane(A, 2);
+    return ((cur << s0) & P13) | ((cur << (s1 - s0)) & P2) | ((low >> (s0 + s1)) & P0);
+}
+
+// A 2 x 2 x 2 block of level-2 cells (bit m = Morton code m) seen from the
+// 4 x 4 x 4 level-1 cells below it: bit i of the result is bit i >> 3.
+__device__ __forceinline__ uint64_t upsample8(uint64_t b) {
+    b = (b | (b << 28)) & 0x0000000F0000000Full;
+    b = (b | (b << 14)) & 0x0003000300030003ull;
+    b = (b | (b << 7)) & 0x0101010101010101ull;
+    return b * 0xFFull;
+}
+
+// 32 x 32 bit transpose across the warp: lane l bit k <- lane k bit l.
+__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
+#pragma unroll
+    for (int j = 16; j; j >>= 1) {
+        const uint32_t m = j == 16 ? 0x0000FFFFu : j == 8 ? 0x00FF00FFu : j == 4 ? 0x0F0F0F0Fu
+                         : j == 2  ? 0x33333333u : 0x55555555u;
+        const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, x, j);
+        x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
+    }
+    return x;
+}
+
+// Valid cells of a block at a level of side s (only s < 4 leaves some out).
+__device__ __forceinline__ uint64_t block_valid(uint32_t s) {
+    return s >= 4 ? ~0ull : s == 2 ? 0xFFull : 0x1ull;
+}
+
+// Bit e of the cell mask around the lattice point with Morton code vc at the
+// level whose bitmap is `bits` and dilated side sx (cell_mask, one bit per
+// lane: e = lane & 7).
+__device__ __forceinline__ uint32_t cell_bit(const uint64_t *bits, uint64_t vc, uint64_t sx, int e) {
+    const uint64_t xm = vc & kDilX, ym = vc & kDilY, zm = vc & kDilZ;
+    const bool ok = ((e & 1) ? xm != 0 : xm < sx) && ((e & 2) ? ym != 0 : ym < (sx << 1)) &&
+                    ((e & 4) ? zm != 0 : zm < (sx << 2));
+    if (!ok) return 0;
+    const uint64_t c = ((e & 1) ? dil_dec(xm, kDilX) : xm) | ((e & 2) ? dil_dec(ym, kDilY) : ym) |
+                       ((e & 4) ? dil_dec(zm, kDilZ) : zm);
+    return (uint32_t)(bits[c >> 6] >> (c & 63)) & 1u;
+}
+
+// Key kinds of the point with Morton code uc at level l (coarse_ex through
+// the kinds table), the cell mask computed by lanes 8h..8h+7 for the word h
+// of the pair: every lane gets both words' kinds (h = 0 in the low byte).
+__device__ __forceinline__ uint32_t pair_kinds(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                               uint64_t root, int l, uint64_t ucA, uint64_t ucB, int lane) {
+    if (l < p.T) {
+        const uint64_t uc = lane < 8 ? ucA : ucB;
+        const uint32_t bit = lane < 16 ? cell_bit(p.lv[l + 1].bits, uc >> 3, sx[l + 1], lane & 7) : 0u;
+        const uint32_t E = __ballot_sync(0xFFFFFFFFu, bit);
+        return tb.kinds[tb.around[(E & 0xFFu) * 8 + (uint32_t)(ucA & 7)]] |
+               (uint32_t)tb.kinds[tb.around[((E >> 8) & 0xFFu) * 8 + (uint32_t)(ucB & 7)]] << 8;
+    }
+    return tb.kinds[coarse_ex(p, tb, sx, root, l, ucA)] | (uint32_t)tb.kinds[coarse_ex(p, tb, sx, root, l, ucB)] << 8;
+}
+
+// Keys of the point 2Q at levels >= 3 for the Q at bit 0 of each word of
+// the pair (q_deep's walk, warp-wide): vertex flag and edge/face counts,
+// packed like the key counts (v | e << 9 | f << 20) per word.
+__device__ __forceinline__ void pair_deep(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
+                                          uint64_t root, uint64_t bA, uint64_t bB, bool onA, bool onB, int lane,
+                                          uint32_t &dA, uint32_t &dB) {
+    dA = dB = 0;
+    uint32_t vA = 0, vB = 0;
+    uint64_t ucA = bA, ucB = bB;
+    for (int l = 3; l <= p.T && (onA || onB); ++l) {
+        if (l > 3) {
+            onA = onA && (ucA & 7) == 0;
+            onB = onB && (ucB & 7) == 0;
+            if (!onA && !onB) break;
+            ucA >>= 3;
+            ucB >>= 3;
+        }
+        const uint32_t k = pair_kinds(p, tb, sx, root, l, ucA, ucB, lane);
+        if (onA) {
+            vA |= k & 1u;
+            dA += (uint32_t)__popc((k >> 1) & 7u) << 9 | (uint32_t)__popc((k >> 4) & 7u) << 20;
+        }
+        if (onB) {
+            vB |= (k >> 8) & 1u;
+            dB += (uint32_t)__popc((k >> 9) & 7u) << 9 | (uint32_t)__popc((k >> 12) & 7u) << 20;
+        }
+    }
+    dA |= vA << 31;  // the vertex flag, merged with the point's other levels by the caller
+    dB |= vB << 31;
+}
+
+// One warp per touched chunk of D (32 words), its non-empty words taken two
+// at a time: lanes 16h..16h+15 derive word h's rows (M_0..M_7 in lanes +0..7,
+// X_0..X_7 in +8..15) from the blocks around it, three shift steps build the
+// composite offsets (lane bit A set: shifted along A, taking the partner
+// lane's block as `cur`), and two 32 x 32 transposes hand lane j the 16 bits
+// of Q_j and Q_{j+32} of both words.  Each lane then stores the states of
+// its (up to) four Qs at their ranks and counts their keys, aggregated per
+// tile of 32 states.
 __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_state(const __grid_constant__ DedupParams p) {
     __shared__ DedupTables tb;
-    __shared__ uint16_t list[kDedupWarps][2048];
     __shared__ uint64_t sx[kMaxLevels];  // dilated side of each level
     if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
     init_tables(tb);
@@ -297,99 +391,146 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_state(const __grid_c
     const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
     const uint64_t root = *p.root;
     const uint64_t *D64 = reinterpret_cast<const uint64_t *>(p.D);
-    uint16_t *lst = list[warp];
-    for (uint64_t i = (uint64_t)blockIdx.x * kDedupWarps + warp; i < p.ntouched; i += nwarps) {
-        const uint64_t ch = p.list[i];
-        // list the chunk's set bits in order
-        uint64_t word = D64[ch * kChunkWords + lane];
-        const uint32_t n = __popcll(word);
+    const int T = p.T;
+    // rows: level-1 blocks (side s1) or level-2 sub-blocks (side s2, T >= 2)
+    const uint32_t s1 = p.lv[1].side, s2 = T >= 2 ? p.lv[2].side : 1u;
+    const uint64_t nb1 = spread3((s1 + 3) / 4), nb2 = spread3((s2 + 1) / 2);
+    const uint64_t valid1 = block_valid(s1), valid2 = s2 >= 2 ? 0xFFull : 0x1ull;
+    const int r = lane & 15, d = r & 7;
+    const bool xrow = r >= 8;  // an X row (level-2 parents), else an M row
+    const uint32_t lt = (1u << lane) - 1u;
+    for (uint64_t ci = (uint64_t)blockIdx.x * kDedupWarps + warp; ci < p.ntouched; ci += nwarps) {
+        const uint64_t ch = p.list[ci];
+        const uint64_t Wl = D64[ch * kChunkWords + lane];
+        const uint32_t n = __popcll(Wl);
         uint32_t incl = n;
 #pragma unroll
-        for (int d = 1; d < 32; d <<= 1) {
-            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, d);
-            if (lane >= d) incl += y;
+        for (int k = 1; k < 32; k <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, k);
+            if (lane >= k) incl += y;
         }
-        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
-        for (uint32_t k = incl - n; word; word &= word - 1, ++k)
-            lst[k] = (uint16_t)(lane * 64 + __ffsll((long long)word) - 1);
-        __syncwarp();
-        const uint32_t q0 = p.qpre[i];
-        for (uint32_t j0 = 0; j0 < total; j0 += 32) {
-            const uint32_t j = j0 + lane;
-            const bool act = j < total;
-            uint32_t c[3] = {0, 0, 0};
-            if (act) {
-                const uint64_t s = q_state(p, tb, sx, root, ch * 2048 + lst[j]);
-                p.qs[q0 + j] = s;
-                q_count(p, tb, sx, root, s, c);
+        const uint32_t wbase = p.qpre[ci] + incl - n;  // rank of the word's first Q
+        uint32_t nz = __ballot_sync(0xFFFFFFFFu, Wl != 0);
+        while (nz) {
+            const int kA = __ffs(nz) - 1;
+            nz &= nz - 1;
+            const int kB = nz ? __ffs(nz) - 1 : kA;
+            const bool hasB = nz != 0;
+            nz &= nz - 1;
+            const uint64_t WA = __shfl_sync(0xFFFFFFFFu, Wl, kA);
+            const uint64_t WB = hasB ? __shfl_sync(0xFFFFFFFFu, Wl, kB) : 0ull;
+            const uint32_t baseA = __shfl_sync(0xFFFFFFFFu, wbase, kA), baseB = __shfl_sync(0xFFFFFFFFu, wbase, kB);
+            const uint64_t bA = ch * kChunkWords + kA, bB = ch * kChunkWords + kB;  // block codes
+            // this lane's row: the block b - d of its word
+            const uint64_t bc = lane < 16 ? bA : bB;
+            const uint64_t xm = bc & kDilX, ym = bc & kDilY, zm = bc & kDilZ;
+            bool ok = (lane < 16 || hasB) && (!(d & 1) || xm != 0) && (!(d & 2) || ym != 0) && (!(d & 4) || zm != 0);
+            const uint64_t nc = ((d & 1) ? dil_dec(xm, kDilX) : xm) | ((d & 2) ? dil_dec(ym, kDilY) : ym) |
+                                ((d & 4) ? dil_dec(zm, kDilZ) : zm);
+            const uint64_t nb = xrow ? nb2 : nb1;
+            ok = ok && (nc & kDilX) < nb && (nc & kDilY) < (nb << 1) && (nc & kDilZ) < (nb << 2);
+            uint64_t v = 0;
+            if (ok) {
+                if (!xrow) v = p.lv[1].bits[nc] & valid1;
+                else if (T >= 2) v = upsample8((p.lv[2].bits[nc >> 3] >> (8 * (nc & 7))) & valid2);
             }
-            // a round spans at most two tiles: one atomic per tile and kind
-            const uint32_t tile = act ? (q0 + j) >> 5 : 0xFFFFFFFFu;
-            const uint32_t peers = __match_any_sync(0xFFFFFFFFu, tile);
-            if (act) {
+            {
+                uint64_t y = __shfl_xor_sync(0xFFFFFFFFu, v, 1);
+                if (d & 1) v = shift_up<0>(y, v);
+                y = __shfl_xor_sync(0xFFFFFFFFu, v, 2);
+                if (d & 2) v = shift_up<1>(y, v);
+                y = __shfl_xor_sync(0xFFFFFFFFu, v, 4);
+                if (d & 4) v = shift_up<2>(y, v);
+            }
+            // lanes 0..15 hold word A's rows, 16..31 word B's; transpose the
+            // low halves (Q_0..31) and the high halves (Q_32..63)
+            const uint32_t tl = transpose32((uint32_t)v, lane), th = transpose32((uint32_t)(v >> 32), lane);
+            // level 2 (Q even in every coordinate: bits 0, 8, ..., 56) from
+            // the level-3 cells around the block, and the deeper levels of Q_0
+            uint32_t E2 = 0;  // the level-3 cell masks: word A in bits 0-7, B in 8-15
+            if (T > 2) {
+                const uint64_t bc2 = lane < 8 ? bA : bB;
+                const uint32_t bit = lane < 16 ? cell_bit(p.lv[3].bits, bc2, sx[3], lane & 7) : 0u;
+                E2 = __ballot_sync(0xFFFFFFFFu, bit);
+            }
+            uint32_t deepA = 0, deepB = 0;
+            if (T >= 3 && ((WA | WB) & 1ull))
+                pair_deep(p, tb, sx, root, bA, bB, (WA & 1ull) != 0, (WB & 1ull) != 0, lane, deepA, deepB);
+            // the four Qs of this lane: (word, half) = (A, lo), (B, lo), (A, hi), (B, hi)
+            uint32_t acc[2][3] = {{0, 0, 0}, {0, 0, 0}};  // packed counts per word and tile segment
 #pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const uint32_t sum = __reduce_add_sync(peers, c[k]);
-                    if (lane == __ffs(peers) - 1 && sum) atomicAdd(p.tcnt + k * p.ntiles + tile, sum);
+            for (int s = 0; s < 4; ++s) {
+                const int h = s & 1, hi = s >> 1;
+                const uint64_t W = h ? WB : WA;
+                const int i = lane + 32 * hi;
+                if (!((W >> i) & 1ull)) continue;
+                const uint32_t bits16 = ((hi ? th : tl) >> (16 * h)) & 0xFFFFu;
+                const uint32_t E0 = bits16 & 0xFFu;
+                const uint64_t qc = ((h ? bB : bA) << 6) | (uint64_t)i;
+                const uint32_t k1 = T >= 2 ? tb.kinds[bits16 >> 8] : tb.kinds[coarse_ex(p, tb, sx, root, 1, qc)];
+                uint64_t st = qc | (uint64_t)E0 << 36 | (uint64_t)k1 << 44;
+                uint32_t k2 = 0;
+                if (T >= 2 && (i & 7) == 0) {
+                    k2 = T > 2 ? tb.kinds[tb.around[((E2 >> (8 * h)) & 0xFFu) * 8 + (uint32_t)(i >> 3)]]
+                               : tb.kinds[coarse_ex(p, tb, sx, root, 2, qc >> 3)];
+                    st |= (uint64_t)k2 << 51;
+                    if (T >= 3 && i == 0) st |= 1ull << 58;
                 }
+                const uint32_t rho = hi ? __popcll(W & 0xFFFFFFFFull) + __popc((uint32_t)(W >> 32) & lt)
+                                        : __popc((uint32_t)W & lt);
+                const uint32_t base = h ? baseB : baseA;
+                p.qs[base + rho] = st;
+                // keys: cnt0 covers level 0; levels 1, 2 and the deep ones add
+                // edges and faces, and the vertex of 2Q when level 0 has none
+                const uint32_t k0 = tb.cnt0[E0];
+                const uint32_t deep = i == 0 ? (h ? deepB : deepA) : 0u;
+                const uint32_t vtx = (k1 | k2 | (deep >> 31)) & 1u;
+                const uint32_t c = (k0 & 0xFFu) + ((E0 == 0 && vtx) ? 1u : 0u) +
+                                   (((k0 >> 8) & 0xFFu) + __popc((k1 >> 1) & 7u) + __popc((k2 >> 1) & 7u)) * (1u << 9) +
+                                   ((k0 >> 16) + __popc((k1 >> 4) & 7u) + __popc((k2 >> 4) & 7u)) * (1u << 20) +
+                                   (deep & 0x7FFFFFFFu);
+                const uint32_t seg = ((base + rho) >> 5) - (base >> 5);
+                acc[h][0] += seg == 0 ? c : 0u;
+                acc[h][1] += seg == 1 ? c : 0u;
+                acc[h][2] += seg == 2 ? c : 0u;
+            }
+            // one atomic per (word, tile, kind): lanes 0..17
+            uint32_t tot[2][3];
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int g = 0; g < 3; ++g) tot[h][g] = __reduce_add_sync(0xFFFFFFFFu, acc[h][g]);
+            if (lane < 18) {
+                const int h = lane / 9, g = (lane / 3) % 3, k = lane % 3;
+                const uint32_t t = h ? (g == 0 ? tot[1][0] : g == 1 ? tot[1][1] : tot[1][2])
+                                     : (g == 0 ? tot[0][0] : g == 1 ? tot[0][1] : tot[0][2]);
+                const uint32_t val = k == 0 ? (t & 0x1FFu) : k == 1 ? ((t >> 9) & 0x7FFu) : (t >> 20);
+                const uint32_t tile = ((h ? baseB : baseA) >> 5) + g;
+                if (val && (h == 0 || hasB)) atomicAdd(p.tcnt + k * p.ntiles + tile, val);
             }
         }
-        __syncwarp();
     }
 }
 
-// Stage position of key i: XOR-swizzled within rows of 16 keys, so that
-// lanes writing runs that start 16 keys apart hit different banks.
-__device__ __forceinline__ uint32_t stage_at(uint32_t i) { return i ^ ((i >> 4) & 15u); }
-
-// Key offsets of the edge/face slots of el/fl: (r << 6) | (l << 2) | axis.
-struct KeyOffsets {
-    uint16_t lo[32];
-};
-
-__device__ void init_offsets(KeyOffsets &t) {
-    if (threadIdx.x < 32) {
-        const uint32_t s = threadIdx.x;
-        uint32_t off = 0;
-        if (s < 9) off = (s / 3) << 2 | (s % 3);
-        else if (s < 30) off = (1 + (s - 9) / 3) << 6 | ((s - 9) % 3);
-        t.lo[s] = (uint16_t)off;
-    }
+// Key offset of a slot id: ids 0-29 are the bits of el/fl, (r << 6) |
+// (l << 2) | axis; ids 32-61 the bits t of eh/fh, level 3 + t / 3.
+__device__ __forceinline__ uint32_t slot_offset(uint32_t id) {
+    if (id >= 32) return (3 + (id - 32) / 3) << 2 | ((id - 32) % 3);
+    if (id < 9) return (id / 3) << 2 | (id % 3);
+    return (1 + (id - 9) / 3) << 6 | ((id - 9) % 3);
 }
 
-// Writes the keys of one Q (code qc) for one kind at positions at, at + 1, ...
-// of o (through stage_at when STAGED).  Vertices: v's bits; edges/faces:
-// lo's bits 0-8, then hi's, then lo's bits 9-29.
-template <int KIND, bool STAGED>
-__device__ __forceinline__ void put_keys(uint64_t *o, uint32_t at, uint32_t lo, uint32_t hi, uint64_t qc,
-                                         const KeyOffsets &ko) {
-    if (KIND == 0) {
-        const uint64_t b = qc << 3;
-        for (uint32_t m = lo; m; m &= m - 1, ++at) o[STAGED ? stage_at(at) : at] = b | (uint64_t)(__ffs(m) - 1);
-        return;
-    }
-    const uint64_t b = qc << 9;
-    const uint32_t nh = __popc(hi);
-    uint32_t k = at;
-    for (uint32_t m = lo; m; m &= m - 1, ++k) {
-        const int s = __ffs(m) - 1;
-        const uint32_t pos = k + (s >= 9 ? nh : 0u);
-        o[STAGED ? stage_at(pos) : pos] = b | ko.lo[s];
-    }
-    if (hi) {  // levels >= 3 of the point 2Q
-        uint32_t pos = at + __popc(lo & 0x1FFu);
-        for (uint32_t m = hi; m; m &= m - 1, ++pos) {
-            const int s = __ffs(m) - 1, l = 3 + s / 3;
-            o[STAGED ? stage_at(pos) : pos] = b | (uint64_t)((l << 2) | (s % 3));
-        }
-    }
-}
-
-// One kind's keys of the warp's 32 Qs: lane offsets by a warp scan; staged
-// in shared memory and stored coalesced when they fit, else stored directly.
+// One kind's keys of the warp's 32 Qs (lane j: Q j, slot masks lo/hi).  Slot
+// by slot, in output order (vertices: r = 0..7; edges/faces: lo bits 0-8,
+// hi bits, lo bits 9-29), every lane appends an entry (lane << 6 | slot id)
+// for each key its Q has to the warp's stage at its scanned offset: the same
+// short sequence for every lane, no per-lane loops.  The stage is then read
+// in order, each entry expanded to its key (the Q's code and the slot's
+// offset fetched by shuffles from the owning lanes) and stored coalesced.
+// A tile has at most 32 x 60 keys of a kind, so the stage always suffices.
 template <int KIND>
 __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t lo, uint32_t hi, uint64_t qc,
-                                          uint64_t *stage, const KeyOffsets &ko, int lane) {
+                                          uint16_t *stage, uint32_t offA, uint32_t offB, int lane) {
     const uint32_t c = __popc(lo) + __popc(hi);
     uint32_t x = c;
 #pragma unroll
@@ -398,14 +539,42 @@ __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t
         if (lane >= d) x += y;
     }
     const uint32_t tot = __shfl_sync(0xFFFFFFFFu, x, 31);
-    if (tot <= kStageKeys) {
-        put_keys<KIND, true>(stage, x - c, lo, hi, qc, ko);
-        __syncwarp();
-        for (uint32_t i = lane; i < tot; i += 32) out[base + i] = stage[stage_at(i)];
-        __syncwarp();
+    if (tot == 0) return;
+    uint32_t pos = x - c;
+    const uint32_t tag = (uint32_t)lane << 6;
+    if (KIND == 0) {
+#pragma unroll
+        for (int r = 0; r < 8; ++r)
+            if ((lo >> r) & 1u) stage[pos++] = (uint16_t)(tag | r);
     } else {
-        put_keys<KIND, false>(out + base, x - c, lo, hi, qc, ko);
+#pragma unroll
+        for (int sl = 0; sl < 9; ++sl)
+            if ((lo >> sl) & 1u) stage[pos++] = (uint16_t)(tag | sl);
+        const uint32_t anyhi = __reduce_or_sync(0xFFFFFFFFu, hi);
+        for (int t = 0; (anyhi >> t) != 0; ++t)
+            if ((hi >> t) & 1u) stage[pos++] = (uint16_t)(tag | (32 + t));
+#pragma unroll
+        for (int sl = 9; sl < 30; ++sl)
+            if ((lo >> sl) & 1u) stage[pos++] = (uint16_t)(tag | sl);
     }
+    __syncwarp();
+    const uint32_t qlo = (uint32_t)qc, qhi = (uint32_t)(qc >> 32);
+    for (uint32_t i0 = 0; i0 < tot; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const bool act = i < tot;
+        const uint32_t e = act ? stage[i] : 0u;
+        const int owner = (int)(e >> 6), id = (int)(e & 63u);
+        const uint64_t q = (uint64_t)__shfl_sync(0xFFFFFFFFu, qhi, owner) << 32 | __shfl_sync(0xFFFFFFFFu, qlo, owner);
+        uint64_t key;
+        if (KIND == 0) {
+            key = q << 3 | (uint64_t)id;
+        } else {
+            const uint32_t a = __shfl_sync(0xFFFFFFFFu, offA, id & 31), b = __shfl_sync(0xFFFFFFFFu, offB, id & 31);
+            key = q << 9 | (uint64_t)(id < 32 ? a : b);
+        }
+        if (act) out[base + i] = key;
+    }
+    __syncwarp();
 }
 
 // One warp per tile of 32 consecutive states, expanded into keys at the
@@ -413,25 +582,24 @@ __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t
 __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_write(const __grid_constant__ DedupParams p,
                                                                  uint64_t nq) {
     __shared__ DedupTables tb;
-    __shared__ KeyOffsets ko;
-    __shared__ uint64_t stage[kDedupWarps][kStageKeys];
+    __shared__ uint16_t stage[kDedupWarps][kStageKeys];
     __shared__ uint64_t sx[kMaxLevels];
     if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
-    init_offsets(ko);
     init_tables(tb);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
     const uint64_t root = *p.root;
-    uint64_t *stg = stage[warp];
+    const uint32_t offA = slot_offset(lane), offB = slot_offset(32 + lane);
+    uint16_t *stg = stage[warp];
     for (uint64_t t = (uint64_t)blockIdx.x * kDedupWarps + warp; t < p.ntiles; t += nwarps) {
         const uint64_t r = t * 32 + lane;
         const bool act = r < nq;
         const uint64_t s = act ? p.qs[r] : 0;
         const QMasks m = act ? q_masks(p, tb, sx, root, s) : QMasks{0, 0, 0, 0, 0};
         const uint64_t qc = s & kQcMask;
-        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, ko, lane);
-        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, ko, lane);
-        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, ko, lane);
+        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, offA, offB, lane);
+        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, offA, offB, lane);
+        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, offA, offB, lane);
     }
 }
 
