@@ -155,10 +155,15 @@ __device__ __forceinline__ uint32_t cell_mask(const uint64_t *bits, uint64_t vc,
 //     with normal x/y/z, from the cell existence mask ex
 //   cnt0[E]: keys of the 8 points 2Q + r at level 0 given E, packed
 //     (vertices | edges << 8 | faces << 16)
+//   v0/e0/f0[E]: the level-0 slots of those keys as the write pass orders
+//     them (QMasks below): v0 bit r; e0/f0 bits axis (r = 0) and
+//     9 + 3(r - 1) + axis (r = 1..7)
 struct DedupTables {
     uint8_t around[2048];
     uint8_t kinds[256];
     uint32_t cnt0[256];
+    uint8_t v0[256];
+    uint32_t e0[256], f0[256];
 };
 
 __device__ void init_tables(DedupTables &t) {
@@ -184,6 +189,17 @@ __device__ void init_tables(DedupTables &t) {
             f += __popc((k >> 4) & 7);
         }
         t.cnt0[E] = v | e << 8 | f << 16;
+        uint32_t vm = 0, em = 0, fm = 0;
+        for (int r = 0; r < 8; ++r) {
+            const uint32_t k = t.kinds[t.around[E * 8 + r]];
+            const int at = r == 0 ? 0 : 9 + 3 * (r - 1);
+            vm |= (k & 1u) << r;
+            em |= ((k >> 1) & 7u) << at;
+            fm |= ((k >> 4) & 7u) << at;
+        }
+        t.v0[E] = (uint8_t)vm;
+        t.e0[E] = em;
+        t.f0[E] = fm;
     }
     __syncthreads();
 }
@@ -241,20 +257,12 @@ struct QMasks {
 __device__ __forceinline__ QMasks q_masks(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
                                           uint64_t root, uint64_t s) {
     const uint32_t E0 = (uint32_t)(s >> 36) & 0xFFu, k1 = (uint32_t)(s >> 44) & 0x7Fu, k2 = (uint32_t)(s >> 51) & 0x7Fu;
-    const uint32_t k0 = tb.kinds[tb.around[E0 * 8]];
     QMasks m;
-    m.v = (k0 | k1 | k2) & 1u;
-    m.el = ((k0 >> 1) & 7) | ((k1 >> 1) & 7) << 3 | ((k2 >> 1) & 7) << 6;
-    m.fl = ((k0 >> 4) & 7) | ((k1 >> 4) & 7) << 3 | ((k2 >> 4) & 7) << 6;
+    m.v = tb.v0[E0] | ((k1 | k2) & 1u);
+    m.el = tb.e0[E0] | ((k1 >> 1) & 7) << 3 | ((k2 >> 1) & 7) << 6;
+    m.fl = tb.f0[E0] | ((k1 >> 4) & 7) << 3 | ((k2 >> 4) & 7) << 6;
     m.eh = m.fh = 0;
     if ((s >> 58) & 1) q_deep(p, tb, sx, root, s & kQcMask, m.v, m.eh, m.fh);
-#pragma unroll
-    for (int r = 1; r < 8; ++r) {
-        const uint32_t k = tb.kinds[tb.around[E0 * 8 + r]];
-        m.v |= (k & 1u) << r;
-        m.el |= ((k >> 1) & 7) << (9 + 3 * (r - 1));
-        m.fl |= ((k >> 4) & 7) << (9 + 3 * (r - 1));
-    }
     return m;
 }
 
@@ -298,239 +306,176 @@ __device__ __forceinline__ uint64_t upsample8(uint64_t b) {
     return b * 0xFFull;
 }
 
-// 32 x 32 bit transpose across the warp: lane l bit k <- lane k bit l.
-__device__ __forceinline__ uint32_t transpose32(uint32_t x, int lane) {
-#pragma unroll
-    for (int j = 16; j; j >>= 1) {
-        const uint32_t m = j == 16 ? 0x0000FFFFu : j == 8 ? 0x00FF00FFu : j == 4 ? 0x0F0F0F0Fu
-                         : j == 2  ? 0x33333333u : 0x55555555u;
-        const uint32_t y = __shfl_xor_sync(0xFFFFFFFFu, x, j);
-        x = (lane & j) ? ((x & ~m) | ((y >> j) & m)) : ((x & m) | ((y << j) & ~m));
-    }
-    return x;
-}
-
 // Valid cells of a block at a level of side s (only s < 4 leaves some out).
 __device__ __forceinline__ uint64_t block_valid(uint32_t s) {
     return s >= 4 ? ~0ull : s == 2 ? 0xFFull : 0x1ull;
 }
 
-// Bit e of the cell mask around the lattice point with Morton code vc at the
-// level whose bitmap is `bits` and dilated side sx (cell_mask, one bit per
-// lane: e = lane & 7).
-__device__ __forceinline__ uint32_t cell_bit(const uint64_t *bits, uint64_t vc, uint64_t sx, int e) {
-    const uint64_t xm = vc & kDilX, ym = vc & kDilY, zm = vc & kDilZ;
-    const bool ok = ((e & 1) ? xm != 0 : xm < sx) && ((e & 2) ? ym != 0 : ym < (sx << 1)) &&
-                    ((e & 4) ? zm != 0 : zm < (sx << 2));
-    if (!ok) return 0;
-    const uint64_t c = ((e & 1) ? dil_dec(xm, kDilX) : xm) | ((e & 2) ? dil_dec(ym, kDilY) : ym) |
-                       ((e & 4) ? dil_dec(zm, kDilZ) : zm);
-    return (uint32_t)(bits[c >> 6] >> (c & 63)) & 1u;
-}
-
-// Key kinds of the point with Morton code uc at level l (coarse_ex through
-// the kinds table), the cell mask computed by lanes 8h..8h+7 for the word h
-// of the pair: every lane gets both words' kinds (h = 0 in the low byte).
-__device__ __forceinline__ uint32_t pair_kinds(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                               uint64_t root, int l, uint64_t ucA, uint64_t ucB, int lane) {
-    if (l < p.T) {
-        const uint64_t uc = lane < 8 ? ucA : ucB;
-        const uint32_t bit = lane < 16 ? cell_bit(p.lv[l + 1].bits, uc >> 3, sx[l + 1], lane & 7) : 0u;
-        const uint32_t E = __ballot_sync(0xFFFFFFFFu, bit);
-        return tb.kinds[tb.around[(E & 0xFFu) * 8 + (uint32_t)(ucA & 7)]] |
-               (uint32_t)tb.kinds[tb.around[((E >> 8) & 0xFFu) * 8 + (uint32_t)(ucB & 7)]] << 8;
-    }
-    return tb.kinds[coarse_ex(p, tb, sx, root, l, ucA)] | (uint32_t)tb.kinds[coarse_ex(p, tb, sx, root, l, ucB)] << 8;
-}
-
-// Keys of the point 2Q at levels >= 3 for the Q at bit 0 of each word of
-// the pair (q_deep's walk, warp-wide): vertex flag and edge/face counts,
-// packed like the key counts (v | e << 9 | f << 20) per word.
-__device__ __forceinline__ void pair_deep(const DedupParams &p, const DedupTables &tb, const uint64_t *sx,
-                                          uint64_t root, uint64_t bA, uint64_t bB, bool onA, bool onB, int lane,
-                                          uint32_t &dA, uint32_t &dB) {
-    dA = dB = 0;
-    uint32_t vA = 0, vB = 0;
-    uint64_t ucA = bA, ucB = bB;
-    for (int l = 3; l <= p.T && (onA || onB); ++l) {
-        if (l > 3) {
-            onA = onA && (ucA & 7) == 0;
-            onB = onB && (ucB & 7) == 0;
-            if (!onA && !onB) break;
-            ucA >>= 3;
-            ucB >>= 3;
-        }
-        const uint32_t k = pair_kinds(p, tb, sx, root, l, ucA, ucB, lane);
-        if (onA) {
-            vA |= k & 1u;
-            dA += (uint32_t)__popc((k >> 1) & 7u) << 9 | (uint32_t)__popc((k >> 4) & 7u) << 20;
-        }
-        if (onB) {
-            vB |= (k >> 8) & 1u;
-            dB += (uint32_t)__popc((k >> 9) & 7u) << 9 | (uint32_t)__popc((k >> 12) & 7u) << 20;
+// The 8 fields M_e = "cell Q - e" of a block from the blocks b - d
+// (A[d], d in {0,1}^3): 12 shifts, separable per axis.  dst[e] gets M_e.
+__device__ __forceinline__ void block_offsets(const uint64_t (&A)[8], uint64_t *dst, int stride) {
+    const uint64_t Fx[4] = {shift_up<0>(A[0], A[1]), shift_up<0>(A[2], A[3]), shift_up<0>(A[4], A[5]),
+                            shift_up<0>(A[6], A[7])};
+#pragma unroll
+    for (int ex = 0; ex < 2; ++ex) {
+        const uint64_t B0 = ex ? Fx[0] : A[0], B2 = ex ? Fx[1] : A[2], B4 = ex ? Fx[2] : A[4], B6 = ex ? Fx[3] : A[6];
+        const uint64_t Fy0 = shift_up<1>(B0, B2), Fy4 = shift_up<1>(B4, B6);
+#pragma unroll
+        for (int ey = 0; ey < 2; ++ey) {
+            const uint64_t C0 = ey ? Fy0 : B0, C4 = ey ? Fy4 : B4;
+            dst[(ex | ey << 1) * stride] = C0;
+            dst[(ex | ey << 1 | 4) * stride] = shift_up<2>(C0, C4);
         }
     }
-    dA |= vA << 31;  // the vertex flag, merged with the point's other levels by the caller
-    dB |= vB << 31;
 }
 
-// One warp per touched chunk of D (32 words), its non-empty words taken two
-// at a time: lanes 16h..16h+15 derive word h's rows (M_0..M_7 in lanes +0..7,
-// X_0..X_7 in +8..15) from the blocks around it, three shift steps build the
-// composite offsets (lane bit A set: shifted along A, taking the partner
-// lane's block as `cur`), and two 32 x 32 transposes hand lane j the 16 bits
-// of Q_j and Q_{j+32} of both words.  Each lane then stores the states of
-// its (up to) four Qs at their ranks and counts their keys, aggregated per
-// tile of 32 states.
-__global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_state(const __grid_constant__ DedupParams p) {
+// One warp per touched chunk of D (32 words), in two phases.
+//  1. Lane w takes word w (the 64 Q of block b): it fetches the level-1
+//     words of the blocks b - d and the level-2 bytes above them (upsampled
+//     to level-1 cells), shifts them into M_e = "level-1 cell Q - e occupied"
+//     (E0's bits) and X_d = "level-1 cell Q - d exists" (its level-2 parent
+//     is occupied: the cells around the point Q at level 1), and stores the
+//     16 masks in shared memory; with them the level-3 cell mask of b (the
+//     cells around the level-2 points of its even Q) and the deeper levels of
+//     its Q_0 (q_deep).
+//  2. The chunk's set bits are listed in order and taken 32 at a time: lane
+//     j reads its Q's 16 mask bits, stores the Q's state at its rank (the
+//     chunk's first state + j) and counts its keys, summed per tile of 32
+//     states (a round of 32 ranks spans at most two tiles).
+constexpr int kStateWarps = 4;
+
+__global__ void __launch_bounds__(kStateWarps * 32) k_dedup_state(const __grid_constant__ DedupParams p) {
     __shared__ DedupTables tb;
+    __shared__ uint64_t masks[kStateWarps][16][kChunkWords];  // [mask][word]: M_0..7, X_0..7
+    __shared__ uint16_t list[kStateWarps][2048];
+    __shared__ uint32_t wdeep[kStateWarps][kChunkWords];  // E2 | deep key counts of Q_0 (packed as below)
     __shared__ uint64_t sx[kMaxLevels];  // dilated side of each level
     if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
     init_tables(tb);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
+    const uint64_t nwarps = (uint64_t)gridDim.x * kStateWarps;
     const uint64_t root = *p.root;
     const uint64_t *D64 = reinterpret_cast<const uint64_t *>(p.D);
     const int T = p.T;
-    // rows: level-1 blocks (side s1) or level-2 sub-blocks (side s2, T >= 2)
     const uint32_t s1 = p.lv[1].side, s2 = T >= 2 ? p.lv[2].side : 1u;
-    const uint64_t nb1 = spread3((s1 + 3) / 4), nb2 = spread3((s2 + 1) / 2);
+    const uint64_t nb1 = spread3((s1 + 3) / 4), nb2 = spread3((s2 + 1) / 2);  // blocks per axis, dilated
     const uint64_t valid1 = block_valid(s1), valid2 = s2 >= 2 ? 0xFFull : 0x1ull;
-    const int r = lane & 15, d = r & 7;
-    const bool xrow = r >= 8;  // an X row (level-2 parents), else an M row
-    const uint32_t lt = (1u << lane) - 1u;
-    for (uint64_t ci = (uint64_t)blockIdx.x * kDedupWarps + warp; ci < p.ntouched; ci += nwarps) {
+    uint64_t(*mk)[kChunkWords] = masks[warp];
+    const uint32_t *mk32 = reinterpret_cast<const uint32_t *>(masks[warp]);
+    uint16_t *lst = list[warp];
+    uint32_t *wd = wdeep[warp];
+    for (uint64_t ci = (uint64_t)blockIdx.x * kStateWarps + warp; ci < p.ntouched; ci += nwarps) {
         const uint64_t ch = p.list[ci];
-        const uint64_t Wl = D64[ch * kChunkWords + lane];
-        const uint32_t n = __popcll(Wl);
+        const uint64_t bc = ch * kChunkWords + lane;  // this lane's block
+        const uint64_t W = D64[bc];
+        if (W) {
+            const uint64_t xm = bc & kDilX, ym = bc & kDilY, zm = bc & kDilZ;
+            const uint64_t xd = dil_dec(xm, kDilX), yd = dil_dec(ym, kDilY), zd = dil_dec(zm, kDilZ);
+            uint64_t A[8], U[8];
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                const bool low = (!(d & 1) || xm != 0) && (!(d & 2) || ym != 0) && (!(d & 4) || zm != 0);
+                const uint64_t nc = ((d & 1) ? xd : xm) | ((d & 2) ? yd : ym) | ((d & 4) ? zd : zm);
+                const uint64_t ncx = nc & kDilX, ncy = nc & kDilY, ncz = nc & kDilZ;
+                const bool in1 = low && ncx < nb1 && ncy < (nb1 << 1) && ncz < (nb1 << 2);
+                const bool in2 = low && T >= 2 && ncx < nb2 && ncy < (nb2 << 1) && ncz < (nb2 << 2);
+                A[d] = in1 ? p.lv[1].bits[nc] & valid1 : 0ull;
+                U[d] = in2 ? upsample8((p.lv[2].bits[nc >> 3] >> (8 * (nc & 7))) & valid2) : 0ull;
+            }
+            block_offsets(A, &mk[0][lane], kChunkWords);
+            block_offsets(U, &mk[8][lane], kChunkWords);
+            uint32_t info = T > 2 ? cell_mask(p.lv[3].bits, bc, sx[3]) : 0u;
+            if (T >= 3 && (W & 1ull)) {
+                uint32_t v = 0, eh = 0, fh = 0;
+                q_deep(p, tb, sx, root, bc << 6, v, eh, fh);
+                info |= (uint32_t)__popc(eh) << 9 | (uint32_t)__popc(fh) << 20 | (v & 1u) << 8;
+            }
+            wd[lane] = info;
+        }
+        // list the chunk's set bits in order
+        const uint32_t n = __popcll(W);
         uint32_t incl = n;
 #pragma unroll
         for (int k = 1; k < 32; k <<= 1) {
             const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, incl, k);
             if (lane >= k) incl += y;
         }
-        const uint32_t wbase = p.qpre[ci] + incl - n;  // rank of the word's first Q
-        uint32_t nz = __ballot_sync(0xFFFFFFFFu, Wl != 0);
-        while (nz) {
-            const int kA = __ffs(nz) - 1;
-            nz &= nz - 1;
-            const int kB = nz ? __ffs(nz) - 1 : kA;
-            const bool hasB = nz != 0;
-            nz &= nz - 1;
-            const uint64_t WA = __shfl_sync(0xFFFFFFFFu, Wl, kA);
-            const uint64_t WB = hasB ? __shfl_sync(0xFFFFFFFFu, Wl, kB) : 0ull;
-            const uint32_t baseA = __shfl_sync(0xFFFFFFFFu, wbase, kA), baseB = __shfl_sync(0xFFFFFFFFu, wbase, kB);
-            const uint64_t bA = ch * kChunkWords + kA, bB = ch * kChunkWords + kB;  // block codes
-            // this lane's row: the block b - d of its word
-            const uint64_t bc = lane < 16 ? bA : bB;
-            const uint64_t xm = bc & kDilX, ym = bc & kDilY, zm = bc & kDilZ;
-            bool ok = (lane < 16 || hasB) && (!(d & 1) || xm != 0) && (!(d & 2) || ym != 0) && (!(d & 4) || zm != 0);
-            const uint64_t nc = ((d & 1) ? dil_dec(xm, kDilX) : xm) | ((d & 2) ? dil_dec(ym, kDilY) : ym) |
-                                ((d & 4) ? dil_dec(zm, kDilZ) : zm);
-            const uint64_t nb = xrow ? nb2 : nb1;
-            ok = ok && (nc & kDilX) < nb && (nc & kDilY) < (nb << 1) && (nc & kDilZ) < (nb << 2);
-            uint64_t v = 0;
-            if (ok) {
-                if (!xrow) v = p.lv[1].bits[nc] & valid1;
-                else if (T >= 2) v = upsample8((p.lv[2].bits[nc >> 3] >> (8 * (nc & 7))) & valid2);
-            }
-            {
-                uint64_t y = __shfl_xor_sync(0xFFFFFFFFu, v, 1);
-                if (d & 1) v = shift_up<0>(y, v);
-                y = __shfl_xor_sync(0xFFFFFFFFu, v, 2);
-                if (d & 2) v = shift_up<1>(y, v);
-                y = __shfl_xor_sync(0xFFFFFFFFu, v, 4);
-                if (d & 4) v = shift_up<2>(y, v);
-            }
-            // lanes 0..15 hold word A's rows, 16..31 word B's; transpose the
-            // low halves (Q_0..31) and the high halves (Q_32..63)
-            const uint32_t tl = transpose32((uint32_t)v, lane), th = transpose32((uint32_t)(v >> 32), lane);
-            // level 2 (Q even in every coordinate: bits 0, 8, ..., 56) from
-            // the level-3 cells around the block, and the deeper levels of Q_0
-            uint32_t E2 = 0;  // the level-3 cell masks: word A in bits 0-7, B in 8-15
-            if (T > 2) {
-                const uint64_t bc2 = lane < 8 ? bA : bB;
-                const uint32_t bit = lane < 16 ? cell_bit(p.lv[3].bits, bc2, sx[3], lane & 7) : 0u;
-                E2 = __ballot_sync(0xFFFFFFFFu, bit);
-            }
-            uint32_t deepA = 0, deepB = 0;
-            if (T >= 3 && ((WA | WB) & 1ull))
-                pair_deep(p, tb, sx, root, bA, bB, (WA & 1ull) != 0, (WB & 1ull) != 0, lane, deepA, deepB);
-            // the four Qs of this lane: (word, half) = (A, lo), (B, lo), (A, hi), (B, hi)
-            uint32_t acc[2][3] = {{0, 0, 0}, {0, 0, 0}};  // packed counts per word and tile segment
+        const uint32_t total = __shfl_sync(0xFFFFFFFFu, incl, 31);
+        uint64_t word = W;
+        for (uint32_t k = incl - n; word; word &= word - 1, ++k)
+            lst[k] = (uint16_t)(lane * 64 + __ffsll((long long)word) - 1);
+        __syncwarp();
+        const uint32_t q0 = p.qpre[ci];
+        for (uint32_t j0 = 0; j0 < total; j0 += 32) {
+            const uint32_t j = j0 + lane;
+            uint32_t c = 0;
+            if (j < total) {
+                const uint32_t ent = lst[j], w = ent >> 6, i = ent & 63u;
+                const uint32_t *m = mk32 + 2 * w + (i >> 5);  // bits of Q_i in mask e: m[e * 64]
+                const uint32_t sh = i & 31u;
+                uint32_t E0 = 0, X = 0;
 #pragma unroll
-            for (int s = 0; s < 4; ++s) {
-                const int h = s & 1, hi = s >> 1;
-                const uint64_t W = h ? WB : WA;
-                const int i = lane + 32 * hi;
-                if (!((W >> i) & 1ull)) continue;
-                const uint32_t bits16 = ((hi ? th : tl) >> (16 * h)) & 0xFFFFu;
-                const uint32_t E0 = bits16 & 0xFFu;
-                const uint64_t qc = ((h ? bB : bA) << 6) | (uint64_t)i;
-                const uint32_t k1 = T >= 2 ? tb.kinds[bits16 >> 8] : tb.kinds[coarse_ex(p, tb, sx, root, 1, qc)];
+                for (int e = 0; e < 8; ++e) {
+                    E0 |= ((m[e * 2 * kChunkWords] >> sh) & 1u) << e;
+                    X |= ((m[(8 + e) * 2 * kChunkWords] >> sh) & 1u) << e;
+                }
+                const uint64_t qc = ((ch * kChunkWords + w) << 6) | i;
+                const uint32_t k1 = T >= 2 ? tb.kinds[X] : tb.kinds[coarse_ex(p, tb, sx, root, 1, qc)];
                 uint64_t st = qc | (uint64_t)E0 << 36 | (uint64_t)k1 << 44;
-                uint32_t k2 = 0;
-                if (T >= 2 && (i & 7) == 0) {
-                    k2 = T > 2 ? tb.kinds[tb.around[((E2 >> (8 * h)) & 0xFFu) * 8 + (uint32_t)(i >> 3)]]
+                uint32_t k2 = 0, deep = 0;
+                if (T >= 2 && (i & 7u) == 0) {
+                    const uint32_t info = wd[w];
+                    k2 = T > 2 ? tb.kinds[tb.around[(info & 0xFFu) * 8 + (i >> 3)]]
                                : tb.kinds[coarse_ex(p, tb, sx, root, 2, qc >> 3)];
                     st |= (uint64_t)k2 << 51;
-                    if (T >= 3 && i == 0) st |= 1ull << 58;
+                    if (T >= 3 && i == 0) {
+                        st |= 1ull << 58;
+                        deep = info;
+                    }
                 }
-                const uint32_t rho = hi ? __popcll(W & 0xFFFFFFFFull) + __popc((uint32_t)(W >> 32) & lt)
-                                        : __popc((uint32_t)W & lt);
-                const uint32_t base = h ? baseB : baseA;
-                p.qs[base + rho] = st;
-                // keys: cnt0 covers level 0; levels 1, 2 and the deep ones add
-                // edges and faces, and the vertex of 2Q when level 0 has none
+                p.qs[q0 + j] = st;
+                // keys: cnt0 covers level 0; levels 1, 2 and the deep ones
+                // add edges and faces, and the vertex of 2Q when level 0 has none
                 const uint32_t k0 = tb.cnt0[E0];
-                const uint32_t deep = i == 0 ? (h ? deepB : deepA) : 0u;
-                const uint32_t vtx = (k1 | k2 | (deep >> 31)) & 1u;
-                const uint32_t c = (k0 & 0xFFu) + ((E0 == 0 && vtx) ? 1u : 0u) +
-                                   (((k0 >> 8) & 0xFFu) + __popc((k1 >> 1) & 7u) + __popc((k2 >> 1) & 7u)) * (1u << 9) +
-                                   ((k0 >> 16) + __popc((k1 >> 4) & 7u) + __popc((k2 >> 4) & 7u)) * (1u << 20) +
-                                   (deep & 0x7FFFFFFFu);
-                const uint32_t seg = ((base + rho) >> 5) - (base >> 5);
-                acc[h][0] += seg == 0 ? c : 0u;
-                acc[h][1] += seg == 1 ? c : 0u;
-                acc[h][2] += seg == 2 ? c : 0u;
+                const uint32_t vtx = (k1 | k2 | (deep >> 8)) & 1u;
+                c = (k0 & 0xFFu) + ((E0 == 0 && vtx) ? 1u : 0u) +
+                    (((k0 >> 8) & 0xFFu) + __popc((k1 >> 1) & 7u) + __popc((k2 >> 1) & 7u)) * (1u << 9) +
+                    ((k0 >> 16) + __popc((k1 >> 4) & 7u) + __popc((k2 >> 4) & 7u)) * (1u << 20) +
+                    (deep & 0xFFFFFE00u);
             }
-            // one atomic per (word, tile, kind): lanes 0..17
-            uint32_t tot[2][3];
-#pragma unroll
-            for (int h = 0; h < 2; ++h)
-#pragma unroll
-                for (int g = 0; g < 3; ++g) tot[h][g] = __reduce_add_sync(0xFFFFFFFFu, acc[h][g]);
-            if (lane < 18) {
-                const int h = lane / 9, g = (lane / 3) % 3, k = lane % 3;
-                const uint32_t t = h ? (g == 0 ? tot[1][0] : g == 1 ? tot[1][1] : tot[1][2])
-                                     : (g == 0 ? tot[0][0] : g == 1 ? tot[0][1] : tot[0][2]);
+            // the round's ranks q0 + j0 + lane cross a tile boundary at lane `split`
+            const uint32_t r0 = q0 + j0, split = 32u - (r0 & 31u);
+            const uint32_t c0 = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)lane < split ? c : 0u);
+            const uint32_t c1 = __reduce_add_sync(0xFFFFFFFFu, (uint32_t)lane < split ? 0u : c);
+            if (lane < 6) {
+                const uint32_t t = lane < 3 ? c0 : c1, k = lane % 3;
                 const uint32_t val = k == 0 ? (t & 0x1FFu) : k == 1 ? ((t >> 9) & 0x7FFu) : (t >> 20);
-                const uint32_t tile = ((h ? baseB : baseA) >> 5) + g;
-                if (val && (h == 0 || hasB)) atomicAdd(p.tcnt + k * p.ntiles + tile, val);
+                if (val) atomicAdd(p.tcnt + k * p.ntiles + (r0 >> 5) + (lane < 3 ? 0 : 1), val);
             }
         }
+        __syncwarp();
     }
 }
 
-// Key offset of a slot id: ids 0-29 are the bits of el/fl, (r << 6) |
-// (l << 2) | axis; ids 32-61 the bits t of eh/fh, level 3 + t / 3.
-__device__ __forceinline__ uint32_t slot_offset(uint32_t id) {
-    if (id >= 32) return (3 + (id - 32) / 3) << 2 | ((id - 32) % 3);
-    if (id < 9) return (id / 3) << 2 | (id % 3);
-    return (1 + (id - 9) / 3) << 6 | ((id - 9) % 3);
+// Key offsets of the edge/face slots: lo bit sl of el/fl is (r << 6) |
+// (l << 2) | axis; hi bit t of eh/fh is level 3 + t / 3, axis t % 3.
+__host__ __device__ constexpr uint32_t lo_offset(int sl) {
+    return sl < 9 ? (uint32_t)((sl / 3) << 2 | (sl % 3)) : (uint32_t)((1 + (sl - 9) / 3) << 6 | ((sl - 9) % 3));
 }
+__device__ __forceinline__ uint32_t hi_offset(int t) { return (uint32_t)((3 + t / 3) << 2 | (t % 3)); }
 
 // One kind's keys of the warp's 32 Qs (lane j: Q j, slot masks lo/hi).  Slot
 // by slot, in output order (vertices: r = 0..7; edges/faces: lo bits 0-8,
-// hi bits, lo bits 9-29), every lane appends an entry (lane << 6 | slot id)
-// for each key its Q has to the warp's stage at its scanned offset: the same
-// short sequence for every lane, no per-lane loops.  The stage is then read
-// in order, each entry expanded to its key (the Q's code and the slot's
-// offset fetched by shuffles from the owning lanes) and stored coalesced.
-// A tile has at most 32 x 60 keys of a kind, so the stage always suffices.
+// hi bits, lo bits 9-29), every lane appends a 16-bit entry (lane << 9 |
+// the slot's key offset) for each key its Q has to the warp's stage at its
+// scanned offset: the same short sequence for every lane, no per-lane
+// loops.  The stage is then read in order, each entry expanded to its key
+// (the owning lane's key base, Q's code shifted, fetched by shuffles, OR the
+// offset) and stored coalesced.  A tile has at most 32 x 60 keys of a kind,
+// so the stage always suffices.
 template <int KIND>
 __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t lo, uint32_t hi, uint64_t qc,
-                                          uint16_t *stage, uint32_t offA, uint32_t offB, int lane) {
+                                          uint16_t *stage, int lane) {
     const uint32_t c = __popc(lo) + __popc(hi);
     uint32_t x = c;
 #pragma unroll
@@ -541,7 +486,7 @@ __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t
     const uint32_t tot = __shfl_sync(0xFFFFFFFFu, x, 31);
     if (tot == 0) return;
     uint32_t pos = x - c;
-    const uint32_t tag = (uint32_t)lane << 6;
+    const uint32_t tag = (uint32_t)lane << 9;
     if (KIND == 0) {
 #pragma unroll
         for (int r = 0; r < 8; ++r)
@@ -549,30 +494,24 @@ __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t
     } else {
 #pragma unroll
         for (int sl = 0; sl < 9; ++sl)
-            if ((lo >> sl) & 1u) stage[pos++] = (uint16_t)(tag | sl);
+            if ((lo >> sl) & 1u) stage[pos++] = (uint16_t)(tag | lo_offset(sl));
         const uint32_t anyhi = __reduce_or_sync(0xFFFFFFFFu, hi);
         for (int t = 0; (anyhi >> t) != 0; ++t)
-            if ((hi >> t) & 1u) stage[pos++] = (uint16_t)(tag | (32 + t));
+            if ((hi >> t) & 1u) stage[pos++] = (uint16_t)(tag | hi_offset(t));
 #pragma unroll
         for (int sl = 9; sl < 30; ++sl)
-            if ((lo >> sl) & 1u) stage[pos++] = (uint16_t)(tag | sl);
+            if ((lo >> sl) & 1u) stage[pos++] = (uint16_t)(tag | lo_offset(sl));
     }
     __syncwarp();
-    const uint32_t qlo = (uint32_t)qc, qhi = (uint32_t)(qc >> 32);
+    const uint64_t kb = qc << (KIND == 0 ? 3 : 9);
+    const uint32_t kblo = (uint32_t)kb, kbhi = (uint32_t)(kb >> 32);
     for (uint32_t i0 = 0; i0 < tot; i0 += 32) {
         const uint32_t i = i0 + lane;
-        const bool act = i < tot;
-        const uint32_t e = act ? stage[i] : 0u;
-        const int owner = (int)(e >> 6), id = (int)(e & 63u);
-        const uint64_t q = (uint64_t)__shfl_sync(0xFFFFFFFFu, qhi, owner) << 32 | __shfl_sync(0xFFFFFFFFu, qlo, owner);
-        uint64_t key;
-        if (KIND == 0) {
-            key = q << 3 | (uint64_t)id;
-        } else {
-            const uint32_t a = __shfl_sync(0xFFFFFFFFu, offA, id & 31), b = __shfl_sync(0xFFFFFFFFu, offB, id & 31);
-            key = q << 9 | (uint64_t)(id < 32 ? a : b);
-        }
-        if (act) out[base + i] = key;
+        const uint32_t e = i < tot ? stage[i] : 0u;
+        const int owner = (int)(e >> 9);
+        const uint32_t klo = __shfl_sync(0xFFFFFFFFu, kblo, owner) | (e & 511u);
+        const uint32_t khi = __shfl_sync(0xFFFFFFFFu, kbhi, owner);
+        if (i < tot) out[base + i] = (uint64_t)khi << 32 | klo;
     }
     __syncwarp();
 }
@@ -589,7 +528,6 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_write(const __grid_c
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
     const uint64_t root = *p.root;
-    const uint32_t offA = slot_offset(lane), offB = slot_offset(32 + lane);
     uint16_t *stg = stage[warp];
     for (uint64_t t = (uint64_t)blockIdx.x * kDedupWarps + warp; t < p.ntiles; t += nwarps) {
         const uint64_t r = t * 32 + lane;
@@ -597,9 +535,9 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_write(const __grid_c
         const uint64_t s = act ? p.qs[r] : 0;
         const QMasks m = act ? q_masks(p, tb, sx, root, s) : QMasks{0, 0, 0, 0, 0};
         const uint64_t qc = s & kQcMask;
-        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, offA, offB, lane);
-        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, offA, offB, lane);
-        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, offA, offB, lane);
+        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, lane);
+        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, lane);
+        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, lane);
     }
 }
 
@@ -758,12 +696,13 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     auto *scan2 = static_cast<unsigned long long *>(blk2[5]);
     if ((e = cudaMemsetAsync(p.tcnt, 0, sz2[3], st)) != cudaSuccess) return fail(e, "memset");
     if (nt > 0) {
-        const unsigned blocks = (unsigned)std::min<uint64_t>((nt + kDedupWarps - 1) / kDedupWarps, (uint64_t)num_sms * 16);
         k_chunk_bits<<<(unsigned)((nt + 7) / 8), 256, 0, st>>>(p);
         count_launches(1);
         if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "chunk bits");
         if ((e = launch_scan(p.qn, qpre, nt, scan2, status, st)) != cudaSuccess) return fail(e, "scan");
-        k_dedup_state<<<blocks, kDedupWarps * 32, 0, st>>>(p);
+        const unsigned sblocks =
+            (unsigned)std::min<uint64_t>((nt + kStateWarps - 1) / kStateWarps, (uint64_t)num_sms * 32);
+        k_dedup_state<<<sblocks, kStateWarps * 32, 0, st>>>(p);
         count_launches(1);
     }
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "count");
