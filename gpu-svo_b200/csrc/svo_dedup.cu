@@ -87,10 +87,11 @@ __device__ __forceinline__ uint32_t mark_bit(const DedupParams &p, uint64_t bit)
 //     of D gets the sub-points k' with k'_i = 0 wherever e_i = 1;
 //   level l >= 2: Q = (2g + {0,1,2}^3) << (l - 1), one bit each;
 //   the root (level T): Q = (root + {0,1}^3) << (T - 1).
-//   Also counts the bits it sets first (*p.nq: the set bits of D).
-__global__ void k_dedup_mark(const __grid_constant__ DedupParams p, uint32_t total) {
+//   Also counts the bits it sets first (*p.nq: the set bits of D).  Threads
+//   from `first` on (first = gstart[2] when k_dedup_build did level 1).
+__global__ void k_dedup_mark(const __grid_constant__ DedupParams p, uint32_t first, uint32_t total) {
     uint32_t fresh = 0;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    for (uint32_t t = first + blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
         if (t == total - 1) {
             const uint64_t rc = *p.root;
             const uint32_t r[3] = {compact3(rc), compact3(rc >> 1), compact3(rc >> 2)};
@@ -145,6 +146,17 @@ __device__ __forceinline__ uint32_t cell_mask(const uint64_t *bits, uint64_t vc,
         m |= (uint32_t)((bits[c >> 6] >> (c & 63)) & 1ull) << e;
     }
     return m;
+}
+
+// Bit e of cell_mask(bits, vc, sx) alone.
+__device__ __forceinline__ uint32_t cell_bit(const uint64_t *bits, uint64_t vc, uint64_t sx, int e) {
+    const uint64_t xm = vc & kDilX, ym = vc & kDilY, zm = vc & kDilZ;
+    const bool ok = ((e & 1) ? xm != 0 : xm < sx) && ((e & 2) ? ym != 0 : ym < (sx << 1)) &&
+                    ((e & 4) ? zm != 0 : zm < (sx << 2));
+    if (!ok) return 0;
+    const uint64_t c = ((e & 1) ? dil_dec(xm, kDilX) : xm) | ((e & 2) ? dil_dec(ym, kDilY) : ym) |
+                       ((e & 4) ? dil_dec(zm, kDilZ) : zm);
+    return (uint32_t)(bits[c >> 6] >> (c & 63)) & 1u;
 }
 
 // Shared tables.
@@ -473,19 +485,11 @@ __device__ __forceinline__ uint32_t hi_offset(int t) { return (uint32_t)((3 + t 
 // (the owning lane's key base, Q's code shifted, fetched by shuffles, OR the
 // offset) and stored coalesced.  A tile has at most 32 x 60 keys of a kind,
 // so the stage always suffices.
+// `pos` is the lane's first stage position, `tot` the warp's keys of this kind.
 template <int KIND>
 __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t lo, uint32_t hi, uint64_t qc,
-                                          uint16_t *stage, int lane) {
-    const uint32_t c = __popc(lo) + __popc(hi);
-    uint32_t x = c;
-#pragma unroll
-    for (int d = 1; d < 32; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
-        if (lane >= d) x += y;
-    }
-    const uint32_t tot = __shfl_sync(0xFFFFFFFFu, x, 31);
+                                          uint16_t *stage, int lane, uint32_t pos, uint32_t tot) {
     if (tot == 0) return;
-    uint32_t pos = x - c;
     const uint32_t tag = (uint32_t)lane << 9;
     if (KIND == 0) {
 #pragma unroll
@@ -505,13 +509,26 @@ __device__ __forceinline__ void emit_kind(uint64_t *out, uint64_t base, uint32_t
     __syncwarp();
     const uint64_t kb = qc << (KIND == 0 ? 3 : 9);
     const uint32_t kblo = (uint32_t)kb, kbhi = (uint32_t)(kb >> 32);
-    for (uint32_t i0 = 0; i0 < tot; i0 += 32) {
-        const uint32_t i = i0 + lane;
-        const uint32_t e = i < tot ? stage[i] : 0u;
-        const int owner = (int)(e >> 9);
-        const uint32_t klo = __shfl_sync(0xFFFFFFFFu, kblo, owner) | (e & 511u);
-        const uint32_t khi = __shfl_sync(0xFFFFFFFFu, kbhi, owner);
-        if (i < tot) out[base + i] = (uint64_t)khi << 32 | klo;
+    // two keys per lane, as 16-byte stores: an odd base first stores key 0 alone
+    const uint32_t peel = (uint32_t)(base & 1);
+    if (peel) {
+        const uint32_t e = stage[0];
+        const uint32_t klo = __shfl_sync(0xFFFFFFFFu, kblo, (int)(e >> 9)) | (e & 511u);
+        const uint32_t khi = __shfl_sync(0xFFFFFFFFu, kbhi, (int)(e >> 9));
+        if (lane == 0) out[base] = (uint64_t)khi << 32 | klo;
+    }
+    for (uint32_t i0 = peel; i0 < tot; i0 += 64) {
+        const uint32_t i = i0 + 2 * lane;
+        const uint32_t ea = i < tot ? stage[i] : 0u, eb = i + 1 < tot ? stage[i + 1] : 0u;
+        const uint32_t alo = __shfl_sync(0xFFFFFFFFu, kblo, (int)(ea >> 9)) | (ea & 511u);
+        const uint32_t ahi = __shfl_sync(0xFFFFFFFFu, kbhi, (int)(ea >> 9));
+        const uint32_t blo = __shfl_sync(0xFFFFFFFFu, kblo, (int)(eb >> 9)) | (eb & 511u);
+        const uint32_t bhi = __shfl_sync(0xFFFFFFFFu, kbhi, (int)(eb >> 9));
+        if (i + 1 < tot)
+            *reinterpret_cast<ulonglong2 *>(out + base + i) =
+                make_ulonglong2((unsigned long long)ahi << 32 | alo, (unsigned long long)bhi << 32 | blo);
+        else if (i < tot)
+            out[base + i] = (uint64_t)ahi << 32 | alo;
     }
     __syncwarp();
 }
@@ -535,9 +552,21 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_write(const __grid_c
         const uint64_t s = act ? p.qs[r] : 0;
         const QMasks m = act ? q_masks(p, tb, sx, root, s) : QMasks{0, 0, 0, 0, 0};
         const uint64_t qc = s & kQcMask;
-        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, lane);
-        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, lane);
-        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, lane);
+        // one scan for the three kinds: counts packed v | e << 9 | f << 20
+        // (at most 32 x 8 and 32 x 60 per tile)
+        const uint32_t c = (uint32_t)__popc(m.v) | (uint32_t)(__popc(m.el) + __popc(m.eh)) << 9 |
+                           (uint32_t)(__popc(m.fl) + __popc(m.fh)) << 20;
+        uint32_t x = c;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d);
+            if (lane >= d) x += y;
+        }
+        const uint32_t tot = __shfl_sync(0xFFFFFFFFu, x, 31), ex = x - c;
+        emit_kind<0>(p.out[0], p.tpre[t], m.v, 0u, qc, stg, lane, ex & 0x1FFu, tot & 0x1FFu);
+        emit_kind<1>(p.out[1], p.tpre[(p.ntiles + 1) + t], m.el, m.eh, qc, stg, lane, (ex >> 9) & 0x7FFu,
+                     (tot >> 9) & 0x7FFu);
+        emit_kind<2>(p.out[2], p.tpre[2 * (p.ntiles + 1) + t], m.fl, m.fh, qc, stg, lane, ex >> 20, tot >> 20);
     }
 }
 
@@ -564,6 +593,77 @@ __global__ void __launch_bounds__(256) k_dedup_zero(uint64_t *__restrict__ D, ui
 #pragma unroll
         for (int q = 0; q < 4; ++q) w[threadIdx.x + 256 * q] = make_uint4(0, 0, 0, 0);
     }
+}
+
+// The level-1 part of D, word by word over the same regions: bit Q is set
+// iff some level-1 node has corner Q, i.e. a level-1 cell Q - d (d in
+// {0,1}^3) exists -- its level-2 parent is occupied.  The level-2 bytes
+// above the blocks b - d, upsampled to level-1 cells, dilated by one cell
+// along each axis (separable: 7 shifts).  Every word of a region is
+// written, zeros included, so D needs no zeroing; G gets every chunk with a
+// set bit and *p.nq the set bits.  Needs T >= 2 (the level-2 bitmap).
+// Most words lie far from every node: a region (64 x 64 x 32 Q) whose
+// level-7 cells c - e (c = its origin >> 6, e in {0,1}^3: they hold every
+// level-2 parent of the cells Q - d it needs) are all empty is only
+// zeroed, and so is a warp's chunk (16 x 16 x 8 Q) whose level-5 cells
+// c - e (c = its origin >> 4) are empty.
+__global__ void __launch_bounds__(256) k_dedup_build(const __grid_constant__ DedupParams p, uint64_t regions,
+                                                     uint32_t half) {
+    const int lane = threadIdx.x & 31;
+    const uint32_t s2 = p.lv[2].side;
+    const uint64_t nb2 = spread3((s2 + 1) / 2), valid2 = s2 >= 2 ? 0xFFull : 0x1ull;
+    const uint64_t *bits2 = p.lv[2].bits;
+    const int T = p.T;
+    const uint64_t sx5 = T >= 5 ? spread3(p.lv[5].side) : 0, sx7 = T >= 7 ? spread3(p.lv[7].side) : 0;
+    uint64_t *D64 = reinterpret_cast<uint64_t *>(p.D);
+    uint32_t cnt = 0;
+    for (uint64_t r = blockIdx.x; r < regions; r += gridDim.x) {
+        const uint64_t c = r << 17;  // the region's first Q
+        if (compact3(c) > half || compact3(c >> 1) > half || compact3(c >> 2) > half) continue;
+        const uint32_t near7 = T >= 7 && threadIdx.x < 8 ? cell_bit(p.lv[7].bits, c >> 18, sx7, threadIdx.x) : 0u;
+        if (!__syncthreads_or(T < 7 || near7)) {
+            uint4 *w = reinterpret_cast<uint4 *>(D64 + r * 2048);
+#pragma unroll
+            for (int q = 0; q < 4; ++q) w[threadIdx.x + 256 * q] = make_uint4(0, 0, 0, 0);
+            continue;
+        }
+        for (int k = 0; k < 8; ++k) {
+            const uint64_t bc = r * 2048 + k * 256 + threadIdx.x;  // word = block code
+            if (T >= 5) {
+                const uint64_t c5 = ((bc & ~31ull) << 6) >> 12;  // the chunk's origin at level 5
+                const uint32_t near5 = lane < 8 ? cell_bit(p.lv[5].bits, c5, sx5, lane) : 0u;
+                if (!__ballot_sync(0xFFFFFFFFu, near5)) {
+                    D64[bc] = 0;
+                    continue;
+                }
+            }
+            const uint64_t xm = bc & kDilX, ym = bc & kDilY, zm = bc & kDilZ;
+            const uint64_t xd = dil_dec(xm, kDilX), yd = dil_dec(ym, kDilY), zd = dil_dec(zm, kDilZ);
+            uint64_t U[8];
+#pragma unroll
+            for (int d = 0; d < 8; ++d) {
+                const bool low = (!(d & 1) || xm != 0) && (!(d & 2) || ym != 0) && (!(d & 4) || zm != 0);
+                const uint64_t nc = ((d & 1) ? xd : xm) | ((d & 2) ? yd : ym) | ((d & 4) ? zd : zm);
+                const bool in2 = low && (nc & kDilX) < nb2 && (nc & kDilY) < (nb2 << 1) && (nc & kDilZ) < (nb2 << 2);
+                U[d] = in2 ? (bits2[nc >> 3] >> (8 * (nc & 7))) & valid2 : 0ull;
+            }
+            uint64_t w = 0;
+            if (U[0] | U[1] | U[2] | U[3] | U[4] | U[5] | U[6] | U[7]) {
+#pragma unroll
+                for (int d = 0; d < 8; ++d) U[d] = upsample8(U[d]);
+                const uint64_t G0 = U[0] | shift_up<0>(U[0], U[1]), G2 = U[2] | shift_up<0>(U[2], U[3]);
+                const uint64_t G4 = U[4] | shift_up<0>(U[4], U[5]), G6 = U[6] | shift_up<0>(U[6], U[7]);
+                const uint64_t H0 = G0 | shift_up<1>(G0, G2), H4 = G4 | shift_up<1>(G4, G6);
+                w = H0 | shift_up<2>(H0, H4);
+            }
+            D64[bc] = w;
+            const uint32_t any = __ballot_sync(0xFFFFFFFFu, w != 0);  // the warp's 32 words: one chunk
+            if (lane == 0 && any) atomicOr(p.G + (bc >> 10), 1u << ((bc >> 5) & 31));
+            cnt += __popcll(w);
+        }
+    }
+    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
+    if (lane == 0 && cnt) atomicAdd(p.nq, (unsigned long long)cnt);
 }
 
 // The touched chunks in order: per-word popcounts of G, then (after a scan)
@@ -650,18 +750,26 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     auto *scan = static_cast<unsigned long long *>(blk[5]);
     uint32_t *status = static_cast<uint32_t *>(blk[6]);
     p.nq = reinterpret_cast<unsigned long long *>(static_cast<char *>(blk[6]) + 8);
+    // D: in 2048-word regions, level 1 by k_dedup_build (T >= 2), the
+    // coarser levels marked after it; else zeroed and marked at all levels
+    const bool build1 = d_words % 2048 == 0 && T >= 2;
+    if ((e = cudaMemsetAsync(p.G, 0, sz[1], st)) || (e = cudaMemsetAsync(status, 0, 16, st)))
+        return fail(e, "memset");
     if (d_words % 2048 == 0) {
         const uint64_t regions = d_words / 2048;
-        k_dedup_zero<<<(unsigned)std::min<uint64_t>(regions, (uint64_t)num_sms * 8), 256, 0, st>>>(
-            reinterpret_cast<uint64_t *>(p.D), regions, (uint32_t)(side / 2));
+        const unsigned rb = (unsigned)std::min<uint64_t>(regions, (uint64_t)num_sms * 8);
+        if (build1)
+            k_dedup_build<<<rb, 256, 0, st>>>(p, regions, (uint32_t)(side / 2));
+        else
+            k_dedup_zero<<<rb, 256, 0, st>>>(reinterpret_cast<uint64_t *>(p.D), regions, (uint32_t)(side / 2));
         count_launches(1);
         e = cudaGetLastError();
     } else {
         e = cudaMemsetAsync(p.D, 0, sz[0], st);
     }
-    if (e != cudaSuccess || (e = cudaMemsetAsync(p.G, 0, sz[1], st)) || (e = cudaMemsetAsync(status, 0, 16, st)))
-        return fail(e, "memset");
-    k_dedup_mark<<<(mark_total + 255) / 256, 256, 0, st>>>(p, mark_total);
+    if (e != cudaSuccess) return fail(e, "clear");
+    const uint32_t mark_first = build1 ? p.gstart[2] : 0u;
+    k_dedup_mark<<<(mark_total - mark_first + 255) / 256, 256, 0, st>>>(p, mark_first, mark_total);
     k_touched_count<<<(unsigned)((g_words + 255) / 256), 256, 0, st>>>(p.G, g_words, gcnt);
     count_launches(2);
     if ((e = cudaGetLastError()) != cudaSuccess) return fail(e, "mark");
