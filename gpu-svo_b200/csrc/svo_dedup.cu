@@ -64,6 +64,7 @@ struct DedupParams {
     uint32_t *tcnt;             // [3][ntiles] keys per tile and kind
     const uint32_t *tpre;       // [3][ntiles + 1] their prefixes
     uint64_t *out[3];
+    const struct DedupTables *tables;  // built once per dedup by k_dedup_tables
 };
 
 __device__ __forceinline__ void mark_chunk(const DedupParams &p, uint64_t bit) {
@@ -170,7 +171,7 @@ __device__ __forceinline__ uint32_t cell_bit(const uint64_t *bits, uint64_t vc, 
 //   v0/e0/f0[E]: the level-0 slots of those keys as the write pass orders
 //     them (QMasks below): v0 bit r; e0/f0 bits axis (r = 0) and
 //     9 + 3(r - 1) + axis (r = 1..7)
-struct DedupTables {
+struct alignas(16) DedupTables {
     uint8_t around[2048];
     uint8_t kinds[256];
     uint32_t cnt0[256];
@@ -213,6 +214,17 @@ __device__ void init_tables(DedupTables &t) {
         t.e0[E] = em;
         t.f0[E] = fm;
     }
+    __syncthreads();
+}
+
+// The tables of one dedup, built by one block into global memory; the state
+// and write passes copy them into shared memory.
+__global__ void __launch_bounds__(256) k_dedup_tables(DedupTables *t) { init_tables(*t); }
+
+__device__ __forceinline__ void load_tables(DedupTables &sh, const DedupTables *g) {
+    const uint4 *src = reinterpret_cast<const uint4 *>(g);
+    uint4 *dst = reinterpret_cast<uint4 *>(&sh);
+    for (int i = threadIdx.x; i < (int)(sizeof(DedupTables) / 16); i += blockDim.x) dst[i] = src[i];
     __syncthreads();
 }
 
@@ -363,7 +375,7 @@ __global__ void __launch_bounds__(kStateWarps * 32) k_dedup_state(const __grid_c
     __shared__ uint32_t wdeep[kStateWarps][kChunkWords];  // E2 | deep key counts of Q_0 (packed as below)
     __shared__ uint64_t sx[kMaxLevels];  // dilated side of each level
     if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
-    init_tables(tb);
+    load_tables(tb, p.tables);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t nwarps = (uint64_t)gridDim.x * kStateWarps;
     const uint64_t root = *p.root;
@@ -541,7 +553,7 @@ __global__ void __launch_bounds__(kDedupWarps * 32) k_dedup_write(const __grid_c
     __shared__ uint16_t stage[kDedupWarps][kStageKeys];
     __shared__ uint64_t sx[kMaxLevels];
     if (threadIdx.x < kMaxLevels) sx[threadIdx.x] = (int)threadIdx.x <= p.T ? spread3(p.lv[threadIdx.x].side) : 0;
-    init_tables(tb);
+    load_tables(tb, p.tables);
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const uint64_t nwarps = (uint64_t)gridDim.x * kDedupWarps;
     const uint64_t root = *p.root;
@@ -721,13 +733,13 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     const uint64_t g_words = (p.chunks + 31) / 32;
 
     if (p.chunks > 0xFFFFFFFFull) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup grid too large");
-    // scratch: D, G, G popcounts + prefix, touched list, scan scratch, status
-    void *blk[7] = {};
-    const size_t sz[7] = {d_words * 8, g_words * 4, g_words * 4, (g_words + 1) * 4, p.chunks * 4,
-                          scan_scratch_words(std::max<uint64_t>(p.chunks, g_words)) * 8, 256};
+    // scratch: D, G, G popcounts + prefix, touched list, scan scratch, status, tables
+    void *blk[8] = {};
+    const size_t sz[8] = {d_words * 8, g_words * 4, g_words * 4, (g_words + 1) * 4, p.chunks * 4,
+                          scan_scratch_words(std::max<uint64_t>(p.chunks, g_words)) * 8, 256, sizeof(DedupTables)};
     void *blk2[6] = {};  // sized once the counts are known: states per chunk, the states, keys per tile
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < 7 && e == cudaSuccess; ++i) e = pool_malloc(&blk[i], sz[i], pool, st);
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = pool_malloc(&blk[i], sz[i], pool, st);
     auto release = [&]() {
         for (void *b : blk)
             if (b) cudaFreeAsync(b, st);
@@ -750,6 +762,9 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     auto *scan = static_cast<unsigned long long *>(blk[5]);
     uint32_t *status = static_cast<uint32_t *>(blk[6]);
     p.nq = reinterpret_cast<unsigned long long *>(static_cast<char *>(blk[6]) + 8);
+    p.tables = static_cast<const DedupTables *>(blk[7]);
+    k_dedup_tables<<<1, 256, 0, st>>>(static_cast<DedupTables *>(blk[7]));
+    count_launches(1);
     // D: in 2048-word regions, level 1 by k_dedup_build (T >= 2), the
     // coarser levels marked after it; else zeroed and marked at all levels
     const bool build1 = d_words % 2048 == 0 && T >= 2;
