@@ -236,7 +236,6 @@ struct Row {
     float inner;      // tail of n.dot(p)
     float xyb[3];     // XY: b * p.y
     float zxp[3];     // ZX: a * p.z
-    uint64_t syz;     // Morton bits of y and z
 };
 
 template <bool S>
@@ -252,7 +251,6 @@ __device__ __forceinline__ bool row_prep(const Tri &t, const GridParams &g, int 
         r.xyb[k] = __fmul_rn(t.eb[k], py);
         r.zxp[k] = __fmul_rn(t.ea[6 + k], pz);
     }
-    r.syz = (spread3((uint32_t)y) << 1) | (spread3((uint32_t)z) << 2);
     return true;
 }
 
@@ -293,14 +291,16 @@ struct HitSink {
     }
 };
 
-// Tests voxels x in [x0, x1] of row (y, z).
+// Tests voxels x in [x0, x1] of row (y, z); syz holds the Morton bits of y
+// and z, and x's are stepped in place (dil_inc).
 template <bool S>
-__device__ __forceinline__ void row_segment(const Tri &t, const GridParams &g, int y, int z, int x0,
+__device__ __forceinline__ void row_segment(const Tri &t, const GridParams &g, int y, int z, uint64_t syz, int x0,
                                             int x1, HitSink &sink) {
     Row r;
     if (!row_prep<S>(t, g, y, z, r)) return;
-    for (int x = x0; x <= x1; ++x)
-        if (voxel_test<S>(t, g, r, x)) sink.add(spread3((uint32_t)x) | r.syz);
+    uint64_t xm = spread3((uint32_t)x0);
+    for (int x = x0; x <= x1; ++x, xm = dil_inc(xm, kDilX))
+        if (voxel_test<S>(t, g, r, x)) sink.add(xm | syz);
 }
 
 // The full voxel test at one voxel (the same arithmetic as row_prep +
@@ -630,7 +630,8 @@ __device__ __forceinline__ void warp_rows(const BatchDev &bd, const Tri *st, con
             const GridParams g = *bd.mesh[mm].gp;
             const uint32_t ny = (uint32_t)(t.hi[1] - t.lo[1] + 1);
             HitSink sink{reinterpret_cast<uint32_t *>(bd.mesh[mm].bits)};
-            row_segment<S>(t, g, t.lo[1] + (int)(j % ny), t.lo[2] + (int)(j / ny), t.lo[0], t.hi[0], sink);
+            const int y = t.lo[1] + (int)(j % ny), z = t.lo[2] + (int)(j / ny);
+            row_segment<S>(t, g, y, z, spread3((uint32_t)y) << 1 | spread3((uint32_t)z) << 2, t.lo[0], t.hi[0], sink);
             sink.flush();
         }
     }
@@ -702,8 +703,13 @@ __global__ void __launch_bounds__(256, INPLACE ? 2 : 3)
             const MeshDev &md = bd.mesh[m];
             const GridParams g = *md.gp;
             HitSink sink{reinterpret_cast<uint32_t *>(md.bits)};
-            for (int z = t.lo[2]; z <= t.hi[2]; ++z)
-                for (int y = t.lo[1]; y <= t.hi[1]; ++y) row_segment<S>(t, g, y, z, t.lo[0], t.hi[0], sink);
+            const uint64_t ym0 = spread3((uint32_t)t.lo[1]) << 1;
+            uint64_t zm = spread3((uint32_t)t.lo[2]) << 2;
+            for (int z = t.lo[2]; z <= t.hi[2]; ++z, zm = dil_inc(zm, kDilZ)) {
+                uint64_t ym = ym0;
+                for (int y = t.lo[1]; y <= t.hi[1]; ++y, ym = dil_inc(ym, kDilY))
+                    row_segment<S>(t, g, y, z, ym | zm, t.lo[0], t.hi[0], sink);
+            }
             sink.flush();
         }
         if (INPLACE) {
