@@ -672,6 +672,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 job.l1 = mh.T + 1;
                 job.out = K + kbase[j];
                 job.wpre = WP + wbase[j];
+                // region mode: words of levels 1-3 of unflagged regions are empty, not read
+                job.rflag = mh.py.words[0] >= kRegionWords ? b->rflag + mh.cta0 : nullptr;
                 uint64_t ko = 0;
                 for (int l = 1; l <= mh.T; ++l) {
                     job.koff[l] = ko;
@@ -690,7 +692,6 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                     k0.out = r->keys;
                     k0.wpre = nullptr;
                     std::memset(k0.koff, 0, sizeof(k0.koff));
-                    k0.rflag = mh.py.words[0] >= kRegionWords ? b->rflag + mh.cta0 : nullptr;
                     jobs.push_back(k0);
                     word_off.push_back(word_off.back() + mh.py.words[0]);
                 }

@@ -408,6 +408,9 @@ __global__ void k_level_totals(BatchDev bd) {
 // word's rank in its level is the block's scanned base plus an 8-lane prefix
 // of popcounts.  Writes the sorted set-bit positions and, for levels >= 1
 // when wpre is given, the rank at each non-empty word (rank_of's table).
+// In a region-mode mesh a word of levels 0-3 lies inside one level-0 region
+// (level-l word w covers level-0 words w * 8^l ..): an unflagged one is
+// empty and is not read.
 __global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total) {
     const uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (gi >= ((total + 31) & ~31ull)) return;  // whole warps stay for the shuffles
@@ -423,7 +426,7 @@ __global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total
         l = job.l0;
         while (l + 1 < job.l1 && gw >= py.woff[l + 1]) ++l;
         w = gw - py.woff[l];
-        v = (l == 0 && job.rflag && !job.rflag[w >> 11]) ? 0ull : job.bits[gw];
+        v = (l <= 3 && job.rflag && !job.rflag[w >> (11 - 3 * l)]) ? 0ull : job.bits[gw];
         if (v) r = job.pre[py.coff[l] + (w >> 3)] - job.pre[py.coff[l]];
     }
     const uint32_t pc = __popcll(v);
