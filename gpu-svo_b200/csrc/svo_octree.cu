@@ -594,19 +594,38 @@ __device__ __forceinline__ void full_neighbors(const EmitParams &P, const NodeIn
         const bool ex = in[b] && ((wd[b] >> sh) & 1ull);
         base[b] = ex ? P.lv[ni.l].off + 8u * (wp[b] + (uint32_t)__popcll(wd[b] & ((1ull << sh) - 1ull))) : kNone;
     }
+    // Neighbour d = base[b] | k with, per axis a, (b_a, k_a) = (1, 1), (0, 0),
+    // (0, 1) for d_a = -1, 0, +1 when s_a = 0 and (0, 0), (0, 1), (1, 0) when
+    // s_a = 1 (every base is a multiple of 8, and kNone | k = kNone): the
+    // 3 x 3 x 3 table follows from the 8 bases one axis at a time.
+    const uint32_t sxa = s & 1u, sya = (s >> 1) & 1u, sza = (s >> 2) & 1u;
+    uint32_t X[3][4];  // [dx + 1][b_y | b_z << 1]
 #pragma unroll
-    for (int j = 0; j < 27; ++j) {
-        if (j == 13) continue;
-        const int d[3] = {j % 3 - 1, (j / 3) % 3 - 1, j / 9 - 1};
-        int b = 0, k = 0;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const int sa = (int)((s >> a) & 1);
-            if (d[a] != 0 && (d[a] > 0) == (sa == 1)) b |= 1 << a;
-            k |= (sa ^ (d[a] != 0 ? 1 : 0)) << a;
-        }
-        nb[j] = base[b] == kNone ? kNone : base[b] + (uint32_t)k;
+    for (int r = 0; r < 4; ++r) {
+        const uint32_t b0 = base[r << 1], b1 = base[(r << 1) | 1];
+        X[0][r] = sxa ? b0 : (b1 | 1u);
+        X[1][r] = b0 | sxa;
+        X[2][r] = sxa ? b1 : (b0 | 1u);
     }
+    uint32_t Y[3][3][2];  // [dx + 1][dy + 1][b_z]
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int z = 0; z < 2; ++z) {
+            const uint32_t c0 = X[i][z << 1], c1 = X[i][(z << 1) | 1];
+            Y[i][0][z] = sya ? c0 : (c1 | 2u);
+            Y[i][1][z] = c0 | (sya << 1);
+            Y[i][2][z] = sya ? c1 : (c0 | 2u);
+        }
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int jy = 0; jy < 3; ++jy) {
+            const uint32_t c0 = Y[i][jy][0], c1 = Y[i][jy][1];
+            nb[i + 3 * jy] = sza ? c0 : (c1 | 4u);
+            nb[i + 3 * jy + 9] = c0 | (sza << 2);
+            nb[i + 3 * jy + 18] = sza ? c1 : (c0 | 4u);
+        }
 }
 
 // Corners (Morton-numbered) joined by edge e, in the reference's edge order
