@@ -584,6 +584,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             // outputs, code lists, job tables
             std::vector<CompactJob> jobs;
             std::vector<uint64_t> word_off(1, 0);
+            std::vector<CompactJob> region_jobs;  // region-mode meshes' levels 1-2
+            std::vector<uint32_t> region_counts;
             std::vector<KeyJob> kjobs;
             std::vector<uint64_t> blk_off(1, 0);
             std::vector<EmitParams> ep(n);
@@ -672,15 +674,21 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 job.l1 = mh.T + 1;
                 job.out = K + kbase[j];
                 job.wpre = WP + wbase[j];
-                // region mode: words of levels 1-3 of unflagged regions are empty, not read
-                job.rflag = mh.py.words[0] >= kRegionWords ? b->rflag + mh.cta0 : nullptr;
                 uint64_t ko = 0;
                 for (int l = 1; l <= mh.T; ++l) {
                     job.koff[l] = ko;
                     ko += mh.totals[l];
                 }
+                if (mh.py.words[0] >= kRegionWords) {
+                    // region mode: levels 1-2 region by region (k_compact_regions);
+                    // level 3 words of unflagged regions are empty, not read
+                    job.rflag = b->rflag + mh.cta0;
+                    region_jobs.push_back(job);
+                    region_counts.push_back(mh.py.ctas);
+                    job.l0 = 3;
+                }
                 jobs.push_back(job);
-                word_off.push_back(word_off.back() + mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1]);
+                word_off.push_back(word_off.back() + mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[job.l0]);
                 if (want_keys && mh.T >= 3) {
                     // the level-3 code list is the list of non-empty level-0 blocks
                     kjobs.push_back(KeyJob{md.bits, md.pre, job.out + job.koff[3], r->keys});
@@ -745,6 +753,8 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             check(upload(d_top_ptr, top_ptr, st), "upload");
             tm.mark(StageTimer::kCompact0, st);
             check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
+            for (size_t i = 0; i < region_jobs.size(); ++i)
+                check(launch_compact_regions(region_jobs[i], region_counts[i], st), "compact");
             if (!kjobs.empty())
                 check(launch_compact_keys(KeyBatch{d_kjobs, (int)kjobs.size(), d_blk_off}, blk_off.back(), st), "keys");
             tm.mark(StageTimer::kCompact, st);

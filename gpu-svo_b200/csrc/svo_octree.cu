@@ -411,12 +411,34 @@ __global__ void k_level_totals(BatchDev bd) {
 // In a region-mode mesh a word of levels 0-3 lies inside one level-0 region
 // (level-l word w covers level-0 words w * 8^l ..): an unflagged one is
 // empty and is not read.
+// Word w of level l holding v (read by the caller; 0 for a lane without a
+// word): rank from the block prefix and the 8-lane popcount prefix, then the
+// positions.  All 32 lanes of the warp call (8 aligned lanes per block).
+__device__ __forceinline__ void compact_word(const CompactJob &job, int l, uint64_t w, uint64_t v) {
+    const int sub = threadIdx.x & 7;
+    const uint32_t r0 = v ? job.pre[job.py.coff[l] + (w >> 3)] - job.pre[job.py.coff[l]] : 0u;
+    const uint32_t pc = __popcll(v);
+    uint32_t x = pc;
+#pragma unroll
+    for (int d = 1; d < 8; d <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d, 8);
+        if (sub >= d) x += y;
+    }
+    if (!v) return;
+    const uint32_t r = r0 + x - pc;
+    if (job.wpre && l >= 1) job.wpre[job.py.woff[l] - job.py.woff[1] + w] = r;
+    uint64_t *o = job.out + job.koff[l] + r;
+    const uint64_t b64 = w * 64;
+    while (v) {
+        *o++ = b64 + __ffsll((long long)v) - 1;
+        v &= v - 1;
+    }
+}
+
 __global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total) {
     const uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     if (gi >= ((total + 31) & ~31ull)) return;  // whole warps stay for the shuffles
-    const int sub = threadIdx.x & 7;
     uint64_t v = 0, w = 0;
-    uint32_t r = 0;
     int l = 0, j = 0;
     if (gi < total) {
         j = find_segment(cb.word_off, cb.n, gi);
@@ -427,24 +449,21 @@ __global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total
         while (l + 1 < job.l1 && gw >= py.woff[l + 1]) ++l;
         w = gw - py.woff[l];
         v = (l <= 3 && job.rflag && !job.rflag[w >> (11 - 3 * l)]) ? 0ull : job.bits[gw];
-        if (v) r = job.pre[py.coff[l] + (w >> 3)] - job.pre[py.coff[l]];
     }
-    const uint32_t pc = __popcll(v);
-    uint32_t x = pc;
-#pragma unroll
-    for (int d = 1; d < 8; d <<= 1) {
-        const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d, 8);
-        if (sub >= d) x += y;
-    }
-    if (!v) return;
-    r += x - pc;
-    const CompactJob &job = cb.job[j];
-    if (job.wpre && l >= 1) job.wpre[job.py.woff[l] - job.py.woff[1] + w] = r;
-    uint64_t *o = job.out + job.koff[l] + r;
-    const uint64_t b64 = w * 64;
-    while (v) {
-        *o++ = b64 + __ffsll((long long)v) - 1;
-        v &= v - 1;
+    compact_word(cb.job[j], l, w, v);
+}
+
+// Levels 1 and 2 of a region-mode mesh, one block per level-0 region: the
+// 256 level-1 and 32 level-2 words above a region lie inside it, so the
+// block of an unflagged region returns at once (most of them at res 2048).
+__global__ void __launch_bounds__(256) k_compact_regions(const __grid_constant__ CompactJob job) {
+    const uint32_t rg = blockIdx.x;
+    if (!job.rflag[rg]) return;
+    const uint64_t w1 = (uint64_t)rg * 256 + threadIdx.x;
+    compact_word(job, 1, w1, job.bits[job.py.woff[1] + w1]);
+    if (threadIdx.x < 32) {
+        const uint64_t w2 = (uint64_t)rg * 32 + threadIdx.x;
+        compact_word(job, 2, w2, job.bits[job.py.woff[2] + w2]);
     }
 }
 
@@ -980,6 +999,13 @@ cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st) {
 cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st) {
     if (total_words == 0) return cudaSuccess;
     k_compact<<<(unsigned)((total_words + 255) / 256), 256, 0, st>>>(c, total_words);
+    count_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_compact_regions(const CompactJob &job, uint32_t regions, cudaStream_t st) {
+    if (regions == 0) return cudaSuccess;
+    k_compact_regions<<<regions, 256, 0, st>>>(job);
     count_launches(1);
     return cudaGetLastError();
 }

@@ -880,30 +880,54 @@ namespace {
 // reciprocal voxel size in place of the division: the two differ by a few
 // ulps at coordinates <= 2048, far less than the margin, so the flagged
 // regions cover every voxel the voxel test can set.
+// Bits of v (< 2^10) spread to every third bit.
+__device__ __forceinline__ uint32_t spread3_small(uint32_t v) {
+    v = (v | (v << 16)) & 0x030000FFu;
+    v = (v | (v << 8)) & 0x0300F00Fu;
+    v = (v | (v << 4)) & 0x030C30C3u;
+    return (v | (v << 2)) & 0x09249249u;
+}
+
+// The flags of the level-0 regions (64 x 64 x 32 voxels, region index =
+// morton3(x, y, z) >> 17) each triangle's voxel box (with a one-voxel margin)
+// reaches.  The mesh's grid and reciprocal units are kept across the
+// grid-stride loop while the mesh stays the same.
 __global__ void __launch_bounds__(256) k_region_mark(BatchDev bd, int64_t total) {
+    int cur = -1;
+    bool regions = false;
+    float org[3] = {0, 0, 0}, inv[3] = {0, 0, 0};
     for (int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gid < total;
          gid += (int64_t)gridDim.x * blockDim.x) {
         const int m = find_segment(bd.tri_off, bd.n, (uint64_t)gid);
         const MeshDev &md = bd.mesh[m];
-        if (!md.regions) continue;
-        const GridParams g = *md.gp;
+        if (m != cur) {
+            cur = m;
+            regions = md.regions != 0;
+            const GridParams g = *md.gp;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                org[a] = g.origin[a];
+                inv[a] = __frcp_rn(g.unit[a]);
+            }
+        }
+        if (!regions) continue;
         float p[3][3];
         if (!load_tri_checked(md.pts, md.tris, md.n_pts, gid - (int64_t)bd.tri_off[m], p)) continue;  // k_voxelize reports it
         int lo[3], hi[3];
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const float v0 = __fsub_rn(p[0][a], g.origin[a]), v1 = __fsub_rn(p[1][a], g.origin[a]),
-                        v2 = __fsub_rn(p[2][a], g.origin[a]);
-            const float inv = __frcp_rn(g.unit[a]);
+            const float v0 = __fsub_rn(p[0][a], org[a]), v1 = __fsub_rn(p[1][a], org[a]),
+                        v2 = __fsub_rn(p[2][a], org[a]);
             // the margin is applied before the conversion, so +-inf and NaN clamp as in tri_box
-            lo[a] = clampi(f2i_rz(__fsub_rn(__fmul_rn(cminf(v0, cminf(v1, v2)), inv), 1.0f)), 0, md.res[a] - 1);
-            hi[a] = clampi(f2i_rz(__fadd_rn(__fmul_rn(cmaxf(v0, cmaxf(v1, v2)), inv), 1.0f)), 0, md.res[a] - 1);
+            lo[a] = clampi(f2i_rz(__fsub_rn(__fmul_rn(cminf(v0, cminf(v1, v2)), inv[a]), 1.0f)), 0, md.res[a] - 1);
+            hi[a] = clampi(f2i_rz(__fadd_rn(__fmul_rn(cmaxf(v0, cmaxf(v1, v2)), inv[a]), 1.0f)), 0, md.res[a] - 1);
         }
         uint8_t *flag = bd.rflag + bd.cta_off[m];
+        // region bits: z at 3i, x at 3i + 1, y at 3i + 2 (z in 32-voxel, x and y in 64-voxel steps)
         for (uint32_t rz = (uint32_t)lo[2] >> 5; rz <= (uint32_t)hi[2] >> 5; ++rz)
             for (uint32_t ry = (uint32_t)lo[1] >> 6; ry <= (uint32_t)hi[1] >> 6; ++ry)
                 for (uint32_t rx = (uint32_t)lo[0] >> 6; rx <= (uint32_t)hi[0] >> 6; ++rx) {
-                    uint8_t *f = flag + (morton3(rx << 6, ry << 6, rz << 5) >> 17);
+                    uint8_t *f = flag + (spread3_small(rz) | spread3_small(rx) << 1 | spread3_small(ry) << 2);
                     if (!*f) *f = 1;
                 }
     }
