@@ -581,6 +581,55 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
         // status loop below, which marks every mesh of the wave as failed.
         const int wave_rc = [&]() -> int {
             cudaError_t err = cudaSuccess;
+            // The dedup keys read only the bitmaps and code lists: they run on
+            // a stream of their own, forked here, where their first step (the
+            // level-1 candidate bitmap, from the bitmaps alone) runs while the
+            // host prepares the wave; the rest follows the code lists and runs
+            // beside the emission.  The wave joins it before returning.
+            const bool dd = (flags & SVO_FLAG_DEDUP) != 0;
+            AuxStreams *dset = dd ? aux_acquire(ctx) : nullptr;
+            const cudaStream_t ds = dset ? dset->s[0] : st;
+            auto join_dedup = [&]() {
+                if (!dset) return;
+                check(cudaEventRecord(dset->join[0], ds), "join");
+                check(cudaStreamWaitEvent(st, dset->join[0], 0), "join");
+                aux_release(ctx, dset);
+                dset = nullptr;
+            };
+            std::vector<DedupRun *> druns(n, nullptr);
+            std::vector<int> drc(n, SVO_OK);
+            std::vector<std::string> dmsg(n);
+            struct DedupGuard {  // on every exit: unfinished runs freed, the dedup stream joined
+                std::vector<DedupRun *> &runs;
+                decltype(join_dedup) &join;
+                ~DedupGuard() {
+                    for (DedupRun *&r : runs) {
+                        dedup_abort(r);
+                        r = nullptr;
+                    }
+                    join();
+                }
+            } dguard{druns, join_dedup};
+            if (dd) {
+                if (dset) {
+                    check(cudaEventRecord(dset->fork, st), "fork");
+                    check(cudaStreamWaitEvent(ds, dset->fork, 0), "fork");
+                }
+                tm.mark(StageTimer::kDedup0, ds);
+                for (int j = 0; j < n; ++j) {
+                    const MeshHost &mh = b->m[wave[j]];
+                    const MeshDev &md = b->h_mesh[dev_k[j]];
+                    const uint32_t R = 1u << (mh.py.grid_levels - 1);
+                    const uint64_t *bits[kMaxLevels];
+                    uint32_t sides[kMaxLevels];
+                    for (int l = 0; l <= mh.T && l < kMaxLevels; ++l) {
+                        bits[l] = md.bits + mh.py.woff[l];
+                        sides[l] = std::max<uint32_t>(1u, R >> l);
+                    }
+                    drc[j] = dedup_begin(ctx->pool, ds, mh.T, bits, sides, ctx->num_sms, &druns[j]);
+                    if (drc[j] != SVO_OK) dmsg[j] = svo_last_error();
+                }
+            }
             // outputs, code lists, job tables
             std::vector<CompactJob> jobs;
             std::vector<uint64_t> word_off(1, 0);
@@ -760,20 +809,11 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             tm.mark(StageTimer::kCompact, st);
             // The dedup keys read only the bitmaps and code lists: they run on
             // a stream of their own, forked here, while the emission writes.
-            const bool dd = (flags & SVO_FLAG_DEDUP) != 0;
-            AuxStreams *dset = dd ? aux_acquire(ctx) : nullptr;
-            const cudaStream_t ds = dset ? dset->s[0] : st;
+            // the dedup's coarse marks, states and keys need the code lists
             if (dset) {
                 check(cudaEventRecord(dset->fork, st), "fork");
                 check(cudaStreamWaitEvent(ds, dset->fork, 0), "fork");
             }
-            auto join_dedup = [&]() {
-                if (!dset) return;
-                check(cudaEventRecord(dset->join[0], ds), "join");
-                check(cudaStreamWaitEvent(st, dset->join[0], 0), "join");
-                aux_release(ctx, dset);
-                dset = nullptr;
-            };
             // Large meshes get launches of their own (parameters in the kernel's
             // constant space); the rest share one launch over the mesh table.
             // With two or more of them, they spread round-robin over the build
@@ -828,14 +868,11 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             // Dedup of every mesh on the forked stream (its host-side waits
             // overlap the emission running on the GPU); statuses are applied
             // after the emission's own checks.
-            std::vector<int> drc(n, SVO_OK);
-            std::vector<std::string> dmsg(n);
             if (dd) {
-                tm.mark(StageTimer::kDedup0, ds);
                 for (int j = 0; j < n && rc == SVO_OK; ++j) {
-                    if (b->m[wave[j]].status != SVO_OK) continue;
-                    drc[j] = build_dedup(ctx->pool, ctx->out_pool, ds, ep[j], res[j]->n_dedup, res[j]->dedup,
-                                         ctx->num_sms);
+                    if (b->m[wave[j]].status != SVO_OK || !druns[j]) continue;
+                    drc[j] = dedup_finish(druns[j], ctx->out_pool, ep[j], res[j]->n_dedup, res[j]->dedup);
+                    druns[j] = nullptr;
                     if (drc[j] != SVO_OK) dmsg[j] = svo_last_error();
                 }
                 tm.mark(StageTimer::kDedup, ds);

@@ -28,6 +28,7 @@
 // D has R^3 bits (1 GiB at R = 2048); a 1-bit-per-chunk summary lets the walk
 // skip untouched chunks without reading them.
 #include <cstdio>
+#include <cstring>
 
 #include "svo_host.h"
 #include "svo_internal.h"
@@ -704,63 +705,69 @@ int dedup_fail(int code, const char *msg) {
 
 }  // namespace
 
-int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, const EmitParams &ep,
-                uint64_t n_out[3], uint64_t *out[3], int num_sms) {
-    svo::host::TraceRange trace("svo: dedup keys");
-    for (int k = 0; k < 3; ++k) {
-        n_out[k] = 0;
-        out[k] = nullptr;
-    }
-    const int T = ep.T;
+// A dedup between dedup_begin (scratch, tables, the candidate bitmap's
+// level-1 part: bitmaps only) and dedup_finish (coarse marks, states, keys:
+// they need the code lists).  Its scratch is freed on its stream.
+struct DedupRun {
+    cudaMemPool_t pool;
+    cudaStream_t st;
+    int num_sms;
+    DedupParams p;
+    void *blk[8];
+    size_t sz[8];
+    uint64_t side, d_words, g_words;
+    bool build1;
+};
+
+void dedup_abort(DedupRun *run) {
+    if (!run) return;
+    for (void *b : run->blk)
+        if (b) cudaFreeAsync(b, run->st);
+    delete run;
+}
+
+int dedup_begin(cudaMemPool_t pool, cudaStream_t st, int T, const uint64_t *const *bits, const uint32_t *sides,
+                int num_sms, DedupRun **out) {
+    svo::host::TraceRange trace("svo: dedup candidates");
+    *out = nullptr;
     if (T < 1) return dedup_fail(SVO_ERR_DEGENERATE, "dedup needs at least two levels");
     if (T > 12) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup of more than 13 levels");
-    if ((uint64_t)ep.N * 12 > 0xFFFFFFFFull) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup of more than 357M nodes");
-    DedupParams p{};
+    DedupRun *run = new DedupRun{};
+    run->pool = pool;
+    run->st = st;
+    run->num_sms = num_sms;
+    DedupParams &p = run->p;
     p.T = T;
-    p.root = ep.lv[T].K1;
-    for (int l = 0; l <= T; ++l) p.lv[l] = DedupLevel{ep.lv[l].bits, ep.lv[l].K1, ep.lv[l].n / 8, ep.lv[l].side};
-    uint32_t g = 0;
-    for (int l = 1; l < T; ++l) {
-        p.gstart[l] = g;
-        g += p.lv[l].groups;
-    }
-    p.gstart[T] = g;
-    const uint32_t mark_total = g + 1;
-    const uint64_t side = ep.lv[0].side;
+    for (int l = 0; l <= T; ++l) p.lv[l] = DedupLevel{bits[l], nullptr, 0, sides[l]};
+    const uint64_t side = sides[0];
     const uint64_t d_bits = side * side * side;
     const uint64_t d_words = std::max<uint64_t>((d_bits + 63) / 64 + kChunkWords - 1, kChunkWords) / kChunkWords * kChunkWords;
     p.chunks = d_words / kChunkWords;
     const uint64_t g_words = (p.chunks + 31) / 32;
-
-    if (p.chunks > 0xFFFFFFFFull) return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup grid too large");
+    run->side = side;
+    run->d_words = d_words;
+    run->g_words = g_words;
+    if (p.chunks > 0xFFFFFFFFull) {
+        delete run;
+        return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup grid too large");
+    }
     // scratch: D, G, G popcounts + prefix, touched list, scan scratch, status, tables
-    void *blk[8] = {};
     const size_t sz[8] = {d_words * 8, g_words * 4, g_words * 4, (g_words + 1) * 4, p.chunks * 4,
                           scan_scratch_words(std::max<uint64_t>(p.chunks, g_words)) * 8, 256, sizeof(DedupTables)};
-    void *blk2[6] = {};  // sized once the counts are known: states per chunk, the states, keys per tile
+    std::memcpy(run->sz, sz, sizeof sz);
     cudaError_t e = cudaSuccess;
-    for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = pool_malloc(&blk[i], sz[i], pool, st);
-    auto release = [&]() {
-        for (void *b : blk)
-            if (b) cudaFreeAsync(b, st);
-        for (void *b : blk2)
-            if (b) cudaFreeAsync(b, st);
-    };
+    for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = pool_malloc(&run->blk[i], sz[i], pool, st);
     auto fail = [&](cudaError_t err, const char *what) {
-        release();
+        dedup_abort(run);
         char msg[256];
         snprintf(msg, sizeof msg, "dedup %s: %s", what, cudaGetErrorString(err));
         return dedup_fail(err == cudaErrorMemoryAllocation ? SVO_ERR_OUT_OF_MEMORY : SVO_ERR_CUDA, msg);
     };
     if (e != cudaSuccess) return fail(e, "scratch");
+    void **blk = run->blk;
     p.D = static_cast<uint32_t *>(blk[0]);
     p.G = static_cast<uint32_t *>(blk[1]);
-    uint32_t *gcnt = static_cast<uint32_t *>(blk[2]);
-    uint32_t *gpre = static_cast<uint32_t *>(blk[3]);
-    uint32_t *list = static_cast<uint32_t *>(blk[4]);
-    p.list = list;
-    auto *scan = static_cast<unsigned long long *>(blk[5]);
-    uint32_t *status = static_cast<uint32_t *>(blk[6]);
+    p.list = static_cast<uint32_t *>(blk[4]);
     p.nq = reinterpret_cast<unsigned long long *>(static_cast<char *>(blk[6]) + 8);
     p.tables = static_cast<const DedupTables *>(blk[7]);
     k_dedup_tables<<<1, 256, 0, st>>>(static_cast<DedupTables *>(blk[7]));
@@ -768,7 +775,8 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
     // D: in 2048-word regions, level 1 by k_dedup_build (T >= 2), the
     // coarser levels marked after it; else zeroed and marked at all levels
     const bool build1 = d_words % 2048 == 0 && T >= 2;
-    if ((e = cudaMemsetAsync(p.G, 0, sz[1], st)) || (e = cudaMemsetAsync(status, 0, 16, st)))
+    run->build1 = build1;
+    if ((e = cudaMemsetAsync(p.G, 0, sz[1], st)) || (e = cudaMemsetAsync(blk[6], 0, 16, st)))
         return fail(e, "memset");
     if (d_words % 2048 == 0) {
         const uint64_t regions = d_words / 2048;
@@ -783,6 +791,58 @@ int build_dedup(cudaMemPool_t pool, cudaMemPool_t out_pool, cudaStream_t st, con
         e = cudaMemsetAsync(p.D, 0, sz[0], st);
     }
     if (e != cudaSuccess) return fail(e, "clear");
+    *out = run;
+    return SVO_OK;
+}
+
+int dedup_finish(DedupRun *run, cudaMemPool_t out_pool, const EmitParams &ep, uint64_t n_out[3], uint64_t *out[3]) {
+    svo::host::TraceRange trace("svo: dedup keys");
+    for (int k = 0; k < 3; ++k) {
+        n_out[k] = 0;
+        out[k] = nullptr;
+    }
+    const cudaMemPool_t pool = run->pool;
+    const cudaStream_t st = run->st;
+    const int num_sms = run->num_sms;
+    DedupParams &p = run->p;
+    const int T = p.T;
+    if (ep.T != T || (uint64_t)ep.N * 12 > 0xFFFFFFFFull) {
+        dedup_abort(run);
+        return dedup_fail(SVO_ERR_UNSUPPORTED, "dedup of more than 357M nodes");
+    }
+    p.root = ep.lv[T].K1;
+    for (int l = 0; l <= T; ++l) {
+        p.lv[l].K1 = ep.lv[l].K1;
+        p.lv[l].groups = ep.lv[l].n / 8;
+    }
+    uint32_t g = 0;
+    for (int l = 1; l < T; ++l) {
+        p.gstart[l] = g;
+        g += p.lv[l].groups;
+    }
+    p.gstart[T] = g;
+    const uint32_t mark_total = g + 1;
+    const uint64_t g_words = run->g_words;
+    void **blk = run->blk;
+    void *blk2[6] = {};  // sized once the counts are known: states per chunk, the states, keys per tile
+    uint32_t *gcnt = static_cast<uint32_t *>(blk[2]);
+    uint32_t *gpre = static_cast<uint32_t *>(blk[3]);
+    uint32_t *list = static_cast<uint32_t *>(blk[4]);
+    auto *scan = static_cast<unsigned long long *>(blk[5]);
+    uint32_t *status = static_cast<uint32_t *>(blk[6]);
+    cudaError_t e = cudaSuccess;
+    auto release = [&]() {
+        for (void *b : blk2)
+            if (b) cudaFreeAsync(b, st);
+        dedup_abort(run);
+    };
+    auto fail = [&](cudaError_t err, const char *what) {
+        release();
+        char msg[256];
+        snprintf(msg, sizeof msg, "dedup %s: %s", what, cudaGetErrorString(err));
+        return dedup_fail(err == cudaErrorMemoryAllocation ? SVO_ERR_OUT_OF_MEMORY : SVO_ERR_CUDA, msg);
+    };
+    const bool build1 = run->build1;
     const uint32_t mark_first = build1 ? p.gstart[2] : 0u;
     k_dedup_mark<<<(mark_total - mark_first + 255) / 256, 256, 0, st>>>(p, mark_first, mark_total);
     k_touched_count<<<(unsigned)((g_words + 255) / 256), 256, 0, st>>>(p.G, g_words, gcnt);

@@ -216,9 +216,17 @@ cudaError_t launch_unique_edges(const svo_edge *in, uint64_t n, svo_edge *out, u
                                 uint32_t *status, cudaStream_t st);
 constexpr uint32_t kUniqueTile = 4096;
 
-// Morton-keyed unique vertex/edge/face keys of all nodes (SVO_FLAG_DEDUP).
-int build_dedup(cudaMemPool_t scratch_pool, cudaMemPool_t out_pool, cudaStream_t st, const EmitParams &p,
-                uint64_t n_out[3], uint64_t *out[3], int num_sms);
+// Morton-keyed unique vertex/edge/face keys of all nodes (SVO_FLAG_DEDUP), in
+// two steps on one stream.  dedup_begin needs only the level bitmaps (bits[l],
+// side sides[l], l = 0..T): it takes the scratch and builds the level-1 part
+// of the candidate bitmap, so it can run before the code lists exist.
+// dedup_finish (after the code lists, ep) writes the keys and frees the run;
+// dedup_abort frees a run that will not be finished.
+struct DedupRun;
+int dedup_begin(cudaMemPool_t scratch_pool, cudaStream_t st, int T, const uint64_t *const *bits,
+                const uint32_t *sides, int num_sms, DedupRun **run);
+int dedup_finish(DedupRun *run, cudaMemPool_t out_pool, const EmitParams &ep, uint64_t n_out[3], uint64_t *out[3]);
+void dedup_abort(DedupRun *run);
 
 // Blocks of the bbox reduction for a mesh of n points.
 inline uint32_t bbox_blocks(int64_t n) {
