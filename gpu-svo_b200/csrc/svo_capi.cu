@@ -263,6 +263,32 @@ int mesh_error(MeshHost &mh, int code, const char *msg) {
     return code;
 }
 
+// Offsets of arrays laid out one after another in one block (256-byte aligned):
+// fewer pool allocations per build.
+struct Layout {
+    size_t bytes = 0;
+    template <class T>
+    size_t add(size_t count) {
+        const size_t at = bytes;
+        bytes += (std::max<size_t>(count * sizeof(T), 1) + 255) / 256 * 256;
+        return at;
+    }
+};
+
+// Small host tables packed into one buffer, uploaded with one copy.
+struct HostPack {
+    std::vector<unsigned char> buf;
+    template <class T>
+    size_t add(const T *src, size_t count) {
+        const size_t at = (buf.size() + 15) / 16 * 16;
+        buf.resize(at + count * sizeof(T));
+        if (count) std::memcpy(buf.data() + at, src, count * sizeof(T));
+        return at;
+    }
+    template <class T>
+    size_t add(const std::vector<T> &v) { return add(v.data(), v.size()); }
+};
+
 template <class T>
 cudaError_t upload(T *dst, const std::vector<T> &src, cudaStream_t st) {
     if (src.empty()) return cudaSuccess;
@@ -354,19 +380,26 @@ int batch_phase_a(svo_batch *b) {
     cta_off[n] = ctas;
     bbox_off[n] = bblocks;
     b->total_blocks = blocks;
-    b->bits = batch_alloc<uint64_t>(b, words, err);
-    b->cnt = batch_alloc<uint32_t>(b, blocks, err);
-    b->pre = batch_alloc<uint32_t>(b, blocks + 1, err);
-    unsigned long long *scan = batch_alloc<unsigned long long>(b, scan_scratch_words(blocks), err);
-    b->d_mesh = batch_alloc<MeshDev>(b, n, err);
-    uint64_t *d_tri_off = batch_alloc<uint64_t>(b, n + 1, err);
-    uint32_t *d_cta_off = batch_alloc<uint32_t>(b, n + 1, err);
-    uint32_t *d_bbox_off = batch_alloc<uint32_t>(b, n + 1, err);
+    // the batch's scratch arrays and its mesh tables: one block, one upload
     uint32_t big_cap = (uint32_t)std::min<uint64_t>(std::max<uint64_t>(2 * tris, 1 << 16), 0x7FFFFFFFu);
-    uint4 *big = batch_alloc<uint4>(b, big_cap, err);
-    uint64_t *small = big ? batch_alloc<uint64_t>(b, std::max<uint64_t>(tris, 1), err) : nullptr;
-    uint8_t *rflag = b->rflag = batch_alloc<uint8_t>(b, std::max<uint32_t>(ctas, 1), err);
-    if (err != cudaSuccess) return cuda_fail(err, "batch scratch");
+    HostPack tables;  // mesh table, triangle / CTA / bbox-block offsets (filled below)
+    auto a16 = [](size_t x) { return (x + 15) / 16 * 16; };
+    const size_t t_bytes = a16(sizeof(MeshDev) * n) + a16(8 * (size_t)(n + 1)) + a16(4 * (size_t)(n + 1)) + 4 * (size_t)(n + 1);
+    Layout lay;
+    const size_t o_bits = lay.add<uint64_t>(words), o_cnt = lay.add<uint32_t>(blocks),
+                 o_pre = lay.add<uint32_t>(blocks + 1), o_scan = lay.add<unsigned long long>(scan_scratch_words(blocks)),
+                 o_big = lay.add<uint4>(big_cap), o_small = lay.add<uint64_t>(std::max<uint64_t>(tris, 1)),
+                 o_rflag = lay.add<uint8_t>(std::max<uint32_t>(ctas, 1));
+    const size_t o_tables = lay.add<unsigned char>(t_bytes);
+    unsigned char *blk = batch_alloc<unsigned char>(b, lay.bytes, err);
+    if (err != cudaSuccess || !blk) return cuda_fail(err, "batch scratch");
+    b->bits = reinterpret_cast<uint64_t *>(blk + o_bits);
+    b->cnt = reinterpret_cast<uint32_t *>(blk + o_cnt);
+    b->pre = reinterpret_cast<uint32_t *>(blk + o_pre);
+    unsigned long long *scan = reinterpret_cast<unsigned long long *>(blk + o_scan);
+    uint4 *big = reinterpret_cast<uint4 *>(blk + o_big);
+    uint64_t *small = reinterpret_cast<uint64_t *>(blk + o_small);
+    uint8_t *rflag = b->rflag = blk + o_rflag;
     GridParams *gp = reinterpret_cast<GridParams *>(b->meta + ml.gp);
     uint32_t *totals = reinterpret_cast<uint32_t *>(b->meta + ml.totals);
     uint32_t *mm = reinterpret_cast<uint32_t *>(b->meta + ml.mm);
@@ -391,10 +424,14 @@ int batch_phase_a(svo_batch *b) {
         d.py = mh.py;
         d.regions = mh.py.words[0] >= kRegionWords ? 1 : 0;
     }
-    SVO_TRY(upload(b->d_mesh, b->h_mesh, st), "upload meshes");
-    SVO_TRY(upload(d_tri_off, tri_off, st), "upload");
-    SVO_TRY(upload(d_cta_off, cta_off, st), "upload");
-    SVO_TRY(upload(d_bbox_off, bbox_off, st), "upload");
+    const size_t p_mesh = tables.add(b->h_mesh), p_tri = tables.add(tri_off), p_cta = tables.add(cta_off),
+                 p_bbox = tables.add(bbox_off);
+    unsigned char *dt = blk + o_tables;
+    b->d_mesh = reinterpret_cast<MeshDev *>(dt + p_mesh);
+    const uint64_t *d_tri_off = reinterpret_cast<const uint64_t *>(dt + p_tri);
+    const uint32_t *d_cta_off = reinterpret_cast<const uint32_t *>(dt + p_cta);
+    const uint32_t *d_bbox_off = reinterpret_cast<const uint32_t *>(dt + p_bbox);
+    SVO_TRY(cudaMemcpyAsync(dt, tables.buf.data(), tables.buf.size(), cudaMemcpyHostToDevice, st), "upload meshes");
     const BatchDev bd{b->d_mesh, n, d_tri_off, d_cta_off, d_bbox_off, rflag};
     const bool strict = (b->flags & SVO_FLAG_STRICT_FP) != 0;
     StageTimer tm((b->flags & SVO_FLAG_TIMINGS) != 0);
@@ -646,7 +683,6 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 kbase[j] = ktot;
                 for (int l = 1; l <= mh.T; ++l) ktot += mh.totals[l];
             }
-            uint64_t *K = S.get<uint64_t>(ktot + 1);
             // per-word ranks of levels >= 1 (k_compact writes them, rank lookups read them)
             uint64_t wtot = 0;
             std::vector<uint64_t> wbase(n);
@@ -655,10 +691,16 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 wbase[j] = wtot;
                 wtot += mh.py.woff[mh.T] + mh.py.words[mh.T] - mh.py.woff[1];
             }
-            uint32_t *WP = S.get<uint32_t>(wtot + 1);
-            unsigned long long *dups = S.get<unsigned long long>(2 * (size_t)n);
-            uint64_t *top = S.get<uint64_t>(n);
-            if (!K || !WP || !dups || !top) return cuda_fail(S.err, "wave scratch");
+            // code lists, word ranks, duplicate counts, top codes: one block
+            Layout wl;
+            const size_t o_K = wl.add<uint64_t>(ktot + 1), o_WP = wl.add<uint32_t>(wtot + 1),
+                         o_dups = wl.add<unsigned long long>(2 * (size_t)n), o_top = wl.add<uint64_t>(n);
+            unsigned char *wblk = S.get<unsigned char>(wl.bytes);
+            if (!wblk) return cuda_fail(S.err, "wave scratch");
+            uint64_t *K = reinterpret_cast<uint64_t *>(wblk + o_K);
+            uint32_t *WP = reinterpret_cast<uint32_t *>(wblk + o_WP);
+            unsigned long long *dups = reinterpret_cast<unsigned long long *>(wblk + o_dups);
+            uint64_t *top = reinterpret_cast<uint64_t *>(wblk + o_top);
             check(cudaMemsetAsync(dups, 0, 16 * (size_t)n, st), "memset");
             // one block for the output arrays of the whole wave
             size_t arena_bytes = 0;
@@ -783,23 +825,22 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                 drop_arena();
                 return cuda_fail(err, "output allocation");
             }
-            CompactJob *d_jobs = S.get<CompactJob>(jobs.size());
-            uint64_t *d_word_off = S.get<uint64_t>(word_off.size());
-            KeyJob *d_kjobs = kjobs.empty() ? nullptr : S.get<KeyJob>(kjobs.size());
-            uint64_t *d_blk_off = kjobs.empty() ? nullptr : S.get<uint64_t>(blk_off.size());
-            const uint64_t **d_top_ptr = S.get<const uint64_t *>(n);
+            // the wave's job tables: one block, one upload
+            HostPack wt;
+            const size_t p_jobs = wt.add(jobs), p_woff = wt.add(word_off), p_kjobs = wt.add(kjobs),
+                         p_boff = wt.add(blk_off), p_top = wt.add(top_ptr);
+            unsigned char *dwt = S.get<unsigned char>(wt.buf.size());
+            CompactJob *d_jobs = dwt ? reinterpret_cast<CompactJob *>(dwt + p_jobs) : nullptr;
+            uint64_t *d_word_off = dwt ? reinterpret_cast<uint64_t *>(dwt + p_woff) : nullptr;
+            KeyJob *d_kjobs = (dwt && !kjobs.empty()) ? reinterpret_cast<KeyJob *>(dwt + p_kjobs) : nullptr;
+            uint64_t *d_blk_off = (dwt && !kjobs.empty()) ? reinterpret_cast<uint64_t *>(dwt + p_boff) : nullptr;
+            const uint64_t **d_top_ptr = dwt ? reinterpret_cast<const uint64_t **>(dwt + p_top) : nullptr;
             if (S.err != cudaSuccess) {
                 free_results();
                 drop_arena();
                 return cuda_fail(S.err, "wave tables");
             }
-            check(upload(d_jobs, jobs, st), "upload");
-            check(upload(d_word_off, word_off, st), "upload");
-            if (!kjobs.empty()) {
-                check(upload(d_kjobs, kjobs, st), "upload");
-                check(upload(d_blk_off, blk_off, st), "upload");
-            }
-            check(upload(d_top_ptr, top_ptr, st), "upload");
+            check(cudaMemcpyAsync(dwt, wt.buf.data(), wt.buf.size(), cudaMemcpyHostToDevice, st), "upload");
             tm.mark(StageTimer::kCompact0, st);
             check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
             for (size_t i = 0; i < region_jobs.size(); ++i)

@@ -713,6 +713,7 @@ struct DedupRun {
     cudaStream_t st;
     int num_sms;
     DedupParams p;
+    void *base;    // one pool block holding blk[0..7]
     void *blk[8];
     size_t sz[8];
     uint64_t side, d_words, g_words;
@@ -721,8 +722,7 @@ struct DedupRun {
 
 void dedup_abort(DedupRun *run) {
     if (!run) return;
-    for (void *b : run->blk)
-        if (b) cudaFreeAsync(b, run->st);
+    if (run->base) cudaFreeAsync(run->base, run->st);
     delete run;
 }
 
@@ -755,8 +755,14 @@ int dedup_begin(cudaMemPool_t pool, cudaStream_t st, int T, const uint64_t *cons
     const size_t sz[8] = {d_words * 8, g_words * 4, g_words * 4, (g_words + 1) * 4, p.chunks * 4,
                           scan_scratch_words(std::max<uint64_t>(p.chunks, g_words)) * 8, 256, sizeof(DedupTables)};
     std::memcpy(run->sz, sz, sizeof sz);
-    cudaError_t e = cudaSuccess;
-    for (int i = 0; i < 8 && e == cudaSuccess; ++i) e = pool_malloc(&run->blk[i], sz[i], pool, st);
+    size_t at[8], total = 0;
+    for (int i = 0; i < 8; ++i) {
+        at[i] = total;
+        total += (sz[i] + 255) / 256 * 256;
+    }
+    cudaError_t e = pool_malloc(&run->base, total, pool, st);
+    if (e == cudaSuccess)
+        for (int i = 0; i < 8; ++i) run->blk[i] = static_cast<char *>(run->base) + at[i];
     auto fail = [&](cudaError_t err, const char *what) {
         dedup_abort(run);
         char msg[256];
@@ -825,6 +831,7 @@ int dedup_finish(DedupRun *run, cudaMemPool_t out_pool, const EmitParams &ep, ui
     const uint64_t g_words = run->g_words;
     void **blk = run->blk;
     void *blk2[6] = {};  // sized once the counts are known: states per chunk, the states, keys per tile
+    void *base2 = nullptr;  // one pool block holding blk2
     uint32_t *gcnt = static_cast<uint32_t *>(blk[2]);
     uint32_t *gpre = static_cast<uint32_t *>(blk[3]);
     uint32_t *list = static_cast<uint32_t *>(blk[4]);
@@ -832,8 +839,7 @@ int dedup_finish(DedupRun *run, cudaMemPool_t out_pool, const EmitParams &ep, ui
     uint32_t *status = static_cast<uint32_t *>(blk[6]);
     cudaError_t e = cudaSuccess;
     auto release = [&]() {
-        for (void *b : blk2)
-            if (b) cudaFreeAsync(b, st);
+        if (base2) cudaFreeAsync(base2, st);
         dedup_abort(run);
     };
     auto fail = [&](cudaError_t err, const char *what) {
@@ -867,8 +873,13 @@ int dedup_finish(DedupRun *run, cudaMemPool_t out_pool, const EmitParams &ep, ui
     const size_t sz2[6] = {std::max<uint64_t>(nt, 1) * 4, (nt + 1) * 4, std::max<uint64_t>(h_nq, 1) * 8,
                            3 * std::max<uint64_t>(ntiles, 1) * 4, 3 * (ntiles + 1) * 4,
                            scan_scratch_words(std::max<uint64_t>(std::max<uint64_t>(nt, ntiles), 1)) * 8};
-    for (int i = 0; i < 6 && e == cudaSuccess; ++i) e = pool_malloc(&blk2[i], sz2[i], pool, st);
-    if (e != cudaSuccess) return fail(e, "scratch");
+    size_t at2[6], total2 = 0;
+    for (int i = 0; i < 6; ++i) {
+        at2[i] = total2;
+        total2 += (sz2[i] + 255) / 256 * 256;
+    }
+    if ((e = pool_malloc(&base2, total2, pool, st)) != cudaSuccess) return fail(e, "scratch");
+    for (int i = 0; i < 6; ++i) blk2[i] = static_cast<char *>(base2) + at2[i];
     p.qn = static_cast<uint32_t *>(blk2[0]);
     uint32_t *qpre = static_cast<uint32_t *>(blk2[1]);
     p.qpre = qpre;
