@@ -844,7 +844,7 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             tm.mark(StageTimer::kCompact0, st);
             check(launch_compact(CompactBatch{d_jobs, (int)jobs.size(), d_word_off}, word_off.back(), st), "compact");
             for (size_t i = 0; i < region_jobs.size(); ++i)
-                check(launch_compact_regions(region_jobs[i], region_counts[i], st), "compact");
+                check(launch_compact_regions(region_jobs[i], region_counts[i], ctx->num_sms, st), "compact");
             if (!kjobs.empty())
                 check(launch_compact_keys(KeyBatch{d_kjobs, (int)kjobs.size(), d_blk_off}, blk_off.back(), st), "keys");
             tm.mark(StageTimer::kCompact, st);

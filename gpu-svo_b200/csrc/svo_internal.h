@@ -201,7 +201,7 @@ cudaError_t launch_level_totals(const BatchDev &b, cudaStream_t st);
 cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStream_t st);
 cudaError_t launch_compact_keys(const KeyBatch &k, uint64_t total_blocks, cudaStream_t st);
 // Levels 1 and 2 of a region-mode job (job.rflag set), one block per level-0 region.
-cudaError_t launch_compact_regions(const CompactJob &job, uint32_t regions, cudaStream_t st);
+cudaError_t launch_compact_regions(const CompactJob &job, uint32_t regions, int num_sms, cudaStream_t st);
 // one: the EmitParams of a one-mesh batch (host copy, passed by value to the
 // kernel), or null for a batch of several meshes.
 cudaError_t launch_emit(const EmitBatch &b, const EmitParams *one, uint64_t total_nodes, uint32_t flags,

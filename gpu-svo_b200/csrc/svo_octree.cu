@@ -453,17 +453,19 @@ __global__ void __launch_bounds__(256) k_compact(CompactBatch cb, uint64_t total
     compact_word(cb.job[j], l, w, v);
 }
 
-// Levels 1 and 2 of a region-mode mesh, one block per level-0 region: the
-// 256 level-1 and 32 level-2 words above a region lie inside it, so the
-// block of an unflagged region returns at once (most of them at res 2048).
-__global__ void __launch_bounds__(256) k_compact_regions(const __grid_constant__ CompactJob job) {
-    const uint32_t rg = blockIdx.x;
-    if (!job.rflag[rg]) return;
-    const uint64_t w1 = (uint64_t)rg * 256 + threadIdx.x;
-    compact_word(job, 1, w1, job.bits[job.py.woff[1] + w1]);
-    if (threadIdx.x < 32) {
-        const uint64_t w2 = (uint64_t)rg * 32 + threadIdx.x;
-        compact_word(job, 2, w2, job.bits[job.py.woff[2] + w2]);
+// Levels 1 and 2 of a region-mode mesh, region by region (a block takes
+// level-0 regions in turn): the 256 level-1 and 32 level-2 words above a
+// region lie inside it, so an unflagged region (most of them at res 2048)
+// costs one flag read.
+__global__ void __launch_bounds__(256) k_compact_regions(const __grid_constant__ CompactJob job, uint32_t regions) {
+    for (uint32_t rg = blockIdx.x; rg < regions; rg += gridDim.x) {
+        if (!job.rflag[rg]) continue;
+        const uint64_t w1 = (uint64_t)rg * 256 + threadIdx.x;
+        compact_word(job, 1, w1, job.bits[job.py.woff[1] + w1]);
+        if (threadIdx.x < 32) {
+            const uint64_t w2 = (uint64_t)rg * 32 + threadIdx.x;
+            compact_word(job, 2, w2, job.bits[job.py.woff[2] + w2]);
+        }
     }
 }
 
@@ -1003,9 +1005,9 @@ cudaError_t launch_compact(const CompactBatch &c, uint64_t total_words, cudaStre
     return cudaGetLastError();
 }
 
-cudaError_t launch_compact_regions(const CompactJob &job, uint32_t regions, cudaStream_t st) {
+cudaError_t launch_compact_regions(const CompactJob &job, uint32_t regions, int num_sms, cudaStream_t st) {
     if (regions == 0) return cudaSuccess;
-    k_compact_regions<<<regions, 256, 0, st>>>(job);
+    k_compact_regions<<<std::min<uint32_t>(regions, (uint32_t)num_sms * 8), 256, 0, st>>>(job, regions);
     count_launches(1);
     return cudaGetLastError();
 }

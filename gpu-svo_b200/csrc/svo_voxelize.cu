@@ -890,46 +890,74 @@ __device__ __forceinline__ uint32_t spread3_small(uint32_t v) {
 
 // The flags of the level-0 regions (64 x 64 x 32 voxels, region index =
 // morton3(x, y, z) >> 17) each triangle's voxel box (with a one-voxel margin)
-// reaches.  The mesh's grid and reciprocal units are kept across the
-// grid-stride loop while the mesh stays the same.
+// reaches.  The kernel waits on gathers (indices, then vertices), so each
+// thread takes 3 triangles at a time and issues all their loads before using
+// them; the mesh's grid and reciprocal units are kept while the mesh stays
+// the same.
+constexpr int kMarkBatch = 3;
+
 __global__ void __launch_bounds__(256) k_region_mark(BatchDev bd, int64_t total) {
     int cur = -1;
-    bool regions = false;
     float org[3] = {0, 0, 0}, inv[3] = {0, 0, 0};
-    for (int64_t gid = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gid < total;
-         gid += (int64_t)gridDim.x * blockDim.x) {
-        const int m = find_segment(bd.tri_off, bd.n, (uint64_t)gid);
-        const MeshDev &md = bd.mesh[m];
-        if (m != cur) {
-            cur = m;
-            regions = md.regions != 0;
-            const GridParams g = *md.gp;
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t g0 = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; g0 < total; g0 += stride * kMarkBatch) {
+        int mk[kMarkBatch];
+        bool live[kMarkBatch];
+        int64_t vi[kMarkBatch][3];
+#pragma unroll
+        for (int k = 0; k < kMarkBatch; ++k) {
+            const int64_t gid = g0 + k * stride;
+            live[k] = gid < total;
+            mk[k] = live[k] ? find_segment(bd.tri_off, bd.n, (uint64_t)gid) : 0;
+            const MeshDev &md = bd.mesh[mk[k]];
+            live[k] = live[k] && md.regions != 0;
+            const int64_t t = gid - (int64_t)bd.tri_off[mk[k]];
+#pragma unroll
+            for (int j = 0; j < 3; ++j) vi[k][j] = live[k] ? (md.tris ? (int64_t)__ldg(md.tris + 3 * t + j) : 3 * t + j) : 0;
+        }
+        float p[kMarkBatch][3][3];
+#pragma unroll
+        for (int k = 0; k < kMarkBatch; ++k) {
+            const MeshDev &md = bd.mesh[mk[k]];
+            // an index outside the mesh: skipped here, k_voxelize reports it
+            live[k] = live[k] && (uint64_t)vi[k][0] < (uint64_t)md.n_pts && (uint64_t)vi[k][1] < (uint64_t)md.n_pts &&
+                      (uint64_t)vi[k][2] < (uint64_t)md.n_pts;
+#pragma unroll
+            for (int j = 0; j < 3; ++j)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) p[k][j][a] = live[k] ? __ldg(md.pts + 3 * vi[k][j] + a) : 0.0f;
+        }
+#pragma unroll
+        for (int k = 0; k < kMarkBatch; ++k) {
+            if (!live[k]) continue;
+            const MeshDev &md = bd.mesh[mk[k]];
+            if (mk[k] != cur) {
+                cur = mk[k];
+                // the one-voxel margin absorbs an approximate reciprocal (2 ulp)
+#pragma unroll
+                for (int a = 0; a < 3; ++a) {
+                    org[a] = md.gp->origin[a];
+                    inv[a] = __fdividef(1.0f, md.gp->unit[a]);
+                }
+            }
+            int lo[3], hi[3];
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
-                org[a] = g.origin[a];
-                inv[a] = __frcp_rn(g.unit[a]);
+                const float v0 = __fsub_rn(p[k][0][a], org[a]), v1 = __fsub_rn(p[k][1][a], org[a]),
+                            v2 = __fsub_rn(p[k][2][a], org[a]);
+                // the margin is applied before the conversion, so +-inf and NaN clamp as in tri_box
+                lo[a] = clampi(f2i_rz(__fsub_rn(__fmul_rn(cminf(v0, cminf(v1, v2)), inv[a]), 1.0f)), 0, md.res[a] - 1);
+                hi[a] = clampi(f2i_rz(__fadd_rn(__fmul_rn(cmaxf(v0, cmaxf(v1, v2)), inv[a]), 1.0f)), 0, md.res[a] - 1);
             }
+            uint8_t *flag = bd.rflag + bd.cta_off[mk[k]];
+            // region bits: z at 3i, x at 3i + 1, y at 3i + 2 (z in 32-voxel, x and y in 64-voxel steps)
+            for (uint32_t rz = (uint32_t)lo[2] >> 5; rz <= (uint32_t)hi[2] >> 5; ++rz)
+                for (uint32_t ry = (uint32_t)lo[1] >> 6; ry <= (uint32_t)hi[1] >> 6; ++ry)
+                    for (uint32_t rx = (uint32_t)lo[0] >> 6; rx <= (uint32_t)hi[0] >> 6; ++rx) {
+                        uint8_t *f = flag + (spread3_small(rz) | spread3_small(rx) << 1 | spread3_small(ry) << 2);
+                        if (!*f) *f = 1;
+                    }
         }
-        if (!regions) continue;
-        float p[3][3];
-        if (!load_tri_checked(md.pts, md.tris, md.n_pts, gid - (int64_t)bd.tri_off[m], p)) continue;  // k_voxelize reports it
-        int lo[3], hi[3];
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const float v0 = __fsub_rn(p[0][a], org[a]), v1 = __fsub_rn(p[1][a], org[a]),
-                        v2 = __fsub_rn(p[2][a], org[a]);
-            // the margin is applied before the conversion, so +-inf and NaN clamp as in tri_box
-            lo[a] = clampi(f2i_rz(__fsub_rn(__fmul_rn(cminf(v0, cminf(v1, v2)), inv[a]), 1.0f)), 0, md.res[a] - 1);
-            hi[a] = clampi(f2i_rz(__fadd_rn(__fmul_rn(cmaxf(v0, cmaxf(v1, v2)), inv[a]), 1.0f)), 0, md.res[a] - 1);
-        }
-        uint8_t *flag = bd.rflag + bd.cta_off[m];
-        // region bits: z at 3i, x at 3i + 1, y at 3i + 2 (z in 32-voxel, x and y in 64-voxel steps)
-        for (uint32_t rz = (uint32_t)lo[2] >> 5; rz <= (uint32_t)hi[2] >> 5; ++rz)
-            for (uint32_t ry = (uint32_t)lo[1] >> 6; ry <= (uint32_t)hi[1] >> 6; ++ry)
-                for (uint32_t rx = (uint32_t)lo[0] >> 6; rx <= (uint32_t)hi[0] >> 6; ++rx) {
-                    uint8_t *f = flag + (spread3_small(rz) | spread3_small(rx) << 1 | spread3_small(ry) << 2);
-                    if (!*f) *f = 1;
-                }
     }
 }
 
