@@ -13,9 +13,11 @@
 // level: at level l (P a multiple of 2^l, u = P >> l) the cells u - d,
 // d in {0,1}^3, and a cell exists iff its parent is set in the level l+1
 // occupancy bitmap (at the top level: iff it is the root).  So:
-//   1. mark a candidate bitmap D over Q = P >> 1 (each bit stands for the 8
-//      lattice points 2Q + r) from the node groups of levels >= 1 -- every
-//      level-0 corner is also a corner of a level-1 node;
+//   1. build a candidate bitmap D over Q = P >> 1 (each bit stands for the 8
+//      lattice points 2Q + r): the corners of the nodes of levels >= 1 --
+//      every level-0 corner is also a corner of a level-1 node.  The
+//      level-1 corners come word by word from the level-2 bitmap
+//      (k_dedup_build), the coarser levels' by marking their node groups;
 //   2. walk D's words in order and derive, per Q, what its 8 points need
 //      from the parent bitmaps (coarser levels only for r = 0), for the 64 Q
 //      of a word at once by shifts of whole bitmap words; pack it into one
