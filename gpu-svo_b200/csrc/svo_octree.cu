@@ -411,6 +411,29 @@ __global__ void k_level_totals(BatchDev bd) {
 // In a region-mode mesh a word of levels 0-3 lies inside one level-0 region
 // (level-l word w covers level-0 words w * 8^l ..): an unflagged one is
 // empty and is not read.
+// The set-bit codes of the warp's 32 words, whose outputs are one contiguous
+// range in lane order (lane i's codes at o, o + 1, ...; lanes without bits
+// hold pc = 0): staged in shared memory as (lane, bit) entries, then read in
+// order, each turned into its code (the owning lane's b64 + bit) and stored
+// coalesced.  All 32 lanes call; lane 0 must hold a word of the range.
+__device__ __forceinline__ void warp_codes(uint64_t *out, uint32_t o, uint32_t pc, uint64_t v, uint64_t b64,
+                                           uint16_t *stage, int lane) {
+    const uint32_t start = __shfl_sync(0xFFFFFFFFu, o, 0);
+    const uint32_t tot = __reduce_add_sync(0xFFFFFFFFu, pc);
+    uint32_t at = o - start;
+    for (uint64_t m = v; m; m &= m - 1) stage[at++] = (uint16_t)((uint32_t)lane << 6 | (uint32_t)(__ffsll((long long)m) - 1));
+    __syncwarp();
+    const uint32_t blo = (uint32_t)b64, bhi = (uint32_t)(b64 >> 32);
+    for (uint32_t i0 = 0; i0 < tot; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        const uint32_t e = i < tot ? stage[i] : 0u;
+        const int src = (int)(e >> 6);
+        const uint64_t base = (uint64_t)__shfl_sync(0xFFFFFFFFu, bhi, src) << 32 | __shfl_sync(0xFFFFFFFFu, blo, src);
+        if (i < tot) out[start + i] = base + (e & 63u);
+    }
+    __syncwarp();
+}
+
 // Word w of level l holding v (read by the caller; 0 for a lane without a
 // word): rank from the block prefix and the 8-lane popcount prefix, then the
 // positions.  All 32 lanes of the warp call (8 aligned lanes per block).
@@ -424,8 +447,8 @@ __device__ __forceinline__ void compact_word(const CompactJob &job, int l, uint6
         const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d, 8);
         if (sub >= d) x += y;
     }
-    if (!v) return;
     const uint32_t r = r0 + x - pc;
+    if (!v) return;
     if (job.wpre && l >= 1) job.wpre[job.py.woff[l] - job.py.woff[1] + w] = r;
     uint64_t *o = job.out + job.koff[l] + r;
     const uint64_t b64 = w * 64;
@@ -473,6 +496,7 @@ __global__ void __launch_bounds__(256) k_compact_regions(const __grid_constant__
 // only: a mesh's level-3 code list is exactly its non-empty level-0 blocks,
 // in order.  8 lanes per block, one word each.
 __global__ void __launch_bounds__(256) k_compact_keys(KeyBatch kb, uint64_t total_blocks) {
+    __shared__ uint16_t stage[8][2048];  // a warp's 4 blocks x 512 bits
     const uint64_t gi = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
     const uint64_t item = gi >> 3;
     if (((gi >> 5) << 2) >= total_blocks) return;  // whole warps stay for the shuffles
@@ -493,6 +517,14 @@ __global__ void __launch_bounds__(256) k_compact_keys(KeyBatch kb, uint64_t tota
     for (int d = 1; d < 8; d <<= 1) {
         const uint32_t y = __shfl_up_sync(0xFFFFFFFFu, x, d, 8);
         if (sub >= d) x += y;
+    }
+    // the warp's blocks are consecutive non-empty blocks of one mesh (its
+    // outputs one range) unless it straddles two meshes
+    const int j0 = __shfl_sync(0xFFFFFFFFu, j, 0);
+    if (__all_sync(0xFFFFFFFFu, item >= total_blocks || j == j0)) {
+        warp_codes(kb.job[j0].out, item < total_blocks ? r + x - pc : 0xFFFFFFFFu, pc, v, (blk * 8 + sub) * 64,
+                   stage[threadIdx.x >> 5], threadIdx.x & 31);
+        return;
     }
     if (!v) return;
     uint64_t *o = kb.job[j].out + r + x - pc;
