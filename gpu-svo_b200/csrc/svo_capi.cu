@@ -636,6 +636,21 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             std::vector<DedupRun *> druns(n, nullptr);
             std::vector<int> drc(n, SVO_OK);
             std::vector<std::string> dmsg(n);
+            std::vector<char> dstarted(n, 0);
+            auto dedup_start = [&](int j) {  // the first step of mesh j's dedup (bitmaps only)
+                dstarted[j] = 1;
+                const MeshHost &mh = b->m[wave[j]];
+                const MeshDev &md = b->h_mesh[dev_k[j]];
+                const uint32_t R = 1u << (mh.py.grid_levels - 1);
+                const uint64_t *bits[kMaxLevels];
+                uint32_t sides[kMaxLevels];
+                for (int l = 0; l <= mh.T && l < kMaxLevels; ++l) {
+                    bits[l] = md.bits + mh.py.woff[l];
+                    sides[l] = std::max<uint32_t>(1u, R >> l);
+                }
+                drc[j] = dedup_begin(ctx->pool, ds, mh.T, bits, sides, ctx->num_sms, &druns[j]);
+                if (drc[j] != SVO_OK) dmsg[j] = svo_last_error();
+            };
             struct DedupGuard {  // on every exit: unfinished runs freed, the dedup stream joined
                 std::vector<DedupRun *> &runs;
                 decltype(join_dedup) &join;
@@ -653,18 +668,15 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
                     check(cudaStreamWaitEvent(ds, dset->fork, 0), "fork");
                 }
                 tm.mark(StageTimer::kDedup0, ds);
+                // early starts hold their candidate bitmaps (R^3 / 8 bytes each) until their
+                // finish: up to 4 GiB of them; the other meshes start just before they finish
+                uint64_t early = 0;
                 for (int j = 0; j < n; ++j) {
                     const MeshHost &mh = b->m[wave[j]];
-                    const MeshDev &md = b->h_mesh[dev_k[j]];
-                    const uint32_t R = 1u << (mh.py.grid_levels - 1);
-                    const uint64_t *bits[kMaxLevels];
-                    uint32_t sides[kMaxLevels];
-                    for (int l = 0; l <= mh.T && l < kMaxLevels; ++l) {
-                        bits[l] = md.bits + mh.py.woff[l];
-                        sides[l] = std::max<uint32_t>(1u, R >> l);
-                    }
-                    drc[j] = dedup_begin(ctx->pool, ds, mh.T, bits, sides, ctx->num_sms, &druns[j]);
-                    if (drc[j] != SVO_OK) dmsg[j] = svo_last_error();
+                    const uint64_t R = 1ull << (mh.py.grid_levels - 1);
+                    if (j > 0 && early + R * R * R / 8 > (4ull << 30)) break;
+                    early += R * R * R / 8;
+                    dedup_start(j);
                 }
             }
             // outputs, code lists, job tables
@@ -911,7 +923,9 @@ int batch_phase_b(svo_batch *b, int first, int count, svo_result **out, int *sta
             // after the emission's own checks.
             if (dd) {
                 for (int j = 0; j < n && rc == SVO_OK; ++j) {
-                    if (b->m[wave[j]].status != SVO_OK || !druns[j]) continue;
+                    if (b->m[wave[j]].status != SVO_OK) continue;
+                    if (!dstarted[j]) dedup_start(j);
+                    if (!druns[j]) continue;
                     drc[j] = dedup_finish(druns[j], ctx->out_pool, ep[j], res[j]->n_dedup, res[j]->dedup);
                     druns[j] = nullptr;
                     if (drc[j] != SVO_OK) dmsg[j] = svo_last_error();
