@@ -100,7 +100,9 @@ uint64_t estimate_parts(int64_t n_points, int64_t n_tris, const int res[3], uint
     while (side < (uint64_t)max_res(res)) side *= 2;
     const uint64_t nt = n_tris > 0 ? (uint64_t)n_tris : (uint64_t)std::max<int64_t>(n_points, 0) / 3;
     const uint64_t inputs = 12 * (uint64_t)std::max<int64_t>(n_points, 0) + 12 * nt;
-    const uint64_t scratch = side * side * side / 7 + 32 * nt + (1u << 20);
+    // level bitmaps (side^3 / 7 bytes), triangle queues; with dedup its candidate bitmap (side^3 / 8)
+    const uint64_t scratch = side * side * side / 7 + 32 * nt + (1u << 20) +
+                             ((flags & SVO_FLAG_DEDUP) ? side * side * side / 8 : 0);
     const uint64_t nodes = 16 * side * side;
     uint64_t per_node = sizeof(svo_node);
     if (!(flags & SVO_FLAG_NO_VERT_EDGE)) per_node += 8 * sizeof(svo_vertex) + 12 * sizeof(svo_edge);

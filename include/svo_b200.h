@@ -241,7 +241,8 @@ typedef struct svo_server_stats_t {
     uint64_t decided_batches;     /* of those, batches that have made their keep/requeue decision */
 } svo_server_stats_t;
 /* Device bytes admission reserves for a mesh: inputs, scratch of a res^3
- * grid and the outputs of 16*res^2 nodes (a closed surface spanning it). */
+ * grid (with SVO_FLAG_DEDUP its res^3-bit candidate bitmap too) and the
+ * outputs of 16*res^2 nodes (a closed surface spanning it). */
 uint64_t svo_estimate_bytes(int64_t n_points, int64_t n_tris, int res_x, int res_y, int res_z, uint32_t flags);
 int svo_server_create(svo_ctx *ctx, const svo_server_config *cfg, svo_server **out);
 int svo_server_submit(svo_server *s, const svo_mesh_desc *desc, uint64_t *ticket);

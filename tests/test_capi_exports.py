@@ -35,3 +35,6 @@ def test_estimate_bytes_host_only(svo_mod):
     assert svo_mod.estimate_bytes(1000, 2000, 1024, svo_mod.FLAG_NO_VERT_EDGE) < svo_mod.estimate_bytes(1000, 2000, 1024)
     # 16 res^2 nodes of 632 bytes dominate at res 1024
     assert 16 * 1024 ** 2 * 632 < svo_mod.estimate_bytes(0, 0, 1024) < 12e9
+    # the dedup's candidate bitmap (res^3 bits) comes on top of its 32 key bytes per node
+    plain, dedup = svo_mod.estimate_bytes(0, 0, 1024), svo_mod.estimate_bytes(0, 0, 1024, svo_mod.FLAG_DEDUP)
+    assert dedup - plain == 1024 ** 3 // 8 + 16 * 1024 ** 2 * 32
