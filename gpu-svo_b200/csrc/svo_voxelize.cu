@@ -84,12 +84,23 @@ __global__ void k_bbox_reduce(BatchDev bd) {
         hi[a] = __reduce_max_sync(0xFFFFFFFFu, hi[a]);
     }
     if (__any_sync(0xFFFFFFFFu, bad) && (threadIdx.x & 31) == 0) atomicOr(&md.gp->status, kStatusNonFinite);
+    // the block's extremes, then one atomic per value and block (the 6 words
+    // are shared by every block of the mesh)
+    __shared__ uint32_t wmm[32][6];
+    const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     if ((threadIdx.x & 31) == 0) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            atomicMin(md.mm + a, lo[a]);
-            atomicMax(md.mm + 3 + a, hi[a]);
+            wmm[warp][a] = lo[a];
+            wmm[warp][3 + a] = hi[a];
         }
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        uint32_t v = wmm[0][threadIdx.x];
+        for (int w = 1; w < nwarp; ++w) v = threadIdx.x < 3 ? min(v, wmm[w][threadIdx.x]) : max(v, wmm[w][threadIdx.x]);
+        if (threadIdx.x < 3) atomicMin(md.mm + threadIdx.x, v);
+        else atomicMax(md.mm + threadIdx.x, v);
     }
 }
 
