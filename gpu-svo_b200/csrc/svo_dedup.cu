@@ -70,6 +70,20 @@ struct DedupParams {
     const struct DedupTables *tables;  // built once per dedup by k_dedup_tables
 };
 
+// Adds the block's sum of v (each thread's share) to *dst with one atomic.
+// All threads of the block call.
+__device__ __forceinline__ void block_add(unsigned long long *dst, uint32_t v) {
+    __shared__ uint32_t part[32];
+    v = __reduce_add_sync(0xFFFFFFFFu, v);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        uint32_t s = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0u;
+        s = __reduce_add_sync(0xFFFFFFFFu, s);
+        if (threadIdx.x == 0 && s) atomicAdd(dst, (unsigned long long)s);
+    }
+}
+
 __device__ __forceinline__ void mark_chunk(const DedupParams &p, uint64_t bit) {
     const uint64_t ch = bit >> 11;
     uint32_t *g = p.G + (ch >> 5);
@@ -128,8 +142,7 @@ __global__ void k_dedup_mark(const __grid_constant__ DedupParams p, uint32_t fir
             }
         }
     }
-    fresh = __reduce_add_sync(0xFFFFFFFFu, fresh);
-    if ((threadIdx.x & 31) == 0 && fresh) atomicAdd(p.nq, (unsigned long long)fresh);
+    block_add(p.nq, fresh);
 }
 
 // Bit e of the result: cell v - e exists at the level whose occupancy bitmap
@@ -677,8 +690,7 @@ __global__ void __launch_bounds__(256) k_dedup_build(const __grid_constant__ Ded
             cnt += __popcll(w);
         }
     }
-    cnt = __reduce_add_sync(0xFFFFFFFFu, cnt);
-    if (lane == 0 && cnt) atomicAdd(p.nq, (unsigned long long)cnt);
+    block_add(p.nq, cnt);
 }
 
 // The touched chunks in order: per-word popcounts of G, then (after a scan)
