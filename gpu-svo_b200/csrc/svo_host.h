@@ -23,4 +23,10 @@ struct TraceRange {
 // min + width * (x, y, z) computed on the host (separately rounded).
 int write_voxels(const uint64_t *keys, int64_t n, const float origin[3], float width, const char *path);
 
+// Installs a function a server calls, under its own lock, each time one of its
+// requests finishes (built, failed or cancelled), with the request's ticket.
+// The function must not call back into that server.  A fleet collects its
+// members' completions this way.
+void server_on_finish(svo_server *s, void (*fn)(void *arg, uint64_t ticket), void *arg);
+
 }  // namespace svo::host

@@ -62,6 +62,8 @@ struct svo_server {
     std::vector<cudaStream_t> streams;
     uint64_t batches = 0, built = 0, requeued = 0;
     double build_s = 0.0, queue_s = 0.0;  // summed over batches / requests
+    void (*on_finish)(void *, uint64_t) = nullptr;  // called under mu for each finished request
+    void *on_finish_arg = nullptr;
 };
 
 namespace {
@@ -133,6 +135,7 @@ void publish(svo_server *s, svo_server::Req *r, svo_result *res, int status, uin
     r->t_done = now;
     r->done = true;
     s->finished.push_back(r->ticket);
+    if (s->on_finish) s->on_finish(s->on_finish_arg, r->ticket);
 }
 
 // seq: the batch's admission sequence number.  Batches count concurrently but
@@ -264,6 +267,16 @@ void worker(svo_server *s, int w) {
 }
 
 }  // namespace
+
+namespace svo::host {
+
+void server_on_finish(svo_server *s, void (*fn)(void *, uint64_t), void *arg) {
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->on_finish = fn;
+    s->on_finish_arg = arg;
+}
+
+}  // namespace svo::host
 
 extern "C" {
 

@@ -157,6 +157,16 @@ def lib() -> C.CDLL:
         L.svo_debug_fail_alloc.restype = i64
         L.svo_server_destroy.argtypes = [vp]
         L.svo_server_destroy.restype = None
+        L.svo_fleet_create.argtypes = [C.POINTER(vp), C.c_int, C.POINTER(ServerConfig), C.POINTER(vp)]
+        L.svo_fleet_submit.argtypes = L.svo_server_submit.argtypes
+        L.svo_fleet_wait.argtypes = L.svo_server_wait.argtypes
+        L.svo_fleet_next.argtypes = L.svo_server_next.argtypes
+        L.svo_fleet_release.argtypes = L.svo_server_release.argtypes
+        L.svo_fleet_cancel.argtypes = L.svo_server_cancel.argtypes
+        L.svo_fleet_member.argtypes = [vp, C.c_uint64]
+        L.svo_fleet_stats.argtypes = [vp, C.c_int, C.POINTER(ServerStats)]
+        L.svo_fleet_destroy.argtypes = [vp]
+        L.svo_fleet_destroy.restype = None
         L.svo_ctx_device.argtypes = [vp, C.POINTER(C.c_int)]
         L.svo_kernel_launches.restype = i64
         L.svo_result_num_dedup.argtypes = [vp, C.c_int]
@@ -323,6 +333,8 @@ class Server:
     """svo_server: continuous batching of build requests under a device-memory
     budget.  Mesh arrays must stay alive until their request is released."""
 
+    _api = "svo_server_"
+
     def __init__(self, ctx: "Context", mem_budget: int, workers: int = 2, max_batch: int = 64, flags: int = 0):
         cfg = ServerConfig(int(mem_budget), int(workers), int(max_batch), int(flags))
         h = C.c_void_p()
@@ -331,10 +343,13 @@ class Server:
         self._flags = flags
         self._keep = {}
 
+    def _fn(self, name):
+        return getattr(lib(), self._api + name)
+
     def submit(self, points, tris, res) -> int:
         descs, keep = _descs([(points, tris, res)], self._flags)
         t = C.c_uint64()
-        _check(lib().svo_server_submit(self._h, descs, C.byref(t)))
+        _check(self._fn("submit")(self._h, descs, C.byref(t)))
         self._keep[t.value] = (descs, keep)
         return t.value
 
@@ -343,7 +358,7 @@ class Server:
         r = C.c_void_p()
         st = C.c_int()
         lat = C.c_double()
-        rc = lib().svo_server_wait(self._h, ticket, timeout_us, C.byref(r), C.byref(st), C.byref(lat))
+        rc = self._fn("wait")(self._h, ticket, timeout_us, C.byref(r), C.byref(st), C.byref(lat))
         if rc == ERR_TIMEOUT:
             return None
         _check(rc)
@@ -356,19 +371,19 @@ class Server:
         r = C.c_void_p()
         st = C.c_int()
         lat = C.c_double()
-        rc = lib().svo_server_next(self._h, timeout_us, C.byref(t), C.byref(r), C.byref(st), C.byref(lat))
+        rc = self._fn("next")(self._h, timeout_us, C.byref(t), C.byref(r), C.byref(st), C.byref(lat))
         if rc == ERR_TIMEOUT:
             return None
         _check(rc)
         return t.value, (Result(r, owned=False) if st.value == OK else None), st.value, lat.value
 
     def release(self, ticket: int) -> None:
-        _check(lib().svo_server_release(self._h, ticket))
+        _check(self._fn("release")(self._h, ticket))
         self._keep.pop(ticket, None)
 
     def cancel(self, ticket: int) -> None:
         """Withdraws a queued request (it finishes with ERR_CANCELLED)."""
-        _check(lib().svo_server_cancel(self._h, ticket))
+        _check(self._fn("cancel")(self._h, ticket))
 
     def stats(self) -> dict:
         s = ServerStats()
@@ -377,7 +392,7 @@ class Server:
 
     def close(self) -> None:
         if self._h:
-            lib().svo_server_destroy(self._h)
+            self._fn("destroy")(self._h)
             self._h = None
             self._keep.clear()
 
@@ -386,6 +401,36 @@ class Server:
             self.close()
         except Exception:
             pass
+
+
+class Fleet(Server):
+    """svo_fleet: one server per context (one context per GPU) behind one
+    ticket space; each request is built whole on the member holding the fewest
+    estimated bytes.  The contexts must outlive the fleet."""
+
+    _api = "svo_fleet_"
+
+    def __init__(self, ctxs, mem_budget: int, workers: int = 2, max_batch: int = 64, flags: int = 0):
+        cfg = ServerConfig(int(mem_budget), int(workers), int(max_batch), int(flags))
+        hs = (C.c_void_p * len(ctxs))(*[c.handle for c in ctxs])
+        h = C.c_void_p()
+        _check(lib().svo_fleet_create(hs, len(ctxs), C.byref(cfg), C.byref(h)))
+        self._h = h
+        self._flags = flags
+        self._keep = {}
+        self._n = len(ctxs)
+
+    def member(self, ticket: int) -> int:
+        """Index of the context that builds `ticket` (-1: not held)."""
+        return lib().svo_fleet_member(self._h, ticket)
+
+    def stats(self, member: int = None):
+        """One member's server statistics, or a list of all of them."""
+        if member is None:
+            return [self.stats(i) for i in range(self._n)]
+        s = ServerStats()
+        _check(lib().svo_fleet_stats(self._h, member, C.byref(s)))
+        return {k: getattr(s, k) for k, _ in ServerStats._fields_}
 
 
 def _descs(meshes, flags):

@@ -268,6 +268,32 @@ int svo_server_stats(const svo_server *s, svo_server_stats_t *out);
  * that request from being admitted. */
 void svo_server_destroy(svo_server *s);
 
+/* ---- served builds over several GPUs (no counterpart in the reference) -----
+ * One svo_server per context -- one context per GPU, each made by
+ * svo_ctx_create on its own device -- behind one ticket space.  Every request
+ * is built whole on one member: a submission goes to the member with the
+ * fewest estimated bytes (svo_estimate_bytes) submitted and not yet released,
+ * ties to the lowest index.  The members share nothing and never exchange
+ * data; cfg (mem_budget included) applies to each member.  The calls mirror
+ * svo_server_*: results stay owned by their member until svo_fleet_release,
+ * svo_fleet_next reports finished requests of all members in completion
+ * order.  The contexts must outlive the fleet. */
+typedef struct svo_fleet svo_fleet;
+int svo_fleet_create(svo_ctx *const *ctxs, int n, const svo_server_config *cfg, svo_fleet **out);
+int svo_fleet_submit(svo_fleet *f, const svo_mesh_desc *desc, uint64_t *ticket);
+int svo_fleet_wait(svo_fleet *f, uint64_t ticket, int64_t timeout_us, svo_result **result, int *status,
+                   double *latency_s);
+int svo_fleet_next(svo_fleet *f, int64_t timeout_us, uint64_t *ticket, svo_result **result, int *status,
+                   double *latency_s);
+int svo_fleet_release(svo_fleet *f, uint64_t ticket);
+int svo_fleet_cancel(svo_fleet *f, uint64_t ticket);
+/* The member (index into ctxs) that builds a ticket, -1 for a ticket the fleet
+ * does not hold (never issued, or released). */
+int svo_fleet_member(const svo_fleet *f, uint64_t ticket);
+int svo_fleet_stats(const svo_fleet *f, int member, svo_server_stats_t *out);
+/* Destroys the members (svo_server_destroy each), then the fleet. */
+void svo_fleet_destroy(svo_fleet *f);
+
 /* Sorted surface-voxel Morton keys of a mesh (the first stage of svo_build:
  * same bounding cube, same voxel test, same key list as svo_result_copy_keys)
  * without allocating any device memory.  No counterpart in the reference.

@@ -38,3 +38,21 @@ def test_estimate_bytes_host_only(svo_mod):
     # the dedup's candidate bitmap (res^3 bits) comes on top of its 32 key bytes per node
     plain, dedup = svo_mod.estimate_bytes(0, 0, 1024), svo_mod.estimate_bytes(0, 0, 1024, svo_mod.FLAG_DEDUP)
     assert dedup - plain == 1024 ** 3 // 8 + 16 * 1024 ** 2 * 32
+
+
+def test_fleet_argument_checks_host_only(svo_mod):
+    """The multi-GPU fleet rejects bad arguments before touching a device."""
+    import ctypes as C
+
+    L = svo_mod.lib()
+    h = C.c_void_p()
+    cfg = svo_mod.ServerConfig(1 << 30, 1, 1, 0)
+    assert L.svo_fleet_create(None, 1, C.byref(cfg), C.byref(h)) == svo_mod.ERR_INVALID_ARGUMENT
+    none = (C.c_void_p * 1)(None)
+    assert L.svo_fleet_create(none, 1, C.byref(cfg), C.byref(h)) == svo_mod.ERR_INVALID_ARGUMENT
+    assert L.svo_fleet_create(none, 0, C.byref(cfg), C.byref(h)) == svo_mod.ERR_INVALID_ARGUMENT
+    assert not h.value
+    assert L.svo_fleet_member(None, 5) == -1
+    assert L.svo_fleet_stats(None, 0, None) == svo_mod.ERR_INVALID_ARGUMENT
+    assert L.svo_fleet_release(None, 1) == svo_mod.ERR_INVALID_ARGUMENT
+    L.svo_fleet_destroy(None)

@@ -188,3 +188,75 @@ def test_served_results_match_oracle(gpu_ctx, svo_mod, oracle_mod):
         assert_same(r, oracle_mod.build_svo(p, f, res))
         srv.release(t)
     srv.close()
+
+
+def test_fleet_spreads_requests_and_matches_alone(gpu_ctx, svo_mod):
+    """svo_fleet over two contexts (two GPUs in production; here two contexts
+    of one GPU, which share nothing and never wait on each other): requests
+    spread over both members, every result is bit for bit the plain build's,
+    svo_fleet_next reports each ticket once, and released tickets leave the
+    fleet."""
+    reqs = _requests(20, seed=14)
+    ctx2 = svo_mod.Context(0)
+    fleet = svo_mod.Fleet([gpu_ctx, ctx2], 16 << 30, workers=2, max_batch=8)
+    tickets = [fleet.submit(*r) for r in reqs]
+    assert len(set(tickets)) == len(tickets)
+    members = [fleet.member(t) for t in tickets]
+    assert set(members) == {0, 1}
+    by_ticket = dict(zip(tickets, reqs))
+    seen = set()
+    for _ in reqs:
+        got = fleet.next(timeout_us=WAIT_US)
+        assert got is not None, f"request not built in time; {fleet.stats()}"
+        t, r, st, lat = got
+        assert t in by_ticket and t not in seen and st == 0 and lat > 0
+        seen.add(t)
+        _same(r, gpu_ctx.build(*by_ticket[t]))
+        fleet.release(t)
+        assert fleet.member(t) == -1
+    assert fleet.next(timeout_us=1000) is None
+    stats = fleet.stats()
+    assert [s["built"] for s in stats] == [members.count(0), members.count(1)]
+    assert all(s["reserved_bytes"] == 0 and s["queued"] == 0 for s in stats)
+    with pytest.raises(svo_mod.SvoError) as e:
+        fleet.wait(tickets[0], timeout_us=0)
+    assert e.value.code == svo_mod.ERR_INVALID_ARGUMENT
+    fleet.close()
+    ctx2.close()
+
+
+def test_fleet_cancel_and_wait(gpu_ctx, svo_mod):
+    """A request queued behind a large one on its member is cancelled through
+    the fleet: svo_fleet_wait and svo_fleet_next report it with ERR_CANCELLED;
+    the large builds on both members are unaffected."""
+    from svo_b200 import meshgen
+
+    soup, _, _ = meshgen.torus_slivers(200_000)
+    small = _requests(1, seed=15, res_choices=(64,))[0]
+    ctx2 = svo_mod.Context(0)
+    fleet = svo_mod.Fleet([gpu_ctx, ctx2], 8 << 30, workers=1, max_batch=1)
+    a = fleet.submit(soup, None, 512)
+    b = fleet.submit(soup, None, 512)
+    c = fleet.submit(*small)  # both members hold one large request: the tie goes to member 0
+    assert (fleet.member(a), fleet.member(b), fleet.member(c)) == (0, 1, 0)
+    fleet.cancel(c)
+    r, st, _ = fleet.wait(c, timeout_us=WAIT_US)
+    assert st == svo_mod.ERR_CANCELLED and r is None
+    alone = gpu_ctx.build(soup, None, 512)
+    order = []
+    for _ in range(3):
+        got = fleet.next(timeout_us=WAIT_US)
+        assert got is not None, "request not built in time"
+        t, r, st, _ = got
+        order.append(t)
+        if t == c:
+            assert st == svo_mod.ERR_CANCELLED and r is None
+        else:
+            assert st == 0
+            _same(r, alone)
+    assert sorted(order) == sorted([a, b, c]) and order[0] == c
+    for t in (a, b, c):
+        fleet.release(t)
+    assert all(s["reserved_bytes"] == 0 for s in fleet.stats())
+    fleet.close()
+    ctx2.close()
