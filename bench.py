@@ -291,6 +291,13 @@ def batch_cpu_sample(meshes, stride: int = 32):
     return [(p, t, min(r, 256)) for p, t, r in meshes[::stride]]
 
 
+def workload_config(wname: str, triangles: int, res: int, flags: int, gpus: int) -> dict:
+    """The workload as both arms name it: the same dict in our line and in the
+    reference arm's (which times a sample of it, stated in its cpu_baseline)."""
+    return {"workload": wname, "triangles": triangles, "resolution": res, "flags": flags,
+            "parallelism": f"replicas{gpus}"}
+
+
 def run_reference(args, rank: int):
     if rank != 0:
         return
@@ -307,12 +314,16 @@ def run_reference(args, rank: int):
 
         sample = (f"every 32nd mesh of the 256-mesh batch ({len(sample_meshes)} meshes, {nt} triangles), "
                   f"resolution capped at 256, full builds")
+        config = {"workload": wname, "sample_triangles": nt, "resolution": res}
     else:
         pts, tris, res, wname, wflags = workload(args.workload)
         flags = wflags if args.flags < 0 else args.flags
+        if args.res:
+            res, wname = args.res, f"{wname.rsplit('_res', 1)[0]}_res{args.res}"
         stride = CPU_STRIDE[args.workload]
         spts, stris = cpu_sample(pts, tris, stride)
         nt = stris.shape[0]
+        config = workload_config(wname, n_triangles(pts, tris), res, flags, args.gpus)
 
         def one():
             return time_cpu_build(spts, stris, res, threads, flags)
@@ -327,7 +338,7 @@ def run_reference(args, rank: int):
         "impl": "reference", "metric": "tris/s", "value": value, "unit": "tris/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / len(times),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-        "config": {"workload": wname, "triangles": nt, "resolution": res},
+        "config": config, "sample_triangles": nt,
         "cpu_baseline": {"value": value, "unit": "tris/s", "cores": threads, "kind": "port", "sample": sample},
         "e2e": {"value": value, "unit": "tris/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         "note": "the reference has no CPU build path (its build is CUDA); this times the CPU restatement "
@@ -548,9 +559,10 @@ def run_ours(args, rank: int, world: int):
             "metric": "tris/s", "value": value, "unit": "tris/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": dist_max(sum(step_ms)) / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": wname, "triangles": nt, "resolution": res, "parallelism": f"replicas{world}",
-                       "l2_flush": "256 MiB device write before every step, outside the timed span",
-                       "tuning": dict(zip(TUNING_KEYS, tuning)), **info},
+            "config": {**workload_config(wname, nt, res, bflags, world),
+                       "l2_flush": "256 MiB device write before every step, outside the timed span"},
+            "octree": {k: v for k, v in info.items() if k != "flags"},
+            "tuning": dict(zip(TUNING_KEYS, tuning)),
             "nodes_per_s": nodes_per_s,
             "e2e": e2e, "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks.summary(),
             "gpu_launches": launches, "writer": writer, "ref_cuda_input": same_input,
