@@ -714,19 +714,33 @@ def run_batch(args, rank: int, world: int):
         e1.synchronize()
         return e0.elapsed_time(e1), extra
 
-    def batch_once(extra_flags=0):
+    def mark():
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(stream)
+        return e
+
+    def batch_once(extra_flags=0, phases=None):
+        # phases (a list, with FLAG_TIMINGS): the CUDA-event ms of the counting phase and of each wave
+        e = [mark()] if phases is not None else None
         b = ctx.batch(d_meshes, flags | extra_flags, sid)
+        if e:
+            e.append(mark())
         nodes, emit_ms, w = 0, 0.0, waves(b)
         for first, count in w:
             rs, st, rc = b.emit(first, count)
             if rc != 0:
                 raise RuntimeError(f"batch emit failed: {st}")
+            if e:
+                e.append(mark())
             if extra_flags & S.FLAG_TIMINGS:
                 emit_ms += rs[0].timings().get("emit", 0.0)
             for r in rs:
                 nodes += r.num_nodes
                 r.close()
         b.close()
+        if e:
+            e[-1].synchronize()
+            phases[:] = [e[i].elapsed_time(e[i + 1]) for i in range(len(e) - 1)]
         return nodes, emit_ms, len(w)
 
     def plain_once():
@@ -760,6 +774,12 @@ def run_batch(args, rank: int, world: int):
     value = world * nt * args.steps / (t_batch / 1e3)
     plain_value = world * nt * args.steps / (t_plain / 1e3)
     emit_ms = statistics.median([batch_once(S.FLAG_TIMINGS)[1] for _ in range(3)])
+    ph = []
+    flush.fill_(1)
+    batch_once(0, ph)
+    phases = {"count_ms": ph[0], "wave_ms": ph[1:],
+              "what": "one untimed batch after the timed steps: CUDA events on the build stream around "
+                      "svo_batch_create (counting phase of all meshes) and each svo_batch_emit wave"}
     peaks = json.load(open(PEAKS_PATH)) if os.path.exists(PEAKS_PATH) else {}
     peak = float(peaks.get("hbm_gbs", FALLBACK_HBM_GBS))
     emit_bytes = EMIT_BYTES_PER_NODE * nodes
@@ -787,7 +807,7 @@ def run_batch(args, rank: int, world: int):
             "nodes_per_s": world * nodes * args.steps / (t_batch / 1e3),
             "plain": {"value": plain_value, "unit": "tris/s", "ms_per_step": t_plain / args.steps,
                       "path": "one svo_build per mesh, same stream, same flags, default work split"},
-            "batch_over_plain": value / plain_value,
+            "batch_over_plain": value / plain_value, "phases": phases,
             "batch_equals_plain": same,
             "e2e": None,
             "roofline": {"kernel": "k_emit (all waves)", "bound": "hbm", "achieved": achieved, "peak": peak,
@@ -903,7 +923,8 @@ def extras(args, rank: int, world: int) -> dict:
     sv = copy.copy(args)
     sv.rates, sv.window, sv.flags = "500,2000", 0.5, -1
     serve = run_serve(sv, rank, world)
-    keep_b = ("value", "unit", "ms_per_step", "plain", "batch_over_plain", "batch_equals_plain", "config", "clocks")
+    keep_b = ("value", "unit", "ms_per_step", "plain", "batch_over_plain", "batch_equals_plain", "phases", "config",
+              "clocks")
     return {"batch256": {k: batch[k] for k in keep_b} if batch else None,
             "serve": {k: serve[k] for k in ("rates", "config", "clocks")} if serve else None}
 
